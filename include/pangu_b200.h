@@ -1,0 +1,223 @@
+/*
+ * pangu_b200.h -- C ABI of the B200 GRMHD stage engine.
+ *
+ * The engine replaces the per-RK-stage task functions of PANGU's ideal GRMHD
+ * task graph (pangu/src/task_list/ideal_grmhd.cc:62-94 registers them):
+ *
+ *   FixPrimitive            pangu/src/fixer/primitive_fixer.h:12
+ *   CalculateConservative   pangu/src/riemann_solver/conservative.h:12
+ *   CalculateFluxes         pangu/src/riemann_solver/riemann_solver.h (LAXF/HLL)
+ *   ConstraintedTransport   pangu/src/constrained_transport/constrained_transport.h
+ *   FluxDivergence + UpdateIndependentData (Parthenon, ideal_grmhd.cc:73-76)
+ *   AddGeometricSource      pangu/src/riemann_solver/source_term.h
+ *   Recovery                pangu/src/recovery/invertor.h:11
+ *   ApplyElectronHeating    pangu/src/riemann_solver/electron_heating.h:12
+ *   FixRecovery             pangu/src/fixer/recovery_fixer.h:12
+ *   EstimateTimestepMesh    pangu/src/initialization/timestep_estimation.h:10-11
+ *
+ * Every entry point is extern "C", never throws and never traps. It returns
+ * PANGU_OK (0) or a negative PANGU_E* code. Field arrays are caller-owned device memory laid
+ * out like a Parthenon MeshBlockPack with Kokkos LayoutRight:
+ *   [block][variable][k][j][i]  (i fastest), over the "entire" index domain
+ *   (interior plus ng ghost cells on each side of every active direction).
+ * The engine keeps no pointer to them past the call.
+ *
+ * Variable order inside prim/cons is the order of
+ * package_registration.cc:84-96:
+ *   density, energy, weighted_velocity[3], magnetic_field[3] (if enable_B),
+ *   entropy, electron_entropy (if enable_heating).
+ */
+#ifndef PANGU_B200_H
+#define PANGU_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define PANGU_OK 0
+#define PANGU_EINVAL (-1)     /* bad argument (null pointer, bad option)      */
+#define PANGU_ECUDA (-2)      /* a CUDA runtime call failed                    */
+#define PANGU_ENOMEM (-3)     /* engine-internal allocation failed             */
+#define PANGU_ENGHOST (-4)    /* ghost width too small for the limiter         */
+#define PANGU_ETOOBIG (-5)    /* size above a documented maximum               */
+
+/* ---- option enumerations (string values of the reference's params) ---- */
+#define PANGU_RIEMANN_LAXF 0  /* <core>/riemann_solver = laxf */
+#define PANGU_RIEMANN_HLL 1   /* <core>/riemann_solver = hll  */
+#define PANGU_LIMITER_PPM4 0  /* <core>/limiter = ppm4 */
+#define PANGU_LIMITER_MC 1    /* <core>/limiter = mc   */
+#define PANGU_RECOVERY_CHAINER 0  /* <core>/recovery = chainer  */
+#define PANGU_RECOVERY_ROBUSTER 1 /* <core>/recovery = robuster */
+/* <metric>/type, christoffel.h:145-147 */
+#define PANGU_METRIC_MINKOWSKI 0
+#define PANGU_METRIC_BL 1
+#define PANGU_METRIC_CKS 2
+#define PANGU_METRIC_MKS 3
+/* <electron>/model, heating_model.h:13-20 */
+#define PANGU_HEAT_CONSTANT 0
+#define PANGU_HEAT_HOWES 1
+#define PANGU_HEAT_KAWAZURA 2
+#define PANGU_HEAT_WERNER 3
+#define PANGU_HEAT_ROWAN 4
+#define PANGU_HEAT_SHARMA 5
+/* Parthenon <parthenon/mesh> ix*_bc / ox*_bc */
+#define PANGU_BC_PERIODIC 0
+#define PANGU_BC_OUTFLOW 1
+#define PANGU_BC_REFLECTING 2
+
+/* Runtime parameters of the "core" and "metric" packages, with the meaning
+ * and defaults of package_registration.cc:21-81 and :158-173. */
+typedef struct pangu_params {
+  /* <core> */
+  double cfl_number;          /* 0.8 */
+  double adiabatic_index;     /* 5/3 */
+  int32_t riemann_solver;     /* PANGU_RIEMANN_* (laxf) */
+  int32_t limiter;            /* PANGU_LIMITER_* (ppm4) */
+  double density_floor;       /* 1e-6 */
+  double energy_floor;        /* 1e-8 */
+  double density_floor_pow;   /* -1.5 */
+  double energy_floor_pow;    /* -2.5 */
+  int32_t enable_B;           /* false */
+  int32_t recovery;           /* PANGU_RECOVERY_* (chainer) */
+  int32_t enable_heating;     /* false */
+  int32_t reserved0;
+  double sigma_max;           /* 50 */
+  double lorentz_max;         /* 50 */
+  /* <electron> */
+  int32_t model;              /* PANGU_HEAT_* (constant) */
+  int32_t limit_kel;          /* true */
+  int32_t suppress_highb_heat;          /* false */
+  int32_t enforce_positive_dissipation; /* false */
+  double fel_constant;        /* 0.1 */
+  double gamma_e;             /* 4/3 */
+  double gamma_p;             /* 5/3 */
+  double ratio_min;           /* 1e-3 */
+  double ratio_max;           /* 1e3 */
+  double fel_0;               /* 0.1 */
+  /* <metric> */
+  int32_t metric_type;        /* PANGU_METRIC_* (minkowski) */
+  int32_t excise;             /* false */
+  double a;                   /* 0 */
+  double h;                   /* 0 */
+  double r_excise;            /* 1 */
+  double dexcise;             /* 1e-8 */
+  double pexcise;             /* 0.333e-12 */
+} pangu_params;
+
+/* A uniform mesh cut into a regular lattice of equal meshblocks
+ * (<parthenon/mesh> and <parthenon/meshblock>; refinement = none).
+ * Block b sits at lattice position (b1, b2, b3) with
+ * b = (b3 * nbx2 + b2) * nbx1 + b1. */
+typedef struct pangu_mesh {
+  int32_t nx1, nx2, nx3;      /* interior cells per meshblock */
+  int32_t nbx1, nbx2, nbx3;   /* meshblocks along each direction */
+  int32_t ng;                 /* ghost width of every active direction */
+  int32_t reserved0;
+  double x1min, x1max, x2min, x2max, x3min, x3max;
+  int32_t bc[6];              /* ix1, ox1, ix2, ox2, ix3, ox3: PANGU_BC_* */
+} pangu_mesh;
+
+/* One stage container ("base" or "1") of every block, as device pointers.
+ * Shapes use N1 = nx1 + 2 ng (or 1), N2, N3 likewise, NF = number of
+ * prim/cons components, NB = number of blocks.
+ * alfven, efield and flag are Metadata::OneCopy fields in the reference
+ * (package_registration.cc:121-145): both containers point at the same
+ * arrays. */
+typedef struct pangu_pack {
+  double *prim;    /* [NB][NF][N3][N2][N1] */
+  double *cons;    /* [NB][NF][N3][N2][N1] */
+  double *flux1;   /* [NB][NF][N3][N2][N1]; entry i is the face below cell i */
+  double *flux2;   /* [NB][NF][N3][N2][N1]; entry j is the face below cell j */
+  double *flux3;   /* [NB][NF][N3][N2][N1]; entry k is the face below cell k */
+  double *alfven;  /* [NB][3][N3][N2][N1] */
+  double *efield;  /* [NB][3][N3][N2][N1] */
+  double *flag;    /* [NB][N3][N2][N1]; chainer only (may be NULL otherwise) */
+} pangu_pack;
+
+/* Hit counters of the floors and fixers (not present in the reference, which
+ * has no counters; they are what makes "same floor and fixer hit counts"
+ * checkable). Indices into a uint64_t[PANGU_NCOUNTERS] array. */
+#define PANGU_CNT_RHO_FLOOR 0    /* FixPrimitive: density raised to the floor  */
+#define PANGU_CNT_ENG_FLOOR 1    /* FixPrimitive: energy raised to the floor   */
+#define PANGU_CNT_LORENTZ_CAP 2  /* FixPrimitive: velocity rescaled            */
+#define PANGU_CNT_C2P_2D 3       /* Recovery: Scheme2D succeeded               */
+#define PANGU_CNT_C2P_1DVSQ 4    /* Recovery: Scheme1Dvsq succeeded            */
+#define PANGU_CNT_C2P_1D 5       /* Recovery: Scheme1D succeeded               */
+#define PANGU_CNT_C2P_FAIL 6     /* Recovery: all three failed (flag = 0)      */
+#define PANGU_CNT_FIXRECOVERY 7  /* FixRecovery: cells repaired                */
+#define PANGU_CNT_KASTAUN_FAIL 8 /* Recovery (robuster): root solve failed     */
+#define PANGU_CNT_EXCISED 9      /* Recovery: CKS cells inside r_excise        */
+#define PANGU_NCOUNTERS 16
+
+/* Opaque engine handle: validated parameters, mesh geometry and the device
+ * tables derived from them (block origins, ghost-exchange map). */
+typedef struct pangu_engine pangu_engine;
+
+/* Number of prim/cons components for a parameter set
+ * (package_registration.cc:92-96). */
+int pangu_num_fields(const pangu_params *params);
+
+/* Validates params/mesh and builds the engine on the current CUDA device.
+ * Returns PANGU_ENGHOST when limiter = ppm4 and ng < 3 (PPM4 reads i-3,
+ * interpolater_ppm4.h:29-67 via laxf.cc:96-101) or limiter = mc and ng < 2. */
+int pangu_engine_create(const pangu_params *params, const pangu_mesh *mesh,
+                        pangu_engine **out);
+int pangu_engine_destroy(pangu_engine *engine);
+
+/* ---- per-task entry points (one per reference task) ------------------- */
+/* stream is a cudaStream_t passed as void*; NULL = legacy default stream. */
+int pangu_fix_primitive(pangu_engine *e, const pangu_pack *md, void *stream);
+int pangu_calculate_conservative(pangu_engine *e, const pangu_pack *md,
+                                 void *stream);
+int pangu_calculate_fluxes(pangu_engine *e, const pangu_pack *md, void *stream);
+int pangu_constrained_transport(pangu_engine *e, const pangu_pack *md,
+                                void *stream);
+/* mc1.cons = mc_init.cons - (beta*dt) * div(mc0 fluxes) over the interior
+ * (Parthenon FluxDivergence + UpdateIndependentData, ideal_grmhd.cc:73-76).
+ * dt is a DEVICE pointer to one double so a captured graph stays valid. */
+int pangu_flux_divergence_update(pangu_engine *e, const pangu_pack *mc_init,
+                                 const pangu_pack *mc0, const pangu_pack *mc1,
+                                 double beta, const double *dt, void *stream);
+/* Ghost exchange of a container at send time: periodic and block-to-block
+ * ghost cells of prim and flag receive the neighbour's interior values. */
+int pangu_exchange_ghosts(pangu_engine *e, const pangu_pack *md, void *stream);
+int pangu_add_geometric_source(pangu_engine *e, const pangu_pack *md,
+                               double beta, const double *dt, void *stream);
+int pangu_recovery(pangu_engine *e, const pangu_pack *md, void *stream);
+int pangu_apply_electron_heating(pangu_engine *e, const pangu_pack *md,
+                                 void *stream);
+int pangu_fix_recovery(pangu_engine *e, const pangu_pack *md, void *stream);
+/* Physical boundary conditions (outflow / reflecting) on prim and flag, in
+ * the face order inner x1, outer x1, inner x2, outer x2, inner x3, outer x3. */
+int pangu_apply_boundary_conditions(pangu_engine *e, const pangu_pack *md,
+                                    void *stream);
+/* dt estimate from the alfven field (timestep_estimation.cc:13-102),
+ * written to the DEVICE double *dt_out. */
+int pangu_estimate_dt(pangu_engine *e, const pangu_pack *md, double *dt_out,
+                      void *stream);
+
+/* ---- whole stage ------------------------------------------------------- */
+/* One RK stage of Simulator::MakeTaskCollection (ideal_grmhd.cc:23-120):
+ * stage = 1 or 2 of rk2, beta = integrator->beta[stage % 2],
+ * mc0 = stage_name[stage-1], mc1 = stage_name[stage], mc_init = "base".
+ * On the last stage the new dt estimate is written to dt_est (device). */
+int pangu_stage(pangu_engine *e, int stage, const pangu_pack *base,
+                const pangu_pack *one, double beta, const double *dt,
+                double *dt_est, void *stream);
+
+/* Device dt policy applied after each cycle: dt = min(dt_factor*dt, dt_est). */
+int pangu_update_dt(pangu_engine *e, double *dt, const double *dt_est,
+                    double dt_factor, void *stream);
+
+/* Counters accumulated since the last reset (host copy, synchronous). */
+int pangu_counters(pangu_engine *e, uint64_t out[PANGU_NCOUNTERS]);
+int pangu_reset_counters(pangu_engine *e, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PANGU_B200_H */
