@@ -35,12 +35,13 @@ def _newer(target: str, sources: list[str]) -> bool:
 
 def build_oracle(force: bool = False) -> str:
     src = [os.path.join(HERE, "oracle.cc"), os.path.join(HERE, "oracle_cell.h"),
-           os.path.join(ROOT, "include", "pangu_b200.h")]
+           os.path.join(ROOT, "include", "pangu_b200.h"),
+           os.path.join(ROOT, "pangu_b200", "csrc", "pgmath.h")]
     if not force and _newer(ORACLE_SO, src):
         return ORACLE_SO
     os.makedirs(os.path.dirname(ORACLE_SO), exist_ok=True)
     cmd = ["g++", *COMMON, "-fopenmp", "-I", os.path.join(ROOT, "include"),
-           src[0], "-o", ORACLE_SO]
+           "-I", os.path.join(ROOT, "pangu_b200", "csrc"), src[0], "-o", ORACLE_SO]
     subprocess.check_call(cmd)
     return ORACLE_SO
 

@@ -151,8 +151,8 @@ void fix_primitive(Ctx &c, pangu_pack &md) {
             const Real sa = (rad2 - a2) * (rad2 - a2) + 4.0 * a2 * z * z;
             r = std::sqrt(0.5 * (rad2 - a2 + std::sqrt(sa)));
           }
-          Real rho_floor = p.density_floor * std::pow(std::fmax(r, 1.0), p.density_floor_pow);
-          const Real eng_floor = p.energy_floor * std::pow(std::fmax(r, 1.0), p.energy_floor_pow);
+          Real rho_floor = p.density_floor * pgm::pow(std::fmax(r, 1.0), p.density_floor_pow);
+          const Real eng_floor = p.energy_floor * pgm::pow(std::fmax(r, 1.0), p.energy_floor_pow);
           Real gcov[4][4], gcon[4][4], gdet;
           metric_at(p.metric_type, xc, p.a, p.h, gcov, gcon, gdet);
           Real pc[NPRIM];
@@ -183,15 +183,15 @@ void fix_primitive(Ctx &c, pangu_pack &md) {
           const Real rho_after = kmax(pr, small);
           double *pk = p.enable_heating ? &P[at(g, b, g.pidx[KEL], k, j, i, g.NF)] : nullptr;
           if (p.enable_heating && rho_after != rho_before)
-            *pk *= std::pow(rho_after / rho_before, -gam);
+            *pk *= pgm::pow(rho_after / rho_before, -gam);
           double &pe = P[at(g, b, g.pidx[ENT], k, j, i, g.NF)];
-          pe = (gam - 1.0) * pu * std::pow(pr, -gam);
+          pe = (gam - 1.0) * pu * pgm::pow(pr, -gam);
           if (p.enable_heating) *pk = clamp_by_ratio(p.ratio_min, p.ratio_max, pe, *pk);
           if (p.metric_type == CKS && r < p.r_excise) {
             pr = p.dexcise;
             pu = e_excise;
             u1 = 0.0; u2 = 0.0; u3 = 0.0;
-            pe = (gam - 1.0) * e_excise * std::pow(p.dexcise, -gam);
+            pe = (gam - 1.0) * e_excise * pgm::pow(p.dexcise, -gam);
             if (p.enable_heating) *pk = e_excise;
           }
         }
@@ -274,7 +274,17 @@ void flux_dir(Ctx &c, pangu_pack &md, int dir) {
           Real xf[4] = {0.0, Xc(g, b, 0, i), Xc(g, b, 1, j), Xc(g, b, 2, k)};
           xf[dir] = Xf(g, b, dir - 1, dir == 1 ? i : (dir == 2 ? j : k));
           Real gcov[4][4], gcon[4][4], gdet;
-          metric_at(p.metric_type, xf, p.a, p.h, gcov, gcon, gdet);
+          code_metric(p.metric_type, xf, p.a, p.h, gcov);
+          if (!invert(gcov, gcon)) {
+            // Singular code metric (theta = 0 exactly on a polar face): the
+            // reference reads an unwritten inverse here (tensor_algebra.h:91-93
+            // returns before filling it). Defined as zero flux, zero speed.
+            md.alfven[at(g, b, dir - 1, k, j, i, 3)] = 0.0;
+            for (int s = 0; s < NPRIM; ++s)
+              if (g.pidx[s] >= 0) F[at(g, b, g.pidx[s], k, j, i, g.NF)] = 0.0;
+            continue;
+          }
+          gdet = determinant(gcov);
           Real vmaxL, vminL, vmaxR, vminR;
           const Real gam = p.adiabatic_index;
           fast_speed(gam, PL, gcov, gcon, dir, vmaxL, vminL);
@@ -857,6 +867,17 @@ double or_cell_heating(const double hp[6], const int flags[4], const double cell
 }
 double or_cell_clamp(double rmin, double rmax, double total, double electron) {
   return clamp_by_ratio(rmin, rmax, total, electron);
+}
+
+// The shared double-double routines, for their accuracy test.
+void or_pgm_pow(int n, const double *x, const double *y, double *out) {
+  for (int i = 0; i < n; ++i) out[i] = pgm::pow(x[i], y[i]);
+}
+void or_pgm_exp(int n, const double *x, double *out) {
+  for (int i = 0; i < n; ++i) out[i] = pgm::exp(x[i]);
+}
+void or_pgm_log(int n, const double *x, double *out) {
+  for (int i = 0; i < n; ++i) out[i] = pgm::log(x[i]);
 }
 
 }  // extern "C"

@@ -4,14 +4,22 @@
 //
 // Every function follows the reference's operation order line by line
 // (file:line cited on each) and is compiled with -ffp-contract=off so that
-// no multiply-add is fused behind the source's back. Transcendentals are the
-// C library's (std::exp, std::sin, ...), as in the reference's host build.
+// no multiply-add is fused behind the source's back. The coordinate maps use
+// the C library's exp/sin/cos, as the reference's host build does; pow, exp
+// and log of the physics use the double-double routines of pgmath.h, which
+// the engine runs bit-identically (the C2P chain is chaotic with respect to
+// one-ulp differences in floor-dominated cells). Those routines agree with
+// the C library's to the last bit on the golden vectors.
 // Parity anchor: the per-cell functions are checked against golden vectors
 // produced by the reference's own headers (tests/golden/make_golden.py).
 #ifndef PANGU_ORACLE_CELL_H
 #define PANGU_ORACLE_CELL_H
 
 #include <cmath>
+
+// pow/exp/log of the physics: the double-double routines shared with the
+// engine (bit-identical on host and device); see pgmath.h.
+#include "pgmath.h"
 
 namespace orc {
 
@@ -638,7 +646,7 @@ inline int invert(const Real U[9], Real prim[9], Real g,
   if ((rho0 <= 0.) || (uu <= 0.)) return 5;
   prim[RHO] = rho0;
   prim[ENY] = uu;
-  prim[ENT] = (g - 1.) * uu * std::pow(rho0, -g);
+  prim[ENT] = (g - 1.) * uu * pgm::pow(rho0, -g);
   harm_velocity(s, Gamma, W, prim);
   prim[BX1] = U[BX1];
   prim[BX2] = U[BX2];
@@ -660,7 +668,7 @@ inline Real W_of_vsq(Real D, Real K, Real vsq, Real *p, Real *rho, Real *uu,
                      Real g) {
   Real gtmp = (1. - vsq);
   *rho = D * std::sqrt(gtmp);
-  *p = (K * std::pow(*rho, g));
+  *p = (K * pgm::pow(*rho, g));
   *uu = (*p / (g - 1.));
   return ((*rho + *uu + *p) / gtmp);
 }
@@ -742,7 +750,7 @@ inline int invert(const Real U[9], Real prim[9], Real g,
   if ((rho0 <= 0.) || (uu <= 0.)) return 5;
   prim[RHO] = rho0;
   prim[ENY] = uu;
-  prim[ENT] = (g - 1.) * uu * std::pow(rho0, -g);
+  prim[ENT] = (g - 1.) * uu * pgm::pow(rho0, -g);
   harm_velocity(s, Gamma, W, prim);
   prim[BX1] = U[BX1];
   prim[BX2] = U[BX2];
@@ -828,7 +836,7 @@ inline int invert(const Real U[9], Real prim[9], Real g,
   const Real uvsq = 1. + utsq;
   Real Gamma = std::sqrt(uvsq);
   Real rho0 = s.D / Gamma;
-  Real p = (K * std::pow(rho0, g));
+  Real p = (K * pgm::pow(rho0, g));
   Real uu = (p / (g - 1.));
   Real w = rho0 + uu + p;
   Real W_last = w * uvsq;
@@ -851,12 +859,12 @@ inline int invert(const Real U[9], Real prim[9], Real g,
   Gamma = 1. / gtmp;
   rho0 = s.D * gtmp;
   w = W * (1. - vsq);
-  p = (K * std::pow(rho0, g));
+  p = (K * pgm::pow(rho0, g));
   uu = (p / (g - 1.));
   if ((rho0 <= 0.) || (uu <= 0.)) return 5;
   prim[RHO] = rho0;
   prim[ENY] = uu;
-  prim[ENT] = (g - 1.) * uu * std::pow(rho0, -g);
+  prim[ENT] = (g - 1.) * uu * pgm::pow(rho0, -g);
   harm_velocity(s, Gamma, W, prim);
   prim[BX1] = U[BX1];
   prim[BX2] = U[BX2];
@@ -998,7 +1006,7 @@ inline int invert(const Real U[9], Real prim[9], Real g,
   const Real Wmu_x = lorentz * mu * x;
   prim[RHO] = rho;
   prim[ENY] = eps;
-  prim[ENT] = (g - 1.) * eps * std::pow(rho, -g);
+  prim[ENT] = (g - 1.) * eps * pgm::pow(rho, -g);
   for (int d = 0; d < 3; ++d) prim[UX1 + d] = Wmu_x * (r_u[d] + rb * mu * b_u[d]);
   prim[BX1] = U[BX1];
   prim[BX2] = U[BX2];
@@ -1026,7 +1034,7 @@ inline Real heating_fraction(const HeatParams &p, const HeatCell &c) {
   constexpr Real kElectronMass = 9.1093826e-28;
   constexpr Real kProtonMass = 1.67262171e-24;
   const Real tpr = (p.gamma_p - 1.0) * c.energy / c.rho;
-  const Real tel = c.adv_electron * std::pow(c.rho, p.gamma_e - 1.0);
+  const Real tel = c.adv_electron * pgm::pow(c.rho, p.gamma_e - 1.0);
   switch (p.model) {
     case 0:
       return p.fel_constant;
@@ -1034,13 +1042,13 @@ inline Real heating_fraction(const HeatParams &p, const HeatCell &c) {
       const Real trat = tpr / tel;
       const Real pres = c.rho * tpr;
       const Real beta = kmin(2.0 * pres / c.bsq, 1.0e20);
-      const Real log_trat = std::log(trat) / std::log(10.0);
+      const Real log_trat = pgm::log(trat) / pgm::log(10.0);
       const Real mbeta = 2.0 - 0.2 * log_trat;
       const Real c2 = (trat <= 1.0) ? 1.6 / trat : 1.2 / trat;
       const Real c3 = (trat <= 1.0) ? 18.0 + 5.0 * log_trat : 18.0;
-      const Real beta_pow = std::pow(beta, mbeta);
+      const Real beta_pow = pgm::pow(beta, mbeta);
       const Real qrat = 0.92 * (c2 * c2 + beta_pow) / (c3 * c3 + beta_pow) *
-                        std::exp(-1.0 / beta) *
+                        pgm::exp(-1.0 / beta) *
                         std::sqrt(kProtonMass / kElectronMass * trat);
       return 1.0 / (1.0 + qrat);
     }
@@ -1049,7 +1057,7 @@ inline Real heating_fraction(const HeatParams &p, const HeatCell &c) {
       const Real pres = c.rho * tpr;
       const Real beta = kmin(2.0 * pres / c.bsq, 1.0e20);
       const Real qi_qe =
-          35.0 / (1.0 + std::pow(beta / 15.0, -1.4) * std::exp(-0.1 / trat));
+          35.0 / (1.0 + pgm::pow(beta / 15.0, -1.4) * pgm::exp(-0.1 / trat));
       return 1.0 / (1.0 + qi_qe);
     }
     case 3: {
@@ -1062,8 +1070,8 @@ inline Real heating_fraction(const HeatParams &p, const HeatCell &c) {
       const Real beta = 2.0 * pres / c.bsq;
       const Real sigma = c.bsq / (c.rho + c.energy + pg);
       const Real betamax = 0.25 / sigma;
-      return 0.5 * std::exp(-std::pow(1.0 - beta / betamax, 3.3) /
-                            (1.0 + 1.2 * std::pow(sigma, 0.7)));
+      return 0.5 * pgm::exp(-pgm::pow(1.0 - beta / betamax, 3.3) /
+                            (1.0 + 1.2 * pgm::pow(sigma, 0.7)));
     }
     case 5: {
       const Real trat_inv = tel / tpr;
@@ -1078,17 +1086,17 @@ inline Real heating_fraction(const HeatParams &p, const HeatCell &c) {
 inline Real heating_apply(const HeatParams &p, const HeatCell &c) {
   const Real fel = heating_fraction(p, c);
   Real diss = (p.gamma_e - 1.0) / (p.gamma - 1.0) *
-              std::pow(c.rho, p.gamma - p.gamma_e) * (c.rec_total - c.adv_total);
+              pgm::pow(c.rho, p.gamma - p.gamma_e) * (c.rec_total - c.adv_total);
   if (p.suppress_highb_heat && (c.bsq / c.rho > 1.0)) diss = 0.0;
   if (p.enforce_positive_dissipation) diss = kmax(diss, 0.0);
   Real kel = c.adv_electron + fel * diss;
   if (!p.limit_kel && p.model == 0) return kel;
   const Real kel_max =
-      c.adv_total * std::pow(c.rho, p.gamma - p.gamma_e) /
+      c.adv_total * pgm::pow(c.rho, p.gamma - p.gamma_e) /
       (p.ratio_min * (p.gamma - 1.0) / (p.gamma_p - 1.0) +
        (p.gamma - 1.0) / (p.gamma_e - 1.0));
   const Real kel_min =
-      c.adv_total * std::pow(c.rho, p.gamma - p.gamma_e) /
+      c.adv_total * pgm::pow(c.rho, p.gamma - p.gamma_e) /
       (p.ratio_max * (p.gamma - 1.0) / (p.gamma_p - 1.0) +
        (p.gamma - 1.0) / (p.gamma_e - 1.0));
   return clip(kel, kel_min, kel_max);

@@ -1,0 +1,1266 @@
+// engine.cu -- B200 GRMHD stage engine: per-task kernels, the stage sequence
+// and the C ABI of include/pangu_b200.h.
+//
+// Data stay where Parthenon would keep them: caller-owned FP64 arrays in
+// [block][var][k][j][i] order. Every kernel maps consecutive threads to
+// consecutive i so that loads and stores are coalesced in every sweep
+// direction (the reference's X2/X3 loops put a strided index innermost,
+// laxf.cc:185-189, 291-295).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "pangu_b200.h"
+#include "pangu_device.cuh"
+
+using namespace pgd;
+
+namespace pgh {
+struct Layout {
+  int N[3], st[3], nx[3], act[3], nb[3], NB, ng, NF;
+  double dx[3];
+  std::vector<double> origin;
+};
+Layout make_layout(const pangu_params &p, const pangu_mesh &m);
+void build_tables(const pangu_params &p, const Layout &L, std::vector<double> &t1,
+                  std::vector<double> &t2);
+void build_exchange(const pangu_mesh &m, const Layout &L, std::vector<int64_t> &dst,
+                    std::vector<int64_t> &src);
+}  // namespace pgh
+
+// ---------------------------------------------------------------------------
+// geometry passed to every kernel by value
+// ---------------------------------------------------------------------------
+struct Dims {
+  int N1, N2, N3, NF, NB;
+  int is, ie, js, je, ks, ke;
+  int o1, o2, o3, ndim;
+  long long ncell;  // N1 * N2 * N3
+  int pidx[NPRIM];  // pack index of each slot, -1 if absent
+  double dx[3];
+  const double *t1;      // [NB][10][N1 + 1]
+  const double *t2;      // [NB][12][N2 + 1]
+  const double *origin;  // [NB][3]
+};
+
+struct pangu_engine {
+  pangu_params p;
+  pangu_mesh m;
+  Dims d;
+  double *d_t1 = nullptr, *d_t2 = nullptr, *d_origin = nullptr;
+  long long *d_xdst = nullptr, *d_xsrc = nullptr;
+  long long nxch = 0;
+  unsigned long long *d_cnt = nullptr;
+  int *d_fail_count = nullptr;
+  long long *d_fail_list = nullptr;
+  double *d_fail_vals = nullptr;
+  long long fail_cap = 0;
+  unsigned long long *d_dtmin = nullptr;
+};
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kT1Rows = 10;  // rows of the x1 table (host_tables.cc)
+
+__device__ __forceinline__ long long vidx(const Dims &d, int b, int v, int k, int j, int i) {
+  return (((long long)b * d.NF + v) * d.N3 + k) * (long long)d.N2 * d.N1 + (long long)j * d.N1 + i;
+}
+__device__ __forceinline__ long long cidx(const Dims &d, int b, int k, int j, int i) {
+  return ((long long)b * d.N3 + k) * (long long)d.N2 * d.N1 + (long long)j * d.N1 + i;
+}
+__device__ __forceinline__ long long aidx(const Dims &d, int b, int c, int k, int j, int i) {
+  return (((long long)b * 3 + c) * d.N3 + k) * (long long)d.N2 * d.N1 + (long long)j * d.N1 + i;
+}
+
+__device__ __forceinline__ void load_prim(const Dims &d, const double *P, int b, int k, int j,
+                                          int i, double out[NPRIM]) {
+#pragma unroll
+  for (int s = 0; s < NPRIM; ++s) out[s] = d.pidx[s] >= 0 ? P[vidx(d, b, d.pidx[s], k, j, i)] : 0.0;
+}
+
+// Cell-centre coordinate (origin + (idx + 1/2) dx, rounded step by step).
+__device__ __forceinline__ double xc(const Dims &d, int b, int dir, int idx) {
+  return ADD(d.origin[3 * b + dir], MUL((double)idx + 0.5, d.dx[dir]));
+}
+__device__ __forceinline__ double xf(const Dims &d, int b, int dir, int idx) {
+  return ADD(d.origin[3 * b + dir], MUL((double)idx, d.dx[dir]));
+}
+
+// Map point of the x1/x2 tables: q1/q2 select centre (0), +delta (1),
+// -delta (2) or face (3).
+__device__ __forceinline__ MapPt map_pt(const Dims &d, int b, int i, int q1, int j, int q2) {
+  const int W1 = d.N1 + 1, W2 = d.N2 + 1;
+  const double *T1 = d.t1 + (long long)b * kT1Rows * W1;
+  const double *T2 = d.t2 + (long long)b * 12 * W2;
+  MapPt m;
+  m.r = T1[(2 * q1) * W1 + i];
+  m.J1 = T1[(2 * q1 + 1) * W1 + i];
+  m.sth = T2[(3 * q2) * W2 + j];
+  m.cth = T2[(3 * q2 + 1) * W2 + j];
+  m.J2 = T2[(3 * q2 + 2) * W2 + j];
+  return m;
+}
+
+// Covariant code metric at a point given by table selectors (MKS/BL) or
+// coordinates (CKS).
+template <int MT>
+__device__ __forceinline__ void gcov_at(const Dims &d, const pangu_params &p, int b, int i, int q1,
+                                        int j, int q2, const double x[4], double g[4][4]) {
+  if (MT == MKS) {
+    ks_code_gcov(map_pt(d, b, i, q1, j, q2), p.a, g);
+  } else if (MT == BL) {
+    bl_code_gcov(map_pt(d, b, i, q1, j, q2), p.a, g);
+  } else if (MT == CKS) {
+    cks_code_gcov(x[1], x[2], x[3], p.a, g);
+  } else {
+    minkowski_gcov(g);
+  }
+}
+
+// ComputeMetricAtLocation (christoffel.h:53-62) at cell centre (b, k, j, i).
+// Returns 0 if the metric is singular.
+template <int MT>
+__device__ __forceinline__ int cell_metric(const Dims &d, const pangu_params &p, int b, int k,
+                                           int j, int i, Geo &g) {
+  double x[4] = {0.0, 0.0, 0.0, 0.0};
+  if (MT == CKS) {
+    x[1] = xc(d, b, 0, i);
+    x[2] = xc(d, b, 1, j);
+    x[3] = xc(d, b, 2, k);
+  }
+  gcov_at<MT>(d, p, b, i, 0, j, 0, x, g.gcov);
+  const int ok = gj_invert(g.gcov, g.gcon);
+  g.gdet = determinant(g.gcov);
+  return ok;
+}
+
+// Metric at the lower face of (b, k, j, i) along dir (1..3).
+template <int MT>
+__device__ __forceinline__ int face_metric(const Dims &d, const pangu_params &p, int dir, int b,
+                                           int k, int j, int i, Geo &g) {
+  double x[4] = {0.0, 0.0, 0.0, 0.0};
+  if (MT == CKS) {
+    x[1] = dir == 1 ? xf(d, b, 0, i) : xc(d, b, 0, i);
+    x[2] = dir == 2 ? xf(d, b, 1, j) : xc(d, b, 1, j);
+    x[3] = dir == 3 ? xf(d, b, 2, k) : xc(d, b, 2, k);
+  }
+  gcov_at<MT>(d, p, b, i, dir == 1 ? 3 : 0, j, dir == 2 ? 3 : 0, x, g.gcov);
+  const int ok = gj_invert(g.gcov, g.gcon);
+  g.gdet = determinant(g.gcov);
+  return ok;
+}
+
+// Warp-aggregated increment of a hit counter.
+__device__ __forceinline__ void count(unsigned long long *cnt, int which, bool pred) {
+  const unsigned mask = __activemask();
+  const unsigned hits = __ballot_sync(mask, pred);
+  if (hits && (threadIdx.x & 31) == (__ffs(mask) - 1)) atomicAdd(&cnt[which], (unsigned long long)__popc(hits));
+}
+
+// Decomposes a flat index over the box [k0,k1] x [j0,j1] x [i0,i1] of every
+// block. Returns false past the end.
+__device__ __forceinline__ bool box_index(long long t, int NB, int k0, int k1, int j0, int j1,
+                                          int i0, int i1, int &b, int &k, int &j, int &i) {
+  const long long ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
+  if (ni <= 0 || nj <= 0 || nk <= 0) return false;
+  const long long per = ni * nj * nk;
+  if (t >= per * NB) return false;
+  b = (int)(t / per);
+  long long r = t - (long long)b * per;
+  k = k0 + (int)(r / (ni * nj));
+  r -= (long long)(k - k0) * ni * nj;
+  j = j0 + (int)(r / ni);
+  i = i0 + (int)(r - (long long)(j - j0) * ni);
+  return true;
+}
+
+inline unsigned grid_for(long long n) {
+  const long long g = (n + kThreads - 1) / kThreads;
+  return (unsigned)std::max<long long>(1, std::min<long long>(g, 0x7fffffffLL));
+}
+
+// ---------------------------------------------------------------------------
+// FixPrimitive (primitive_fixer.cc:15-169), entire domain.
+// ---------------------------------------------------------------------------
+template <int MT>
+__global__ void __launch_bounds__(kThreads) k_fix_primitive(Dims d, pangu_params p, double *P,
+                                                            unsigned long long *cnt) {
+  int b, k, j, i;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (!box_index(t, d.NB, 0, d.N3 - 1, 0, d.N2 - 1, 0, d.N1 - 1, b, k, j, i)) return;
+  const double gam = p.adiabatic_index;
+  constexpr double small = 1.0e-20;
+  const double sigma_max_safe = kmax(p.sigma_max, small);
+  const long long q = vidx(d, b, 0, k, j, i);
+  const long long vs = d.ncell;
+  const double rho_before = kmax(P[q], small);
+  double r = 1.0;
+  double rho_floor, eng_floor;
+  if (MT == MKS) {
+    // r = exp(Xc1) and the radial floor profiles, from the host tables
+    const double *T1 = d.t1 + (long long)b * kT1Rows * (d.N1 + 1);
+    r = T1[i];
+    rho_floor = T1[8 * (d.N1 + 1) + i];
+    eng_floor = T1[9 * (d.N1 + 1) + i];
+  } else if (MT == CKS) {
+    const double x = xc(d, b, 0, i), y = xc(d, b, 1, j), z = xc(d, b, 2, k);
+    const double a2 = p.a * p.a;
+    const double rad2 = x * x + y * y + z * z;
+    const double sa = (rad2 - a2) * (rad2 - a2) + 4.0 * a2 * z * z;
+    r = sqrt(0.5 * (rad2 - a2 + sqrt(sa)));
+    rho_floor = p.density_floor * pgm::pow(fmax(r, 1.0), p.density_floor_pow);
+    eng_floor = p.energy_floor * pgm::pow(fmax(r, 1.0), p.energy_floor_pow);
+  } else {
+    rho_floor = p.density_floor;  // pgm::pow(max(1, 1), q) == 1
+    eng_floor = p.energy_floor;
+  }
+  Geo g;
+  cell_metric<MT>(d, p, b, k, j, i, g);
+  double pc[NPRIM];
+  load_prim(d, P, b, k, j, i, pc);
+  const double rho = pc[RHO], ug = pc[ENY];
+  State st;
+  calc_state(pc, g, st);
+  if (rho_floor < ug / sigma_max_safe) rho_floor = ug / sigma_max_safe;
+  const double sigma = st.bsq / rho;
+  if (sigma > p.sigma_max) rho_floor = st.bsq / sigma_max_safe;
+  double pr = pc[RHO], pu = pc[ENY];
+  const bool hit_r = pr < rho_floor;
+  if (hit_r) pr = rho_floor;
+  const bool hit_u = pu < eng_floor;
+  if (hit_u) pu = eng_floor;
+  double u1 = pc[UX1], u2 = pc[UX2], u3 = pc[UX3];
+  const double umax2 = p.lorentz_max * p.lorentz_max - 1.0;
+  const double uvsq = g.gcov[1][1] * u1 * u1 + g.gcov[2][2] * u2 * u2 + g.gcov[3][3] * u3 * u3 +
+                      2.0 * (g.gcov[1][2] * u1 * u2 + g.gcov[1][3] * u1 * u3 + g.gcov[2][3] * u2 * u3);
+  const bool cap = umax2 > 0.0 && uvsq > umax2;
+  if (cap) {
+    const double f = sqrt(umax2 / kmax(uvsq, small));
+    u1 *= f;
+    u2 *= f;
+    u3 *= f;
+  }
+  const double rho_after = kmax(pr, small);
+  double kel = pc[KEL];
+  if (p.enable_heating && rho_after != rho_before) kel *= pgm::pow(rho_after / rho_before, -gam);
+  double ent = (gam - 1.0) * pu * pgm::pow(pr, -gam);
+  if (p.enable_heating) kel = clamp_by_ratio(p.ratio_min, p.ratio_max, ent, kel);
+  if (MT == CKS && r < p.r_excise) {
+    const double e_excise = p.pexcise / (gam - 1.0);
+    pr = p.dexcise;
+    pu = e_excise;
+    u1 = u2 = u3 = 0.0;
+    ent = (gam - 1.0) * e_excise * pgm::pow(p.dexcise, -gam);
+    if (p.enable_heating) kel = e_excise;
+  }
+  P[q] = pr;
+  P[q + vs] = pu;
+  P[q + 2 * vs] = u1;
+  P[q + 3 * vs] = u2;
+  P[q + 4 * vs] = u3;
+  P[q + d.pidx[ENT] * vs] = ent;
+  if (p.enable_heating) P[q + d.pidx[KEL] * vs] = kel;
+  count(cnt, PANGU_CNT_RHO_FLOOR, hit_r);
+  count(cnt, PANGU_CNT_ENG_FLOOR, hit_u);
+  count(cnt, PANGU_CNT_LORENTZ_CAP, cap);
+}
+
+// ---------------------------------------------------------------------------
+// CalculateConservative (conservative.cc:15-110), interior.
+// ---------------------------------------------------------------------------
+template <int MT>
+__global__ void __launch_bounds__(kThreads) k_calc_cons(Dims d, pangu_params p, const double *P,
+                                                        double *U) {
+  int b, k, j, i;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
+  Geo g;
+  cell_metric<MT>(d, p, b, k, j, i, g);
+  double pc[NPRIM];
+  load_prim(d, P, b, k, j, i, pc);
+  State s;
+  calc_state(pc, g, s);
+  double f[NPRIM];
+  flux_from_state(p.adiabatic_index, pc, s, sqrt(fabs(g.gdet)), 0, f);
+#pragma unroll
+  for (int v = 0; v < NPRIM; ++v)
+    if (d.pidx[v] >= 0) U[vidx(d, b, d.pidx[v], k, j, i)] = f[v];
+}
+
+// ---------------------------------------------------------------------------
+// CalculateLAXF / CalculateHLL, one direction (laxf.cc:78-181 and twins).
+// ---------------------------------------------------------------------------
+template <int MT, int dir>
+__device__ __forceinline__ void k_flux_body(Dims d, pangu_params p, int k0, int k1,
+                                                   int j0, int j1, int i0, int i1, const double *P,
+                                                   double *F, double *alfven) {
+  int b, k, j, i;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (!box_index(t, d.NB, k0, k1, j0, j1, i0, i1, b, k, j, i)) return;
+  const int di = dir == 1, dj = dir == 2, dk = dir == 3;
+  const long long step = (long long)di + (long long)dj * d.N1 + (long long)dk * d.N1 * d.N2;
+  const bool use_mc = p.limiter == PANGU_LIMITER_MC;
+  double PL[NPRIM], PR[NPRIM];
+#pragma unroll
+  for (int s = 0; s < NPRIM; ++s) {
+    PL[s] = 0.0;
+    PR[s] = 0.0;
+    if (d.pidx[s] < 0) continue;
+    const double *q = P + vidx(d, b, d.pidx[s], k, j, i);
+    double dummy;
+    if (use_mc) {
+      const double qm2 = q[-2 * step], qm1 = q[-step], q0 = q[0], qp1 = q[step];
+      mc(qm2, qm1, q0, PL[s], dummy);
+      mc(qm1, q0, qp1, dummy, PR[s]);
+    } else {
+      const double qm3 = q[-3 * step], qm2 = q[-2 * step], qm1 = q[-step], q0 = q[0],
+                   qp1 = q[step], qp2 = q[2 * step];
+      ppm4(qm3, qm2, qm1, q0, qp1, PL[s], dummy);
+      ppm4(qm2, qm1, q0, qp1, qp2, dummy, PR[s]);
+    }
+  }
+  Geo g;
+  const long long fo = vidx(d, b, 0, k, j, i);
+  if (!face_metric<MT>(d, p, dir, b, k, j, i, g)) {
+    // Singular code metric (theta = 0 exactly on a polar face): zero flux,
+    // zero speed (the reference reads an unwritten inverse here).
+    alfven[aidx(d, b, dir - 1, k, j, i)] = 0.0;
+#pragma unroll
+    for (int s = 0; s < NPRIM; ++s)
+      if (d.pidx[s] >= 0) F[fo + d.pidx[s] * d.ncell] = 0.0;
+    return;
+  }
+  const double gam = p.adiabatic_index;
+  const double sg = sqrt(fabs(g.gdet));
+  State sL, sR;
+  calc_state(PL, g, sL);
+  calc_state(PR, g, sR);
+  double vmaxL, vminL, vmaxR, vminR;
+  fast_speed_from_state(gam, PL, g, sL, dir, vmaxL, vminL);
+  fast_speed_from_state(gam, PR, g, sR, dir, vmaxR, vminR);
+  const double cmax = fabs(kmax(kmax(0., vmaxL), vmaxR));
+  const double cmin = fabs(kmax(kmax(0., -vminL), -vminR));
+  const double cms = kmax(cmax, cmin);
+  alfven[aidx(d, b, dir - 1, k, j, i)] = cms;
+  double UL[NPRIM], UR[NPRIM], FL[NPRIM], FR[NPRIM];
+  flux_from_state(gam, PL, sL, sg, 0, UL);
+  flux_from_state(gam, PR, sR, sg, 0, UR);
+  flux_from_state(gam, PL, sL, sg, dir, FL);
+  flux_from_state(gam, PR, sR, sg, dir, FR);
+  const bool hll = p.riemann_solver == PANGU_RIEMANN_HLL;
+#pragma unroll
+  for (int s = 0; s < NPRIM; ++s) {
+    if (d.pidx[s] < 0) continue;
+    double fx;
+    if (hll)
+      fx = (cmax * FL[s] + cmin * FR[s] - cmax * cmin * (UR[s] - UL[s])) / (cmax + cmin + 1e-20);
+    else
+      fx = 0.5 * (FL[s] + FR[s] - cms * (UR[s] - UL[s]));
+    F[fo + d.pidx[s] * d.ncell] = fx;
+  }
+}
+
+// Direction-specialised entry points (the direction indexes register arrays).
+#define PGD_FLUX_DIR(NAME, DIR)                                                              \
+  template <int MT>                                                                          \
+  __global__ void __launch_bounds__(kThreads)                                                \
+      NAME(Dims d, pangu_params p, int k0, int k1, int j0, int j1, int i0, int i1,            \
+           const double *P, double *F, double *alfven) {                                     \
+    k_flux_body<MT, DIR>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);                        \
+  }
+PGD_FLUX_DIR(k_flux1, 1)
+PGD_FLUX_DIR(k_flux2, 2)
+PGD_FLUX_DIR(k_flux3, 3)
+#undef PGD_FLUX_DIR
+
+// ---------------------------------------------------------------------------
+// ConstraintedTransport (constrained_transport.cc:13-130).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_ct_emf(Dims d, const double *F1, const double *F2,
+                                                     const double *F3, double *E) {
+  int b, k, j, i;
+  const int o1 = d.N1 > 1, o2 = d.N2 > 1, o3 = d.N3 > 1;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (!box_index(t, d.NB, d.ks, d.ke + o3, d.js, d.je + o2, d.is, d.ie + o1, b, k, j, i)) return;
+  const long long sj = d.N1, sk = (long long)d.N1 * d.N2;
+  double e1 = 0.0, e2 = 0.0, e3 = 0.0;
+  if (o2 && o3) {
+    const long long a = vidx(d, b, BX3, k, j, i), c = vidx(d, b, BX2, k, j, i);
+    e1 = 0.25 * ((F2[a] + F2[a - sk]) - (F3[c] + F3[c - sj]));
+  }
+  if (o3 && o1) {
+    const long long a = vidx(d, b, BX1, k, j, i), c = vidx(d, b, BX3, k, j, i);
+    e2 = 0.25 * ((F3[a] + F3[a - 1]) - (F1[c] + F1[c - sk]));
+  }
+  if (o1 && o2) {
+    const long long a = vidx(d, b, BX2, k, j, i), c = vidx(d, b, BX1, k, j, i);
+    e3 = 0.25 * ((F1[a] + F1[a - sj]) - (F2[c] + F2[c - 1]));
+  }
+  E[aidx(d, b, 0, k, j, i)] = e1;
+  E[aidx(d, b, 1, k, j, i)] = e2;
+  E[aidx(d, b, 2, k, j, i)] = e3;
+}
+
+// Face-B overwrite of direction dir (constrained_transport.cc:78-127).
+__global__ void __launch_bounds__(kThreads) k_ct_faces(Dims d, int dir, double *F,
+                                                       const double *E) {
+  int b, k, j, i;
+  const int o1 = d.N1 > 1, o2 = d.N2 > 1, o3 = d.N3 > 1;
+  const int E1 = o2 && o3, E2 = o3 && o1, E3 = o1 && o2;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int ei = dir == 1 ? o1 : 0, ej = dir == 2 ? o2 : 0, ek = dir == 3 ? o3 : 0;
+  if (!box_index(t, d.NB, d.ks, d.ke + ek, d.js, d.je + ej, d.is, d.ie + ei, b, k, j, i)) return;
+  const long long sj = d.N1, sk = (long long)d.N1 * d.N2;
+  const long long e0 = aidx(d, b, 0, k, j, i), e1 = aidx(d, b, 1, k, j, i),
+                  e2 = aidx(d, b, 2, k, j, i);
+  if (dir == 1) {
+    if (o1) F[vidx(d, b, BX1, k, j, i)] = 0;
+    if (E2) F[vidx(d, b, BX3, k, j, i)] = -0.5 * (E[e1] + E[e1 + sk]);
+    if (E3) F[vidx(d, b, BX2, k, j, i)] = 0.5 * (E[e2] + E[e2 + sj]);
+  } else if (dir == 2) {
+    if (E1) F[vidx(d, b, BX3, k, j, i)] = 0.5 * (E[e0] + E[e0 + sk]);
+    if (o2) F[vidx(d, b, BX2, k, j, i)] = 0.;
+    if (E3) F[vidx(d, b, BX1, k, j, i)] = -0.5 * (E[e2] + E[e2 + 1]);
+  } else {
+    if (E1) F[vidx(d, b, BX2, k, j, i)] = -0.5 * (E[e0] + E[e0 + sj]);
+    if (E2) F[vidx(d, b, BX1, k, j, i)] = 0.5 * (E[e1] + E[e1 + 1]);
+    if (o3) F[vidx(d, b, BX3, k, j, i)] = 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FluxDivergence + UpdateIndependentData, interior (ideal_grmhd.cc:73-76).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_flux_div_update(Dims d, const double *F1,
+                                                              const double *F2, const double *F3,
+                                                              const double *Uinit, double *Uout,
+                                                              double beta, const double *dt) {
+  int b, k, j, i;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (!box_index(t, d.NB * d.NF, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
+  // b here runs over (block, variable) pairs; vidx with NF=1 view.
+  const long long q = ((long long)b * d.N3 + k) * (long long)d.N2 * d.N1 + (long long)j * d.N1 + i;
+  const double A1 = MUL(d.dx[1], d.dx[2]), A2 = MUL(d.dx[0], d.dx[2]), A3 = MUL(d.dx[0], d.dx[1]);
+  const double V = MUL(MUL(d.dx[0], d.dx[1]), d.dx[2]);
+  double du = SUB(MUL(A1, F1[q + 1]), MUL(A1, F1[q]));
+  if (d.ndim >= 2) du = ADD(du, SUB(MUL(A2, F2[q + d.N1]), MUL(A2, F2[q])));
+  if (d.ndim == 3) {
+    const long long sk = (long long)d.N1 * d.N2;
+    du = ADD(du, SUB(MUL(A3, F3[q + sk]), MUL(A3, F3[q])));
+  }
+  const double dudt = DIV(-du, V);
+  const double bdt = MUL(beta, *dt);
+  Uout[q] = ADD(Uinit[q], MUL(bdt, dudt));
+}
+
+// ---------------------------------------------------------------------------
+// Ghost exchange: ghost <- neighbour interior, prim and flag.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_exchange(Dims d, long long n, const long long *dst,
+                                                       const long long *src, double *P,
+                                                       double *flag) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const long long dc = dst[t], sc = src[t];
+  const long long db = dc / d.ncell, sb = sc / d.ncell;
+  const long long dp = db * d.NF * d.ncell + (dc - db * d.ncell);
+  const long long sp = sb * d.NF * d.ncell + (sc - sb * d.ncell);
+  for (int v = 0; v < d.NF; ++v) P[dp + v * d.ncell] = P[sp + v * d.ncell];
+  if (flag) flag[dc] = flag[sc];
+}
+
+// ---------------------------------------------------------------------------
+// AddGeometricSource (source_term.cc:15-121): Christoffel symbols by central
+// differences of the code metric (christoffel.h:74-148), rounded step by
+// step like the metric itself.
+// ---------------------------------------------------------------------------
+template <int MT>
+__device__ __forceinline__ void christoffel(const Dims &d, const pangu_params &p, int b, int k,
+                                            int j, int i, const Geo &g, double conn[4][4][4]) {
+  constexpr double twod = 2.0 * 1.0e-5;
+  double dg[4][4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) dg[a][r][c] = 0.0;
+  double x[4] = {0.0, 0.0, 0.0, 0.0};
+  if (MT == CKS) {
+    x[1] = xc(d, b, 0, i);
+    x[2] = xc(d, b, 1, j);
+    x[3] = xc(d, b, 2, k);
+  }
+#pragma unroll
+  for (int dir = 1; dir < 4; ++dir) {
+    if ((MT == MKS || MT == BL) && dir == 3) continue;  // metric independent of x3: exactly 0
+    double gp[4][4], gm[4][4];
+    double xp[4] = {x[0], x[1], x[2], x[3]}, xm[4] = {x[0], x[1], x[2], x[3]};
+    xp[dir] = ADD(xp[dir], 1.0e-5);
+    xm[dir] = SUB(xm[dir], 1.0e-5);
+    gcov_at<MT>(d, p, b, i, dir == 1 ? 1 : 0, j, dir == 2 ? 1 : 0, xp, gp);
+    gcov_at<MT>(d, p, b, i, dir == 1 ? 2 : 0, j, dir == 2 ? 2 : 0, xm, gm);
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) dg[dir][r][c] = DIV(SUB(gp[r][c], gm[r][c]), twod);
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) {
+        double v = 0.0;
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+          const double cc = MUL(0.5, SUB(ADD(dg[jj][l][kk], dg[kk][l][jj]), dg[l][jj][kk]));
+          v = ADD(v, MUL(g.gcon[a][l], cc));
+        }
+        conn[a][jj][kk] = v;
+      }
+}
+
+template <int MT>
+__global__ void __launch_bounds__(kThreads) k_source(Dims d, pangu_params p, const double *P,
+                                                     double *U, double beta, const double *dt) {
+  int b, k, j, i;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
+  if (MT == MINKOWSKI) return;  // connection identically zero (christoffel.h:90)
+  Geo g;
+  cell_metric<MT>(d, p, b, k, j, i, g);
+  const double sg = sqrt(fabs(g.gdet));
+  double conn[4][4][4];
+  christoffel<MT>(d, p, b, k, j, i, g, conn);
+  double pc[NPRIM];
+  load_prim(d, P, b, k, j, i, pc);
+  State s;
+  calc_state(pc, g, s);
+  double T[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) emt_from_state(p.adiabatic_index, pc, s, r, T[r]);
+  const double bdt = beta * (*dt);
+#pragma unroll
+  for (int dir = 0; dir < 4; ++dir) {
+    double con = 0.0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) con += T[r][c] * conn[c][dir][r];
+    const int v = dir == 0 ? d.pidx[ENY] : d.pidx[UX1] + dir - 1;
+    const long long q = vidx(d, b, v, k, j, i);
+    U[q] += con * sg * bdt;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Recovery (invertor.cc:18-210).
+// ---------------------------------------------------------------------------
+template <int MT>
+__global__ void __launch_bounds__(kThreads) k_recovery(Dims d, pangu_params p, double *P,
+                                                       const double *U, double *flag,
+                                                       unsigned long long *cnt) {
+  int b, k, j, i;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
+  const bool robuster = p.recovery == PANGU_RECOVERY_ROBUSTER;
+  const long long fc = cidx(d, b, k, j, i);
+  if (MT == CKS) {
+    const double x = xc(d, b, 0, i), y = xc(d, b, 1, j), z = xc(d, b, 2, k);
+    const double a2 = p.a * p.a;
+    const double rad2 = x * x + y * y + z * z;
+    const double sa = (rad2 - a2) * (rad2 - a2) + 4.0 * a2 * z * z;
+    const bool exc = sqrt(0.5 * (rad2 - a2 + sqrt(sa))) < p.r_excise;
+    count(cnt, PANGU_CNT_EXCISED, exc);
+    if (exc) {
+      if (!robuster) flag[fc] = 0;
+      return;
+    }
+  }
+  Geo g;
+  cell_metric<MT>(d, p, b, k, j, i, g);
+  if (!robuster) flag[fc] = 0;
+  const double sg = sqrt(fabs(g.gdet));
+  const double alpha = 1.0 / sqrt(-g.gcon[0][0]);
+  const long long q = vidx(d, b, 0, k, j, i);
+  const long long vs = d.ncell;
+  double C[9], Pp[9];
+#pragma unroll
+  for (int s = 0; s < 9; ++s) {
+    C[s] = d.pidx[s] >= 0 ? U[q + d.pidx[s] * vs] : 0.0;
+    Pp[s] = d.pidx[s] >= 0 ? P[q + d.pidx[s] * vs] : 0.0;
+  }
+  const double isg = 1.0 / sg;
+  const double aisg = alpha * isg;
+  if (p.enable_B) {
+    P[q + d.pidx[BX1] * vs] = C[BX1] * isg;
+    P[q + d.pidx[BX2] * vs] = C[BX2] * isg;
+    P[q + d.pidx[BX3] * vs] = C[BX3] * isg;
+  }
+  double UH[9], PH[9];
+  UH[RHO] = aisg * C[RHO];
+  UH[ENY] = aisg * (C[ENY] - C[RHO]);
+  UH[UX1] = aisg * C[UX1];
+  UH[UX2] = aisg * C[UX2];
+  UH[UX3] = aisg * C[UX3];
+  UH[BX1] = aisg * C[BX1];
+  UH[BX2] = aisg * C[BX2];
+  UH[BX3] = aisg * C[BX3];
+  UH[ENT] = aisg * C[ENT];
+#pragma unroll
+  for (int s = 0; s < 9; ++s) PH[s] = Pp[s];
+  const double gam = p.adiabatic_index;
+  if (robuster) {
+    const int st = invert_kastaun(UH, PH, gam, g);
+    count(cnt, PANGU_CNT_KASTAUN_FAIL, st != 0);
+    if (st != 0) return;
+  } else {
+    Harm hs;
+    harm_setup(UH, g, hs);
+    int ok = invert_2d(UH, PH, gam, g, hs) == 0;
+    count(cnt, PANGU_CNT_C2P_2D, ok);
+    if (!ok) {
+      ok = invert_1dvsq(UH, PH, gam, g, hs) == 0;
+      count(cnt, PANGU_CNT_C2P_1DVSQ, ok);
+      if (!ok) {
+        ok = invert_1d(UH, PH, gam, g, hs) == 0;
+        count(cnt, PANGU_CNT_C2P_1D, ok);
+        count(cnt, PANGU_CNT_C2P_FAIL, !ok);
+      }
+    }
+    flag[fc] = ok;
+  }
+  P[q] = PH[RHO];
+  P[q + vs] = PH[ENY];
+  P[q + 2 * vs] = PH[UX1];
+  P[q + 3 * vs] = PH[UX2];
+  P[q + 4 * vs] = PH[UX3];
+}
+
+// ---------------------------------------------------------------------------
+// ApplyElectronHeating (electron_heating.cc:14-112).
+// ---------------------------------------------------------------------------
+template <int MT>
+__global__ void __launch_bounds__(kThreads) k_heating(Dims d, pangu_params p, double *P,
+                                                      const double *U) {
+  int b, k, j, i;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
+  Geo g;
+  cell_metric<MT>(d, p, b, k, j, i, g);
+  double pc[NPRIM];
+  load_prim(d, P, b, k, j, i, pc);
+  State s;
+  calc_state(pc, g, s);
+  const long long q = vidx(d, b, 0, k, j, i);
+  const long long vs = d.ncell;
+  const double cr = U[q];
+  const HeatParams hp = {p.model, p.adiabatic_index, p.gamma_p, p.gamma_e, p.fel_constant,
+                         p.ratio_min, p.ratio_max, p.limit_kel, p.suppress_highb_heat,
+                         p.enforce_positive_dissipation};
+  P[q + d.pidx[KEL] * vs] = heating_apply(hp, pc[RHO], pc[ENY], s.bsq, U[q + d.pidx[ENT] * vs] / cr,
+                                          pc[ENT], U[q + d.pidx[KEL] * vs] / cr);
+}
+
+// ---------------------------------------------------------------------------
+// FixRecovery (recovery_fixer.cc:12-119), two phases over the failure list.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_fixrec_scan(Dims d, pangu_params p,
+                                                          const double *flag, int *count_out,
+                                                          long long *list) {
+  int b, k, j, i;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
+  const long long fc = cidx(d, b, k, j, i);
+  if (flag[fc] != 0) return;
+  if (p.metric_type == PANGU_METRIC_CKS) {
+    const double x = xc(d, b, 0, i), y = xc(d, b, 1, j), z = xc(d, b, 2, k);
+    const double a2 = p.a * p.a;
+    const double rad2 = x * x + y * y + z * z;
+    const double sa = (rad2 - a2) * (rad2 - a2) + 4.0 * a2 * z * z;
+    if (sqrt(0.5 * (rad2 - a2 + sqrt(sa))) < p.r_excise) return;
+  }
+  const int n = atomicAdd(count_out, 1);
+  list[n] = fc;
+}
+
+__global__ void __launch_bounds__(kThreads) k_fixrec_compute(Dims d, const int *count_in,
+                                                             const long long *list,
+                                                             const double *P, const double *flag,
+                                                             double *vals) {
+  const int n = *count_in;
+  const int off2 = d.js != d.je ? 1 : 0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long fc = list[t];
+    const long long b = fc / d.ncell;
+    const long long c = fc - b * d.ncell;
+    const long long sj = (long long)off2 * d.N1;
+    auto fl = [&](long long o) { return (int)flag[fc + o]; };
+    const int pf1 = fl(sj - 1), pf2 = fl(sj), pf3 = fl(sj + 1), pf4 = fl(1);
+    const int pf5 = fl(-sj + 1), pf6 = fl(-sj), pf7 = fl(-sj - 1), pf8 = fl(-1);
+    for (int v = 0; v < d.NF; ++v) {
+      const double *q = P + (b * d.NF + v) * d.ncell + c;
+      double val;
+      if (pf2 && pf4 && pf6 && pf8)
+        val = 0.25 * (q[sj] + q[-sj] + q[-1] + q[1]);
+      else if (pf1 && pf3 && pf5 && pf7)
+        val = 0.25 * (q[sj + 1] + q[sj - 1] + q[-sj + 1] + q[-sj - 1]);
+      else
+        val = 0.125 * (q[sj - 1] + q[sj] + q[sj + 1] + q[1] + q[-sj + 1] + q[-sj] + q[-sj - 1] +
+                       q[-1]);
+      vals[t * d.NF + v] = val;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_fixrec_write(Dims d, const int *count_in,
+                                                           const long long *list,
+                                                           const double *vals, double *P,
+                                                           double *flag,
+                                                           unsigned long long *cnt) {
+  const int n = *count_in;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long fc = list[t];
+    const long long b = fc / d.ncell;
+    const long long c = fc - b * d.ncell;
+    for (int v = 0; v < d.NF; ++v) P[(b * d.NF + v) * d.ncell + c] = vals[t * d.NF + v];
+    for (int v = 2; v < 5; ++v) P[(b * d.NF + v) * d.ncell + c] = 0.;
+    flag[fc] = 1;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&cnt[PANGU_CNT_FIXRECOVERY], (unsigned long long)n);
+}
+
+// ---------------------------------------------------------------------------
+// Physical boundary conditions on one face.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_bc_face(Dims d, int face, int kind, int b_sel_dim,
+                                                      int b_sel_val, int nbx1, int nbx2,
+                                                      int enable_B, double *P, double *flag) {
+  const int dir = face / 2, outer = face % 2;
+  int N[3] = {d.N1, d.N2, d.N3};
+  const int s[3] = {d.is, d.js, d.ks}, e[3] = {d.ie, d.je, d.ke};
+  const int ng = outer ? (N[dir] - 1 - e[dir]) : s[dir];
+  int ext[3] = {N[0], N[1], N[2]};
+  ext[dir] = ng;
+  const long long per = (long long)ext[0] * ext[1] * ext[2];
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= per * d.NB) return;
+  const int b = (int)(t / per);
+  const int bl[3] = {b % nbx1, (b / nbx1) % nbx2, b / (nbx1 * nbx2)};
+  if (bl[b_sel_dim] != b_sel_val) return;
+  long long r = t - (long long)b * per;
+  int idx[3];
+  idx[0] = (int)(r % ext[0]);
+  r /= ext[0];
+  idx[1] = (int)(r % ext[1]);
+  idx[2] = (int)(r / ext[1]);
+  idx[dir] = outer ? (e[dir] + 1 + idx[dir]) : idx[dir];
+  const int x = idx[dir];
+  int sidx[3] = {idx[0], idx[1], idx[2]};
+  if (kind == PANGU_BC_OUTFLOW) sidx[dir] = outer ? e[dir] : s[dir];
+  else sidx[dir] = outer ? (2 * e[dir] + 1 - x) : (2 * s[dir] - 1 - x);
+  const long long dc = cidx(d, b, idx[2], idx[1], idx[0]);
+  const long long sc = cidx(d, b, sidx[2], sidx[1], sidx[0]);
+  const long long base = (long long)b * d.NF * d.ncell - (long long)b * d.ncell;
+  for (int v = 0; v < d.NF; ++v) {
+    double val = P[base + sc + v * d.ncell];
+    if (kind == PANGU_BC_REFLECTING) {
+      const bool vel = v == d.pidx[UX1] + dir;
+      const bool mag = enable_B && v == d.pidx[BX1] + dir;
+      if (vel || mag) val = -val;
+    }
+    P[base + dc + v * d.ncell] = val;
+  }
+  if (flag) flag[dc] = flag[sc];
+}
+
+// ---------------------------------------------------------------------------
+// EstimateTimestepMesh (timestep_estimation.cc:13-102).
+// ---------------------------------------------------------------------------
+__global__ void k_dt_init(int n, unsigned long long *mins) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) mins[t] = (unsigned long long)__double_as_longlong(DBL_MAX);
+}
+
+// One CTA row per mesh block (blockIdx.y); warp and CTA minima, then one
+// atomic per CTA and direction. Positive doubles order like their bit
+// patterns; a NaN speed never lowers the minimum (the reference's
+// "if (dt_min > dt)" skips it as well).
+__global__ void __launch_bounds__(kThreads) k_dt_reduce(Dims d, double cfl,
+                                                        const double *alfven,
+                                                        unsigned long long *mins) {
+  __shared__ unsigned long long red[3][kThreads / 32];
+  const int b = blockIdx.y;
+  const int ni = d.ie - d.is + 1, nj = d.je - d.js + 1, nk = d.ke - d.ks + 1;
+  const long long per = (long long)ni * nj * nk;
+  const unsigned long long big = (unsigned long long)__double_as_longlong(DBL_MAX);
+  unsigned long long m[3] = {big, big, big};
+  const double cdx[3] = {MUL(cfl, d.dx[0]), MUL(cfl, d.dx[1]), MUL(cfl, d.dx[2])};
+  const int act[3] = {d.N1 > 1, d.N2 > 1, d.N3 > 1};
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < per;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int k = d.ks + (int)(t / ((long long)ni * nj));
+    const long long r = t - (long long)(k - d.ks) * ni * nj;
+    const int j = d.js + (int)(r / ni);
+    const int i = d.is + (int)(r - (long long)(j - d.js) * ni);
+#pragma unroll
+    for (int dir = 0; dir < 3; ++dir) {
+      if (!act[dir]) continue;
+      const double dt = cdx[dir] / alfven[aidx(d, b, dir, k, j, i)];
+      if (dt >= 0.0) {
+        const unsigned long long bits = (unsigned long long)__double_as_longlong(dt);
+        m[dir] = bits < m[dir] ? bits : m[dir];
+      }
+    }
+  }
+#pragma unroll
+  for (int dir = 0; dir < 3; ++dir) {
+    unsigned long long v = m[dir];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+      v = w < v ? w : v;
+    }
+    if ((threadIdx.x & 31) == 0) red[dir][threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int dir = threadIdx.x;
+    unsigned long long v = red[dir][0];
+    for (int w = 1; w < kThreads / 32; ++w) v = red[dir][w] < v ? red[dir][w] : v;
+    if (act[dir]) atomicMin(&mins[b * 3 + dir], v);
+  }
+}
+
+__global__ void k_dt_finalize(int NB, const unsigned long long *mins, double *dt_out) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  double gmin = DBL_MAX;
+  for (int b = 0; b < NB; ++b) {
+    const double m0 = __longlong_as_double((long long)mins[3 * b + 0]);
+    const double m1 = __longlong_as_double((long long)mins[3 * b + 1]);
+    const double m2 = __longlong_as_double((long long)mins[3 * b + 2]);
+    const double bdt = 1.0 / (1.0 / m0 + 1.0 / m1 + 1.0 / m2);
+    if (bdt < gmin) gmin = bdt;
+  }
+  *dt_out = gmin;
+}
+
+__global__ void k_update_dt(double *dt, const double *dt_est, double factor) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const double grown = factor * (*dt);
+    *dt = (*dt_est < grown) ? *dt_est : grown;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launch helpers
+// ---------------------------------------------------------------------------
+inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+inline int check_launch() {
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? PANGU_OK : PANGU_ECUDA;
+}
+
+inline long long box_count(int NB, int k0, int k1, int j0, int j1, int i0, int i1) {
+  if (k1 < k0 || j1 < j0 || i1 < i0) return 0;
+  return (long long)NB * (k1 - k0 + 1) * (j1 - j0 + 1) * (i1 - i0 + 1);
+}
+
+#define DISPATCH_MT(mt, KERNEL, grid, stream, ...)                          \
+  do {                                                                      \
+    switch (mt) {                                                           \
+      case PANGU_METRIC_MKS: KERNEL<MKS><<<grid, kThreads, 0, stream>>>(__VA_ARGS__); break; \
+      case PANGU_METRIC_BL: KERNEL<BL><<<grid, kThreads, 0, stream>>>(__VA_ARGS__); break;   \
+      case PANGU_METRIC_CKS: KERNEL<CKS><<<grid, kThreads, 0, stream>>>(__VA_ARGS__); break; \
+      default: KERNEL<MINKOWSKI><<<grid, kThreads, 0, stream>>>(__VA_ARGS__); break;         \
+    }                                                                       \
+  } while (0)
+
+bool pack_ok(const pangu_engine *e, const pangu_pack *md) {
+  if (!e || !md || !md->prim || !md->cons || !md->flux1 || !md->alfven || !md->efield) return false;
+  if (e->d.ndim >= 2 && !md->flux2) return false;
+  if (e->d.ndim == 3 && !md->flux3) return false;
+  if (e->p.recovery == PANGU_RECOVERY_CHAINER && !md->flag) return false;
+  return true;
+}
+
+int run_fix_primitive(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
+  const Dims &d = e->d;
+  const long long n = (long long)d.NB * d.ncell;
+  DISPATCH_MT(e->p.metric_type, k_fix_primitive, grid_for(n), s, d, e->p, md->prim, e->d_cnt);
+  return check_launch();
+}
+
+int run_calc_cons(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
+  const Dims &d = e->d;
+  const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
+  DISPATCH_MT(e->p.metric_type, k_calc_cons, grid_for(n), s, d, e->p, md->prim, md->cons);
+  return check_launch();
+}
+
+int run_fluxes(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
+  const Dims &d = e->d;
+  const bool hll = e->p.riemann_solver == PANGU_RIEMANN_HLL;
+  for (int dir = 1; dir <= d.ndim; ++dir) {
+    int k0 = d.ks - d.o3, k1 = d.ke + d.o3, j0 = d.js - d.o2, j1 = d.je + d.o2;
+    int i0 = d.is - d.o1, i1 = d.ie + d.o1;
+    if (dir == 1) { i0 = d.is; i1 = d.ie + 1; }
+    if (dir == 2) { j0 = d.js; j1 = d.je + 1; }
+    if (dir == 3) {  // hll.cc:293-296 narrows the transverse range
+      k0 = d.ks; k1 = d.ke + 1;
+      if (hll) { j0 = d.js; j1 = d.je; i0 = d.is; i1 = d.ie; }
+    }
+    double *F = dir == 1 ? md->flux1 : (dir == 2 ? md->flux2 : md->flux3);
+    const long long n = box_count(d.NB, k0, k1, j0, j1, i0, i1);
+    const unsigned g = grid_for(n);
+#define FLUX_ARGS d, e->p, k0, k1, j0, j1, i0, i1, md->prim, F, md->alfven
+    if (dir == 1) DISPATCH_MT(e->p.metric_type, k_flux1, g, s, FLUX_ARGS);
+    else if (dir == 2) DISPATCH_MT(e->p.metric_type, k_flux2, g, s, FLUX_ARGS);
+    else DISPATCH_MT(e->p.metric_type, k_flux3, g, s, FLUX_ARGS);
+#undef FLUX_ARGS
+    const int rc = check_launch();
+    if (rc) return rc;
+  }
+  return PANGU_OK;
+}
+
+int run_ct(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
+  const Dims &d = e->d;
+  const int o1 = d.N1 > 1, o2 = d.N2 > 1, o3 = d.N3 > 1;
+  k_ct_emf<<<grid_for(box_count(d.NB, d.ks, d.ke + o3, d.js, d.je + o2, d.is, d.ie + o1)),
+             kThreads, 0, s>>>(d, md->flux1, md->flux2, md->flux3, md->efield);
+  double *F[3] = {md->flux1, md->flux2, md->flux3};
+  for (int dir = 1; dir <= 3; ++dir) {
+    if (dir > 1 && !F[dir - 1]) continue;
+    const int ei = dir == 1 ? o1 : 0, ej = dir == 2 ? o2 : 0, ek = dir == 3 ? o3 : 0;
+    const long long n = box_count(d.NB, d.ks, d.ke + ek, d.js, d.je + ej, d.is, d.ie + ei);
+    k_ct_faces<<<grid_for(n), kThreads, 0, s>>>(d, dir, F[dir - 1], md->efield);
+  }
+  return check_launch();
+}
+
+int run_update(pangu_engine *e, const pangu_pack *mi, const pangu_pack *m0, const pangu_pack *m1,
+               double beta, const double *dt, cudaStream_t s) {
+  const Dims &d = e->d;
+  const long long n = box_count(d.NB * d.NF, d.ks, d.ke, d.js, d.je, d.is, d.ie);
+  k_flux_div_update<<<grid_for(n), kThreads, 0, s>>>(d, m0->flux1, m0->flux2, m0->flux3,
+                                                     mi->cons, m1->cons, beta, dt);
+  return check_launch();
+}
+
+int run_exchange(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
+  if (e->nxch == 0) return PANGU_OK;
+  k_exchange<<<grid_for(e->nxch), kThreads, 0, s>>>(e->d, e->nxch, e->d_xdst, e->d_xsrc,
+                                                    md->prim, md->flag);
+  return check_launch();
+}
+
+int run_source(pangu_engine *e, const pangu_pack *md, double beta, const double *dt,
+               cudaStream_t s) {
+  const Dims &d = e->d;
+  if (e->p.metric_type == PANGU_METRIC_MINKOWSKI) return PANGU_OK;  // zero connection
+  const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
+  DISPATCH_MT(e->p.metric_type, k_source, grid_for(n), s, d, e->p, md->prim, md->cons, beta, dt);
+  return check_launch();
+}
+
+int run_recovery(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
+  const Dims &d = e->d;
+  const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
+  DISPATCH_MT(e->p.metric_type, k_recovery, grid_for(n), s, d, e->p, md->prim, md->cons, md->flag,
+              e->d_cnt);
+  return check_launch();
+}
+
+int run_heating(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
+  const Dims &d = e->d;
+  if (!e->p.enable_heating) return PANGU_OK;
+  const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
+  DISPATCH_MT(e->p.metric_type, k_heating, grid_for(n), s, d, e->p, md->prim, md->cons);
+  return check_launch();
+}
+
+int run_fix_recovery(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
+  const Dims &d = e->d;
+  if (cudaMemsetAsync(e->d_fail_count, 0, sizeof(int), s) != cudaSuccess) return PANGU_ECUDA;
+  const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
+  k_fixrec_scan<<<grid_for(n), kThreads, 0, s>>>(d, e->p, md->flag, e->d_fail_count,
+                                                 e->d_fail_list);
+  const unsigned g = 2 * 148;
+  k_fixrec_compute<<<g, kThreads, 0, s>>>(d, e->d_fail_count, e->d_fail_list, md->prim, md->flag,
+                                          e->d_fail_vals);
+  k_fixrec_write<<<g, kThreads, 0, s>>>(d, e->d_fail_count, e->d_fail_list, e->d_fail_vals,
+                                        md->prim, md->flag, e->d_cnt);
+  return check_launch();
+}
+
+int run_bcs(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
+  const Dims &d = e->d;
+  const int act[3] = {d.o1, d.o2, d.o3};
+  const int N[3] = {d.N1, d.N2, d.N3};
+  const int nb[3] = {e->m.nbx1, e->m.nbx2, e->m.nbx3};
+  for (int face = 0; face < 6; ++face) {
+    const int dir = face / 2, outer = face % 2;
+    const int kind = e->m.bc[face];
+    if (!act[dir] || kind == PANGU_BC_PERIODIC) continue;
+    long long ext = (long long)N[0] * N[1] * N[2] / N[dir] * e->m.ng;
+    const long long n = ext * d.NB;
+    k_bc_face<<<grid_for(n), kThreads, 0, s>>>(d, face, kind, dir, outer ? nb[dir] - 1 : 0,
+                                               e->m.nbx1, e->m.nbx2, e->p.enable_B, md->prim,
+                                               md->flag);
+    const int rc = check_launch();
+    if (rc) return rc;
+  }
+  return PANGU_OK;
+}
+
+int run_estimate_dt(pangu_engine *e, const pangu_pack *md, double *dt_out, cudaStream_t s) {
+  const Dims &d = e->d;
+  k_dt_init<<<grid_for(3 * d.NB), kThreads, 0, s>>>(3 * d.NB, e->d_dtmin);
+  const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
+  const unsigned gx = (unsigned)std::min<long long>((n / std::max(1, d.NB) + kThreads - 1) / kThreads, 592);
+  k_dt_reduce<<<dim3(std::max(1u, gx), d.NB), kThreads, 0, s>>>(d, e->p.cfl_number, md->alfven,
+                                                                 e->d_dtmin);
+  k_dt_finalize<<<1, 32, 0, s>>>(d.NB, e->d_dtmin, dt_out);
+  return check_launch();
+}
+
+template <class T>
+int dalloc(T **p, size_t n) {
+  return cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(T)) == cudaSuccess ? PANGU_OK
+                                                                                   : PANGU_ENOMEM;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int pangu_num_fields(const pangu_params *p) {
+  if (!p) return PANGU_EINVAL;
+  return 6 + (p->enable_B ? 3 : 0) + (p->enable_heating ? 1 : 0);
+}
+
+int pangu_engine_destroy(pangu_engine *e) {
+  if (!e) return PANGU_EINVAL;
+  cudaFree(e->d_t1);
+  cudaFree(e->d_t2);
+  cudaFree(e->d_origin);
+  cudaFree(e->d_xdst);
+  cudaFree(e->d_xsrc);
+  cudaFree(e->d_cnt);
+  cudaFree(e->d_fail_count);
+  cudaFree(e->d_fail_list);
+  cudaFree(e->d_fail_vals);
+  cudaFree(e->d_dtmin);
+  delete e;
+  return PANGU_OK;
+}
+
+int pangu_engine_create(const pangu_params *params, const pangu_mesh *mesh, pangu_engine **out) {
+  if (!params || !mesh || !out) return PANGU_EINVAL;
+  *out = nullptr;
+  const pangu_params &p = *params;
+  const pangu_mesh &m = *mesh;
+  if (m.nx1 < 1 || m.nx2 < 1 || m.nx3 < 1 || m.nbx1 < 1 || m.nbx2 < 1 || m.nbx3 < 1 || m.ng < 0)
+    return PANGU_EINVAL;
+  if (p.riemann_solver < 0 || p.riemann_solver > 1 || p.limiter < 0 || p.limiter > 1 ||
+      p.recovery < 0 || p.recovery > 1 || p.metric_type < 0 || p.metric_type > 3 || p.model < 0 ||
+      p.model > 5)
+    return PANGU_EINVAL;
+  const int need_ng = p.limiter == PANGU_LIMITER_PPM4 ? 3 : 2;
+  if (m.ng < need_ng) return PANGU_ENGHOST;
+  const int act[3] = {m.nx1 > 1, m.nx2 > 1, m.nx3 > 1};
+  const int nx[3] = {m.nx1, m.nx2, m.nx3};
+  for (int dd = 0; dd < 3; ++dd)
+    if (act[dd] && nx[dd] < m.ng) return PANGU_EINVAL;
+  for (int f = 0; f < 6; ++f)
+    if (m.bc[f] < 0 || m.bc[f] > 2) return PANGU_EINVAL;
+  pangu_engine *e = new (std::nothrow) pangu_engine;
+  if (!e) return PANGU_ENOMEM;
+  e->p = p;
+  e->m = m;
+  pgh::Layout L = pgh::make_layout(p, m);
+  Dims &d = e->d;
+  d.N1 = L.N[0];
+  d.N2 = L.N[1];
+  d.N3 = L.N[2];
+  d.NF = L.NF;
+  d.NB = L.NB;
+  d.o1 = act[0];
+  d.o2 = act[1];
+  d.o3 = act[2];
+  d.ndim = 1 + d.o2 + d.o3;
+  d.is = L.st[0]; d.ie = d.is + m.nx1 - 1;
+  d.js = L.st[1]; d.je = d.js + m.nx2 - 1;
+  d.ks = L.st[2]; d.ke = d.ks + m.nx3 - 1;
+  d.ncell = (long long)d.N1 * d.N2 * d.N3;
+  for (int dd = 0; dd < 3; ++dd) d.dx[dd] = L.dx[dd];
+  int n = 0;
+  for (int s = 0; s < NPRIM; ++s) d.pidx[s] = -1;
+  d.pidx[RHO] = n++; d.pidx[ENY] = n++;
+  d.pidx[UX1] = n++; d.pidx[UX2] = n++; d.pidx[UX3] = n++;
+  if (p.enable_B) { d.pidx[BX1] = n++; d.pidx[BX2] = n++; d.pidx[BX3] = n++; }
+  d.pidx[ENT] = n++;
+  if (p.enable_heating) d.pidx[KEL] = n++;
+
+  std::vector<double> t1, t2;
+  pgh::build_tables(p, L, t1, t2);
+  std::vector<int64_t> xdst, xsrc;
+  pgh::build_exchange(m, L, xdst, xsrc);
+  e->nxch = (long long)xdst.size();
+  e->fail_cap = (long long)d.NB * m.nx1 * m.nx2 * m.nx3;
+  int rc = PANGU_OK;
+  rc |= dalloc(&e->d_t1, t1.size());
+  rc |= dalloc(&e->d_t2, t2.size());
+  rc |= dalloc(&e->d_origin, L.origin.size());
+  rc |= dalloc(&e->d_xdst, xdst.size());
+  rc |= dalloc(&e->d_xsrc, xsrc.size());
+  rc |= dalloc(&e->d_cnt, PANGU_NCOUNTERS);
+  rc |= dalloc(&e->d_fail_count, 1);
+  rc |= dalloc(&e->d_fail_list, (size_t)e->fail_cap);
+  rc |= dalloc(&e->d_fail_vals, (size_t)e->fail_cap * d.NF);
+  rc |= dalloc(&e->d_dtmin, 3 * (size_t)d.NB);
+  if (rc != PANGU_OK) {
+    pangu_engine_destroy(e);
+    return PANGU_ENOMEM;
+  }
+  bool ok = cudaMemcpy(e->d_t1, t1.data(), t1.size() * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok &= cudaMemcpy(e->d_t2, t2.data(), t2.size() * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok &= cudaMemcpy(e->d_origin, L.origin.data(), L.origin.size() * 8, cudaMemcpyHostToDevice) ==
+        cudaSuccess;
+  if (!xdst.empty()) {
+    ok &= cudaMemcpy(e->d_xdst, xdst.data(), xdst.size() * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+    ok &= cudaMemcpy(e->d_xsrc, xsrc.data(), xsrc.size() * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+  }
+  ok &= cudaMemset(e->d_cnt, 0, PANGU_NCOUNTERS * sizeof(unsigned long long)) == cudaSuccess;
+  if (!ok) {
+    pangu_engine_destroy(e);
+    return PANGU_ECUDA;
+  }
+  d.t1 = e->d_t1;
+  d.t2 = e->d_t2;
+  d.origin = e->d_origin;
+  *out = e;
+  return PANGU_OK;
+}
+
+#define GUARD(e, md)                      \
+  if (!pack_ok(e, md)) return PANGU_EINVAL;
+
+int pangu_fix_primitive(pangu_engine *e, const pangu_pack *md, void *stream) {
+  GUARD(e, md);
+  return run_fix_primitive(e, md, S(stream));
+}
+int pangu_calculate_conservative(pangu_engine *e, const pangu_pack *md, void *stream) {
+  GUARD(e, md);
+  return run_calc_cons(e, md, S(stream));
+}
+int pangu_calculate_fluxes(pangu_engine *e, const pangu_pack *md, void *stream) {
+  GUARD(e, md);
+  return run_fluxes(e, md, S(stream));
+}
+int pangu_constrained_transport(pangu_engine *e, const pangu_pack *md, void *stream) {
+  GUARD(e, md);
+  if (!e->p.enable_B) return PANGU_EINVAL;
+  return run_ct(e, md, S(stream));
+}
+int pangu_flux_divergence_update(pangu_engine *e, const pangu_pack *mc_init, const pangu_pack *mc0,
+                                 const pangu_pack *mc1, double beta, const double *dt,
+                                 void *stream) {
+  if (!pack_ok(e, mc_init) || !pack_ok(e, mc0) || !pack_ok(e, mc1) || !dt) return PANGU_EINVAL;
+  return run_update(e, mc_init, mc0, mc1, beta, dt, S(stream));
+}
+int pangu_exchange_ghosts(pangu_engine *e, const pangu_pack *md, void *stream) {
+  GUARD(e, md);
+  return run_exchange(e, md, S(stream));
+}
+int pangu_add_geometric_source(pangu_engine *e, const pangu_pack *md, double beta, const double *dt,
+                               void *stream) {
+  GUARD(e, md);
+  if (!dt) return PANGU_EINVAL;
+  return run_source(e, md, beta, dt, S(stream));
+}
+int pangu_recovery(pangu_engine *e, const pangu_pack *md, void *stream) {
+  GUARD(e, md);
+  return run_recovery(e, md, S(stream));
+}
+int pangu_apply_electron_heating(pangu_engine *e, const pangu_pack *md, void *stream) {
+  GUARD(e, md);
+  return run_heating(e, md, S(stream));
+}
+int pangu_fix_recovery(pangu_engine *e, const pangu_pack *md, void *stream) {
+  GUARD(e, md);
+  if (e->p.recovery != PANGU_RECOVERY_CHAINER) return PANGU_EINVAL;
+  return run_fix_recovery(e, md, S(stream));
+}
+int pangu_apply_boundary_conditions(pangu_engine *e, const pangu_pack *md, void *stream) {
+  GUARD(e, md);
+  return run_bcs(e, md, S(stream));
+}
+int pangu_estimate_dt(pangu_engine *e, const pangu_pack *md, double *dt_out, void *stream) {
+  GUARD(e, md);
+  if (!dt_out) return PANGU_EINVAL;
+  return run_estimate_dt(e, md, dt_out, S(stream));
+}
+
+int pangu_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
+                double beta, const double *dt, double *dt_est, void *stream) {
+  if (!pack_ok(e, base) || !pack_ok(e, one) || !dt || (stage != 1 && stage != 2))
+    return PANGU_EINVAL;
+  cudaStream_t s = S(stream);
+  const pangu_pack *mc0 = stage == 1 ? base : one;
+  const pangu_pack *mc1 = stage == 1 ? one : base;
+  int rc;
+  if ((rc = run_fix_primitive(e, mc0, s))) return rc;
+  if ((rc = run_calc_cons(e, mc0, s))) return rc;
+  if ((rc = run_fluxes(e, mc0, s))) return rc;
+  if (e->p.enable_B && (rc = run_ct(e, mc0, s))) return rc;
+  if ((rc = run_update(e, base, mc0, mc1, beta, dt, s))) return rc;
+  if ((rc = run_exchange(e, mc1, s))) return rc;
+  if ((rc = run_source(e, mc1, beta, dt, s))) return rc;
+  if ((rc = run_recovery(e, mc1, s))) return rc;
+  if ((rc = run_heating(e, mc1, s))) return rc;
+  if (e->p.recovery == PANGU_RECOVERY_CHAINER && (rc = run_fix_recovery(e, mc1, s))) return rc;
+  if ((rc = run_bcs(e, mc1, s))) return rc;
+  if (stage == 2 && dt_est && (rc = run_estimate_dt(e, mc1, dt_est, s))) return rc;
+  return PANGU_OK;
+}
+
+int pangu_update_dt(pangu_engine *e, double *dt, const double *dt_est, double dt_factor,
+                    void *stream) {
+  if (!e || !dt || !dt_est) return PANGU_EINVAL;
+  k_update_dt<<<1, 32, 0, S(stream)>>>(dt, dt_est, dt_factor);
+  return check_launch();
+}
+
+int pangu_counters(pangu_engine *e, uint64_t out[PANGU_NCOUNTERS]) {
+  if (!e || !out) return PANGU_EINVAL;
+  unsigned long long tmp[PANGU_NCOUNTERS];
+  if (cudaMemcpy(tmp, e->d_cnt, sizeof(tmp), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return PANGU_ECUDA;
+  for (int i = 0; i < PANGU_NCOUNTERS; ++i) out[i] = tmp[i];
+  return PANGU_OK;
+}
+
+int pangu_reset_counters(pangu_engine *e, void *stream) {
+  if (!e) return PANGU_EINVAL;
+  return cudaMemsetAsync(e->d_cnt, 0, PANGU_NCOUNTERS * sizeof(unsigned long long), S(stream)) ==
+                 cudaSuccess
+             ? PANGU_OK
+             : PANGU_ECUDA;
+}
+
+}  // extern "C"

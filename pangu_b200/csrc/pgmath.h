@@ -1,0 +1,220 @@
+// pgmath.h -- pow, exp and log in double-double arithmetic, identical on the
+// host (g++, -ffp-contract=off) and the device (nvcc, --fmad=false).
+//
+// Why: the reference's conservative-to-primitive chain (recovery/scheme_*.h)
+// is chaotic in floor-dominated cells -- whether a Newton solve converges in
+// 30 iterations flips on one-ulp differences of its inputs -- so the engine
+// and the CPU oracle must round every operation identically. Basic IEEE
+// operations (+ - * / sqrt) already do; the C library's pow and CUDA's pow
+// do not agree with each other. Both sides therefore call these routines.
+//
+// Method (textbook double-double arithmetic, own implementation):
+//   * error-free transforms two_sum (Knuth) and two_prod via fused
+//     multiply-add (Dekker's product with an exact fma);
+//   * log x = e ln 2 + 2 atanh(s), s = (m - 1)/(m + 1), m in [1/sqrt2, sqrt2),
+//     the atanh series summed to |s|^42 (first nine terms in double-double);
+//   * exp t = 2^k exp(r), r = (t - k ln 2)/64, Taylor series of exp(r) - 1 to
+//     r^12 (first five terms in double-double), then six squarings;
+//   * pow x^y = exp(y log x).
+// The relative error before the final rounding is below 2^-95, so the result
+// is the correctly rounded one except when the exact value lies within
+// 2^-95 of a rounding boundary. tests/test_pgmath.py checks agreement with
+// the C library's pow/exp/log on many inputs.
+#ifndef PANGU_PGMATH_H
+#define PANGU_PGMATH_H
+
+#include <cmath>
+
+#if defined(__CUDACC__)
+#define PGM_FN __host__ __device__ __forceinline__
+#else
+#define PGM_FN inline
+#endif
+
+namespace pgm {
+
+struct dd {
+  double hi, lo;
+};
+
+PGM_FN double fma_(double a, double b, double c) {
+#if defined(__CUDA_ARCH__)
+  return __fma_rn(a, b, c);
+#else
+  return std::fma(a, b, c);
+#endif
+}
+
+PGM_FN dd two_sum(double a, double b) {
+  const double s = a + b;
+  const double bb = s - a;
+  const double e = (a - (s - bb)) + (b - bb);
+  return {s, e};
+}
+PGM_FN dd quick_two_sum(double a, double b) {  // |a| >= |b| (or a == 0)
+  const double s = a + b;
+  const double e = b - (s - a);
+  return {s, e};
+}
+PGM_FN dd two_prod(double a, double b) {
+  const double p = a * b;
+  return {p, fma_(a, b, -p)};
+}
+PGM_FN dd add(dd a, dd b) {
+  dd s = two_sum(a.hi, b.hi);
+  const dd t = two_sum(a.lo, b.lo);
+  s.lo += t.hi;
+  s = quick_two_sum(s.hi, s.lo);
+  s.lo += t.lo;
+  return quick_two_sum(s.hi, s.lo);
+}
+PGM_FN dd sub(dd a, dd b) { return add(a, dd{-b.hi, -b.lo}); }
+PGM_FN dd mul(dd a, dd b) {
+  dd p = two_prod(a.hi, b.hi);
+  p.lo += a.hi * b.lo + a.lo * b.hi;
+  return quick_two_sum(p.hi, p.lo);
+}
+PGM_FN dd mul_d(dd a, double b) {
+  dd p = two_prod(a.hi, b);
+  p.lo += a.lo * b;
+  return quick_two_sum(p.hi, p.lo);
+}
+PGM_FN dd div(dd a, dd b) {
+  const double q1 = a.hi / b.hi;
+  dd r = sub(a, mul_d(b, q1));
+  const double q2 = r.hi / b.hi;
+  r = sub(r, mul_d(b, q2));
+  const double q3 = r.hi / b.hi;
+  const dd q = quick_two_sum(q1, q2);
+  return add(q, dd{q3, 0.0});
+}
+
+// ln 2 and 1/ln 2
+#define PGM_LN2 (::pgm::dd{0x1.62e42fefa39efp-1, 0x1.abc9e3b39803fp-56})
+#define PGM_INV_LN2 0x1.71547652b82fep+0
+
+// 1/(2k+1), k = 1..9, as double-double
+PGM_FN dd atanh_coef(int k) {
+  switch (k) {
+    case 1: return {0x1.5555555555555p-2, 0x1.5555555555555p-56};
+    case 2: return {0x1.999999999999ap-3, -0x1.999999999999ap-57};
+    case 3: return {0x1.2492492492492p-3, 0x1.2492492492492p-57};
+    case 4: return {0x1.c71c71c71c71cp-4, 0x1.c71c71c71c71cp-58};
+    case 5: return {0x1.745d1745d1746p-4, -0x1.745d1745d1746p-59};
+    case 6: return {0x1.3b13b13b13b14p-4, -0x1.3b13b13b13b14p-58};
+    case 7: return {0x1.1111111111111p-4, 0x1.1111111111111p-60};
+    case 8: return {0x1.e1e1e1e1e1e1ep-5, 0x1.e1e1e1e1e1e1ep-61};
+    default: return {0x1.af286bca1af28p-5, 0x1.af286bca1af28p-59};
+  }
+}
+
+// log x as double-double for finite x > 0.
+PGM_FN dd log_dd(double x) {
+  int e;
+  double m = frexp(x, &e);  // x = m 2^e, m in [0.5, 1)
+  if (m < 0.70710678118654752) {
+    m *= 2.0;
+    e -= 1;
+  }
+  const double f = m - 1.0;  // exact
+  const dd s = div(dd{f, 0.0}, two_sum(m, 1.0));
+  const dd s2 = mul(s, s);
+  // sum_{k=10}^{20} s2^(k-10) / (2k+1) in double
+  double t = 0x1.8f9c18f9c18fap-6;                 // 1/41
+  t = 0x1.a41a41a41a41ap-6 + s2.hi * t;           // 1/39
+  t = 0x1.bacf914c1bad0p-6 + s2.hi * t;           // 1/37
+  t = 0x1.d41d41d41d41dp-6 + s2.hi * t;           // 1/35
+  t = 0x1.f07c1f07c1f08p-6 + s2.hi * t;           // 1/33
+  t = 0x1.0842108421084p-5 + s2.hi * t;           // 1/31
+  t = 0x1.1a7b9611a7b96p-5 + s2.hi * t;           // 1/29
+  t = 0x1.2f684bda12f68p-5 + s2.hi * t;           // 1/27
+  t = 0x1.47ae147ae147bp-5 + s2.hi * t;           // 1/25
+  t = 0x1.642c8590b2164p-5 + s2.hi * t;           // 1/23
+  t = 0x1.8618618618618p-5 + s2.hi * t;           // 1/21
+  dd acc = {t, 0.0};
+  for (int k = 9; k >= 1; --k) acc = add(mul(acc, s2), atanh_coef(k));
+  acc = add(mul(acc, s2), dd{1.0, 0.0});
+  const dd logm = mul(mul_d(s, 2.0), acc);
+  return add(mul_d(PGM_LN2, (double)e), logm);
+}
+
+// exp t rounded to double, t a double-double.
+PGM_FN double exp_round(dd t) {
+  if (t.hi > 709.79) return HUGE_VAL;
+  if (t.hi < -745.2) return 0.0;
+  const double kd = rint(t.hi * PGM_INV_LN2);
+  dd r = sub(t, mul_d(PGM_LN2, kd));
+  r.hi *= 0.015625;  // 2^-6, exact
+  r.lo *= 0.015625;
+  // T6 = sum_{n=6}^{12} r^(n-6)/n! in double
+  double tl = 0x1.1eed8eff8d898p-29;              // 1/12!
+  tl = 0x1.ae64567f544e4p-26 + r.hi * tl;         // 1/11!
+  tl = 0x1.27e4fb7789f5cp-22 + r.hi * tl;         // 1/10!
+  tl = 0x1.71de3a556c734p-19 + r.hi * tl;         // 1/9!
+  tl = 0x1.a01a01a01a01ap-16 + r.hi * tl;         // 1/8!
+  tl = 0x1.a01a01a01a01ap-13 + r.hi * tl;         // 1/7!
+  tl = 0x1.6c16c16c16c17p-10 + r.hi * tl;         // 1/6!
+  dd acc = {tl, 0.0};
+  acc = add(mul(acc, r), dd{0x1.1111111111111p-7, 0x1.1111111111111p-63});  // 1/5!
+  acc = add(mul(acc, r), dd{0x1.5555555555555p-5, 0x1.5555555555555p-59});  // 1/4!
+  acc = add(mul(acc, r), dd{0x1.5555555555555p-3, 0x1.5555555555555p-57});  // 1/3!
+  acc = add(mul(acc, r), dd{0.5, 0.0});
+  acc = add(mul(acc, r), dd{1.0, 0.0});
+  dd q = mul(acc, r);  // exp(r) - 1
+  for (int i = 0; i < 6; ++i) q = add(mul_d(q, 2.0), mul(q, q));  // (1+q)^2 - 1
+  const dd E = add(dd{1.0, 0.0}, q);
+  return ldexp(E.hi, (int)kd);
+}
+
+PGM_FN bool is_inf(double x) { return fabs(x) == HUGE_VAL; }
+PGM_FN bool sign_bit(double x) { return copysign(1.0, x) < 0.0; }
+
+PGM_FN bool is_odd_integer(double y) {
+  if (floor(y) != y) return false;
+  if (fabs(y) >= 9007199254740992.0) return false;  // 2^53: even
+  return fmod(y, 2.0) != 0.0;
+}
+
+PGM_FN double pow(double x, double y) {
+  if (y == 0.0) return 1.0;
+  if (x == 1.0) return 1.0;
+  if (x != x || y != y) return x + y;
+  if (is_inf(y)) {
+    const double ax = fabs(x);
+    if (ax == 1.0) return 1.0;
+    if ((ax < 1.0) == (y > 0.0)) return 0.0;
+    return HUGE_VAL;
+  }
+  bool negate = false;
+  if (x < 0.0 || (x == 0.0 && sign_bit(x))) {
+    if (x != 0.0 && floor(y) != y) return (x - x) / (x - x);  // NaN
+    negate = is_odd_integer(y);
+    x = -x;
+  }
+  double r;
+  if (x == 0.0) {
+    r = y < 0.0 ? HUGE_VAL : 0.0;
+  } else if (is_inf(x)) {
+    r = y < 0.0 ? 0.0 : HUGE_VAL;
+  } else {
+    r = exp_round(mul_d(log_dd(x), y));
+  }
+  return negate ? -r : r;
+}
+
+PGM_FN double exp(double x) {
+  if (x != x) return x;
+  if (is_inf(x)) return x > 0.0 ? x : 0.0;
+  return exp_round(dd{x, 0.0});
+}
+
+PGM_FN double log(double x) {
+  if (x != x) return x;
+  if (x < 0.0) return (x - x) / (x - x);
+  if (x == 0.0) return -HUGE_VAL;
+  if (is_inf(x)) return x;
+  return log_dd(x).hi;
+}
+
+}  // namespace pgm
+#endif  // PANGU_PGMATH_H

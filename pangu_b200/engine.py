@@ -1,0 +1,247 @@
+"""Host side of the engine: library loading, device containers, stage driver.
+
+The compute path is the CUDA library ``_lib/libpangu_b200.so`` reached
+through the C ABI of include/pangu_b200.h. There is no CPU fallback: if the
+library is missing and cannot be built, or no CUDA device is present, the
+calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+from .params import ParameterInput, mesh_struct, params_struct, process_packages
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_lib = None
+
+_P = C.c_void_p
+_PK = C.POINTER(abi.Pack)
+_DP = C.c_void_p  # device double*
+
+
+class EngineError(RuntimeError):
+    pass
+
+
+_ERRORS = {abi.PANGU_EINVAL: "invalid argument", abi.PANGU_ECUDA: "CUDA error",
+           abi.PANGU_ENOMEM: "out of device memory",
+           abi.PANGU_ENGHOST: "ghost width too small for the limiter",
+           abi.PANGU_ETOOBIG: "size above the supported maximum"}
+
+
+def _check(rc, what):
+    if rc != abi.PANGU_OK:
+        raise EngineError(f"{what}: {_ERRORS.get(rc, rc)} ({rc})")
+
+
+def library_path() -> str:
+    return os.path.join(_HERE, "_lib", "libpangu_b200.so")
+
+
+def lib():
+    """Loads the engine library (building it in-tree first if it is absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not os.path.exists(path):
+        from . import build
+        build.build()
+    L = C.CDLL(path)
+    L.pangu_num_fields.argtypes = [C.POINTER(abi.Params)]
+    L.pangu_engine_create.argtypes = [C.POINTER(abi.Params), C.POINTER(abi.Mesh), C.POINTER(_P)]
+    L.pangu_engine_destroy.argtypes = [_P]
+    for name in ("pangu_fix_primitive", "pangu_calculate_conservative", "pangu_calculate_fluxes",
+                 "pangu_constrained_transport", "pangu_exchange_ghosts", "pangu_recovery",
+                 "pangu_apply_electron_heating", "pangu_fix_recovery",
+                 "pangu_apply_boundary_conditions"):
+        getattr(L, name).argtypes = [_P, _PK, _P]
+    L.pangu_flux_divergence_update.argtypes = [_P, _PK, _PK, _PK, C.c_double, _DP, _P]
+    L.pangu_add_geometric_source.argtypes = [_P, _PK, C.c_double, _DP, _P]
+    L.pangu_estimate_dt.argtypes = [_P, _PK, _DP, _P]
+    L.pangu_stage.argtypes = [_P, C.c_int, _PK, _PK, C.c_double, _DP, _DP, _P]
+    L.pangu_update_dt.argtypes = [_P, _DP, _DP, C.c_double, _P]
+    L.pangu_counters.argtypes = [_P, C.POINTER(C.c_uint64)]
+    L.pangu_reset_counters.argtypes = [_P, _P]
+    _lib = L
+    return L
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise EngineError("the engine needs a CUDA device; none is visible")
+    return torch
+
+
+class DeviceContainer:
+    """One stage container ("base" or "1") in device memory (torch tensors).
+
+    ``alfven``, ``efield`` and ``flag`` are shared between the two containers
+    of a job (Metadata::OneCopy, package_registration.cc:121-145)."""
+
+    FIELDS = ("prim", "cons", "flux1", "flux2", "flux3", "alfven", "efield", "flag")
+
+    def __init__(self, nb, nf, shape, device, shared=None):
+        torch = _torch()
+        n3, n2, n1 = shape
+        z = lambda *s: torch.zeros(s, dtype=torch.float64, device=device)  # noqa: E731
+        self.prim = z(nb, nf, n3, n2, n1)
+        self.cons = z(nb, nf, n3, n2, n1)
+        self.flux1 = z(nb, nf, n3, n2, n1)
+        self.flux2 = z(nb, nf, n3, n2, n1)
+        self.flux3 = z(nb, nf, n3, n2, n1)
+        if shared is None:
+            self.alfven = z(nb, 3, n3, n2, n1)
+            self.efield = z(nb, 3, n3, n2, n1)
+            self.flag = z(nb, n3, n2, n1)
+        else:
+            self.alfven, self.efield, self.flag = shared.alfven, shared.efield, shared.flag
+        self._pack = abi.Pack()
+        for f in self.FIELDS:
+            setattr(self._pack, f, getattr(self, f).data_ptr())
+
+    @property
+    def pack(self):
+        return C.byref(self._pack)
+
+
+class Engine:
+    """An engine handle for one parameter set and mesh."""
+
+    def __init__(self, params: abi.Params, mesh: abi.Mesh, device=0):
+        torch = _torch()
+        self.device = torch.device("cuda", device)
+        self.L = lib()
+        self.params, self.mesh = params, mesh
+        h = _P()
+        with torch.cuda.device(self.device):
+            _check(self.L.pangu_engine_create(C.byref(params), C.byref(mesh), C.byref(h)),
+                   "pangu_engine_create")
+        self.h = h
+        self.nf = self.L.pangu_num_fields(C.byref(params))
+        self.nb = mesh.nbx1 * mesh.nbx2 * mesh.nbx3
+        act = [mesh.nx1 > 1, mesh.nx2 > 1, mesh.nx3 > 1]
+        n = [mesh.nx1, mesh.nx2, mesh.nx3]
+        self.shape = tuple(n[d] + 2 * mesh.ng * act[d] for d in (2, 1, 0))
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.L.pangu_engine_destroy(self.h)
+            self.h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def stream(self):
+        import torch
+        return _P(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def new_containers(self):
+        base = DeviceContainer(self.nb, self.nf, self.shape, self.device)
+        one = DeviceContainer(self.nb, self.nf, self.shape, self.device, shared=base)
+        return base, one
+
+    # ---- per-task entry points ------------------------------------------
+    def _task(self, name, md):
+        _check(getattr(self.L, name)(self.h, md.pack, self.stream()), name)
+
+    def fix_primitive(self, md): self._task("pangu_fix_primitive", md)
+    def calculate_conservative(self, md): self._task("pangu_calculate_conservative", md)
+    def calculate_fluxes(self, md): self._task("pangu_calculate_fluxes", md)
+    def constrained_transport(self, md): self._task("pangu_constrained_transport", md)
+    def exchange_ghosts(self, md): self._task("pangu_exchange_ghosts", md)
+    def recovery(self, md): self._task("pangu_recovery", md)
+    def apply_electron_heating(self, md): self._task("pangu_apply_electron_heating", md)
+    def fix_recovery(self, md): self._task("pangu_fix_recovery", md)
+    def apply_boundary_conditions(self, md): self._task("pangu_apply_boundary_conditions", md)
+
+    def flux_divergence_update(self, mc_init, mc0, mc1, beta, dt_dev):
+        _check(self.L.pangu_flux_divergence_update(self.h, mc_init.pack, mc0.pack, mc1.pack,
+                                                   beta, dt_dev.data_ptr(), self.stream()),
+               "pangu_flux_divergence_update")
+
+    def add_geometric_source(self, md, beta, dt_dev):
+        _check(self.L.pangu_add_geometric_source(self.h, md.pack, beta, dt_dev.data_ptr(),
+                                                 self.stream()), "pangu_add_geometric_source")
+
+    def estimate_dt(self, md, out_dev):
+        _check(self.L.pangu_estimate_dt(self.h, md.pack, out_dev.data_ptr(), self.stream()),
+               "pangu_estimate_dt")
+
+    def stage(self, st, base, one, beta, dt_dev, dt_est_dev=None):
+        est = dt_est_dev.data_ptr() if dt_est_dev is not None else None
+        _check(self.L.pangu_stage(self.h, st, base.pack, one.pack, beta, dt_dev.data_ptr(), est,
+                                  self.stream()), "pangu_stage")
+
+    def update_dt(self, dt_dev, dt_est_dev, factor):
+        _check(self.L.pangu_update_dt(self.h, dt_dev.data_ptr(), dt_est_dev.data_ptr(), factor,
+                                      self.stream()), "pangu_update_dt")
+
+    def counters(self):
+        out = (C.c_uint64 * abi.NCOUNTERS)()
+        _check(self.L.pangu_counters(self.h, out), "pangu_counters")
+        return np.array(list(out), dtype=np.uint64)
+
+    def reset_counters(self):
+        _check(self.L.pangu_reset_counters(self.h, self.stream()), "pangu_reset_counters")
+
+
+# rk2 of Parthenon's low-storage integrator: beta[stage % 2] with
+# beta = {1.0, 0.5} (ideal_grmhd.cc:29).
+RK2_BETA = (1.0, 0.5)
+
+
+class Simulation:
+    """A job: packages, mesh, the two stage containers and the dt policy.
+
+    Mirrors Simulator::MakeTaskCollection (ideal_grmhd.cc:23-120) stage by
+    stage, with every task on the GPU.
+    """
+
+    def __init__(self, pin: ParameterInput, device=0):
+        torch = _torch()
+        self.pin = pin
+        self.packages = process_packages(pin)
+        self.params = params_struct(self.packages)
+        self.mesh = mesh_struct(pin)
+        self.engine = Engine(self.params, self.mesh, device)
+        self.base, self.one = self.engine.new_containers()
+        dev = self.engine.device
+        self.dt_init = pin.get_or_add_real("parthenon/time", "dt_init", 1e-5)
+        self.dt_factor = pin.get_or_add_real("parthenon/time", "dt_factor", 2.0)
+        self.dt = torch.full((1,), self.dt_init, dtype=torch.float64, device=dev)
+        self.dt_est = torch.zeros(1, dtype=torch.float64, device=dev)
+        self.cycle = 0
+
+    def set_primitives(self, prim: np.ndarray):
+        """Loads initial primitives (interior values; ghosts are filled here:
+        exchange then physical BCs, as Parthenon does after the problem
+        generator). Container "1" starts as a copy of "base"."""
+        torch = _torch()
+        self.base.prim.copy_(torch.as_tensor(prim, device=self.engine.device))
+        self.engine.exchange_ghosts(self.base)
+        self.engine.apply_boundary_conditions(self.base)
+        self.one.prim.copy_(self.base.prim)
+        self.one.cons.copy_(self.base.cons)
+
+    def stage(self, st: int, dt_est=None):
+        self.engine.stage(st, self.base, self.one, RK2_BETA[st % 2], self.dt, dt_est)
+
+    def step(self, fixed_dt: bool = False):
+        """One rk2 cycle; afterwards dt = min(dt_factor * dt, estimate)."""
+        self.stage(1)
+        self.stage(2, self.dt_est)
+        if not fixed_dt:
+            self.engine.update_dt(self.dt, self.dt_est, self.dt_factor)
+        self.cycle += 1
+
+    def primitives(self) -> np.ndarray:
+        return self.base.prim.cpu().numpy()

@@ -1,0 +1,79 @@
+"""The double-double pow/exp/log shared by the oracle and the engine
+(pangu_b200/csrc/pgmath.h): correctly rounded against 60-digit decimal
+arithmetic, and close to the C library's (which misrounds some results)."""
+import ctypes as C
+from decimal import Decimal, getcontext
+
+import numpy as np
+
+import pyoracle as po
+
+getcontext().prec = 60
+L = po.lib()
+_D = C.POINTER(C.c_double)
+
+
+def _pow(x, y):
+    out = np.empty_like(x)
+    L.or_pgm_pow(len(x), x.ctypes.data_as(_D), y.ctypes.data_as(_D), out.ctypes.data_as(_D))
+    return out
+
+
+def _exp(x):
+    out = np.empty_like(x)
+    L.or_pgm_exp(len(x), x.ctypes.data_as(_D), out.ctypes.data_as(_D))
+    return out
+
+
+def _log(x):
+    out = np.empty_like(x)
+    L.or_pgm_log(len(x), x.ctypes.data_as(_D), out.ctypes.data_as(_D))
+    return out
+
+
+def _is_correctly_rounded(v, exact):
+    """|v - exact| <= half an ulp of v."""
+    v = float(v)
+    ulp = np.spacing(abs(v))
+    return abs(Decimal(v) - exact) <= Decimal(ulp) / 2
+
+
+def test_pow_correctly_rounded():
+    rng = np.random.default_rng(7)
+    x = 10 ** rng.uniform(-10, 6, 3000)
+    y = rng.choice([5 / 3, -5 / 3, 4 / 3, -4 / 3, 2 / 3, -1.5, -2.5, 0.7, -1.4, 3.3], 3000)
+    out = _pow(x, y)
+    for xi, yi, oi in zip(x, y, out):
+        exact = (Decimal(float(xi)).ln() * Decimal(float(yi))).exp()
+        assert _is_correctly_rounded(oi, exact), (xi.hex(), yi.hex(), oi.hex())
+
+
+def test_exp_log_correctly_rounded():
+    rng = np.random.default_rng(8)
+    e = rng.uniform(-700, 700, 2000)
+    for xi, oi in zip(e, _exp(e)):
+        assert _is_correctly_rounded(oi, Decimal(float(xi)).exp())
+    l = 10 ** rng.uniform(-300, 300, 2000)
+    for xi, oi in zip(l, _log(l)):
+        assert _is_correctly_rounded(oi, Decimal(float(xi)).ln())
+
+
+def test_agrees_with_c_library_within_one_ulp():
+    rng = np.random.default_rng(9)
+    x = 10 ** rng.uniform(-12, 6, 200000)
+    y = rng.uniform(-5, 5, 200000)
+    ref = np.power(x, y)
+    out = _pow(x, y)
+    assert np.all(np.abs(out - ref) <= np.spacing(np.abs(ref)))
+    assert np.mean(out == ref) > 0.9
+
+
+def test_special_values():
+    inf, nan = np.inf, np.nan
+    xs = np.array([0.0, -0.0, 0.0, 1.0, 2.0, -2.0, -2.0, inf, inf, 0.5, 2.0, nan, 1.0, -8.0])
+    ys = np.array([2.0, 3.0, -1.0, nan, 0.0, 3.0, 0.5, 2.0, -2.0, inf, -inf, 0.0, inf, 1 / 3])
+    ref = np.power(xs, ys)
+    out = _pow(xs, ys)
+    np.testing.assert_array_equal(np.isnan(out), np.isnan(ref))
+    ok = ~np.isnan(ref)
+    np.testing.assert_array_equal(out[ok], ref[ok])
