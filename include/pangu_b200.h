@@ -217,6 +217,9 @@ int pangu_update_dt(pangu_engine *e, double *dt, const double *dt_est,
 int pangu_counters(pangu_engine *e, uint64_t out[PANGU_NCOUNTERS]);
 int pangu_reset_counters(pangu_engine *e, void *stream);
 
+/* Number of CUDA kernels this handle has launched so far (host-side count). */
+long long pangu_launches(const pangu_engine *e);
+
 #ifdef __cplusplus
 }
 #endif

@@ -61,6 +61,7 @@ struct pangu_engine {
   double *d_fail_vals = nullptr;
   long long fail_cap = 0;
   unsigned long long *d_dtmin = nullptr;
+  long long launches = 0;  // kernels launched through this handle
 };
 
 namespace {
@@ -898,6 +899,7 @@ int run_fix_primitive(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
   const Dims &d = e->d;
   const long long n = (long long)d.NB * d.ncell;
   DISPATCH_MT(e->p.metric_type, k_fix_primitive, grid_for(n), s, d, e->p, md->prim, e->d_cnt);
+  ++e->launches;
   return check_launch();
 }
 
@@ -905,6 +907,7 @@ int run_calc_cons(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
   const Dims &d = e->d;
   const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
   DISPATCH_MT(e->p.metric_type, k_calc_cons, grid_for(n), s, d, e->p, md->prim, md->cons);
+  ++e->launches;
   return check_launch();
 }
 
@@ -928,6 +931,7 @@ int run_fluxes(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
     else if (dir == 2) DISPATCH_MT(e->p.metric_type, k_flux2, g, s, FLUX_ARGS);
     else DISPATCH_MT(e->p.metric_type, k_flux3, g, s, FLUX_ARGS);
 #undef FLUX_ARGS
+    ++e->launches;
     const int rc = check_launch();
     if (rc) return rc;
   }
@@ -939,12 +943,13 @@ int run_ct(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
   const int o1 = d.N1 > 1, o2 = d.N2 > 1, o3 = d.N3 > 1;
   k_ct_emf<<<grid_for(box_count(d.NB, d.ks, d.ke + o3, d.js, d.je + o2, d.is, d.ie + o1)),
              kThreads, 0, s>>>(d, md->flux1, md->flux2, md->flux3, md->efield);
+  ++e->launches;
   double *F[3] = {md->flux1, md->flux2, md->flux3};
-  for (int dir = 1; dir <= 3; ++dir) {
-    if (dir > 1 && !F[dir - 1]) continue;
+  for (int dir = 1; dir <= d.ndim; ++dir) {
     const int ei = dir == 1 ? o1 : 0, ej = dir == 2 ? o2 : 0, ek = dir == 3 ? o3 : 0;
     const long long n = box_count(d.NB, d.ks, d.ke + ek, d.js, d.je + ej, d.is, d.ie + ei);
     k_ct_faces<<<grid_for(n), kThreads, 0, s>>>(d, dir, F[dir - 1], md->efield);
+    ++e->launches;
   }
   return check_launch();
 }
@@ -955,6 +960,7 @@ int run_update(pangu_engine *e, const pangu_pack *mi, const pangu_pack *m0, cons
   const long long n = box_count(d.NB * d.NF, d.ks, d.ke, d.js, d.je, d.is, d.ie);
   k_flux_div_update<<<grid_for(n), kThreads, 0, s>>>(d, m0->flux1, m0->flux2, m0->flux3,
                                                      mi->cons, m1->cons, beta, dt);
+  ++e->launches;
   return check_launch();
 }
 
@@ -962,6 +968,7 @@ int run_exchange(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
   if (e->nxch == 0) return PANGU_OK;
   k_exchange<<<grid_for(e->nxch), kThreads, 0, s>>>(e->d, e->nxch, e->d_xdst, e->d_xsrc,
                                                     md->prim, md->flag);
+  ++e->launches;
   return check_launch();
 }
 
@@ -971,6 +978,7 @@ int run_source(pangu_engine *e, const pangu_pack *md, double beta, const double 
   if (e->p.metric_type == PANGU_METRIC_MINKOWSKI) return PANGU_OK;  // zero connection
   const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
   DISPATCH_MT(e->p.metric_type, k_source, grid_for(n), s, d, e->p, md->prim, md->cons, beta, dt);
+  ++e->launches;
   return check_launch();
 }
 
@@ -979,6 +987,7 @@ int run_recovery(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
   const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
   DISPATCH_MT(e->p.metric_type, k_recovery, grid_for(n), s, d, e->p, md->prim, md->cons, md->flag,
               e->d_cnt);
+  ++e->launches;
   return check_launch();
 }
 
@@ -987,6 +996,7 @@ int run_heating(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
   if (!e->p.enable_heating) return PANGU_OK;
   const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
   DISPATCH_MT(e->p.metric_type, k_heating, grid_for(n), s, d, e->p, md->prim, md->cons);
+  ++e->launches;
   return check_launch();
 }
 
@@ -1001,6 +1011,7 @@ int run_fix_recovery(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
                                           e->d_fail_vals);
   k_fixrec_write<<<g, kThreads, 0, s>>>(d, e->d_fail_count, e->d_fail_list, e->d_fail_vals,
                                         md->prim, md->flag, e->d_cnt);
+  e->launches += 3;
   return check_launch();
 }
 
@@ -1018,6 +1029,7 @@ int run_bcs(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
     k_bc_face<<<grid_for(n), kThreads, 0, s>>>(d, face, kind, dir, outer ? nb[dir] - 1 : 0,
                                                e->m.nbx1, e->m.nbx2, e->p.enable_B, md->prim,
                                                md->flag);
+    ++e->launches;
     const int rc = check_launch();
     if (rc) return rc;
   }
@@ -1032,6 +1044,7 @@ int run_estimate_dt(pangu_engine *e, const pangu_pack *md, double *dt_out, cudaS
   k_dt_reduce<<<dim3(std::max(1u, gx), d.NB), kThreads, 0, s>>>(d, e->p.cfl_number, md->alfven,
                                                                  e->d_dtmin);
   k_dt_finalize<<<1, 32, 0, s>>>(d.NB, e->d_dtmin, dt_out);
+  e->launches += 3;
   return check_launch();
 }
 
@@ -1243,6 +1256,7 @@ int pangu_update_dt(pangu_engine *e, double *dt, const double *dt_est, double dt
                     void *stream) {
   if (!e || !dt || !dt_est) return PANGU_EINVAL;
   k_update_dt<<<1, 32, 0, S(stream)>>>(dt, dt_est, dt_factor);
+  ++e->launches;
   return check_launch();
 }
 
@@ -1254,6 +1268,8 @@ int pangu_counters(pangu_engine *e, uint64_t out[PANGU_NCOUNTERS]) {
   for (int i = 0; i < PANGU_NCOUNTERS; ++i) out[i] = tmp[i];
   return PANGU_OK;
 }
+
+long long pangu_launches(const pangu_engine *e) { return e ? e->launches : PANGU_EINVAL; }
 
 int pangu_reset_counters(pangu_engine *e, void *stream) {
   if (!e) return PANGU_EINVAL;

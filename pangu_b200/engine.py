@@ -67,6 +67,8 @@ def lib():
     L.pangu_update_dt.argtypes = [_P, _DP, _DP, C.c_double, _P]
     L.pangu_counters.argtypes = [_P, C.POINTER(C.c_uint64)]
     L.pangu_reset_counters.argtypes = [_P, _P]
+    L.pangu_launches.argtypes = [_P]
+    L.pangu_launches.restype = C.c_longlong
     _lib = L
     return L
 
@@ -189,6 +191,9 @@ class Engine:
         out = (C.c_uint64 * abi.NCOUNTERS)()
         _check(self.L.pangu_counters(self.h, out), "pangu_counters")
         return np.array(list(out), dtype=np.uint64)
+
+    def launches(self) -> int:
+        return int(self.L.pangu_launches(self.h))
 
     def reset_counters(self):
         _check(self.L.pangu_reset_counters(self.h, self.stream()), "pangu_reset_counters")
