@@ -209,6 +209,21 @@ int pangu_stage(pangu_engine *e, int stage, const pangu_pack *base,
                 const pangu_pack *one, double beta, const double *dt,
                 double *dt_est, void *stream);
 
+/* The dt estimate of pangu_estimate_dt without an engine handle and without
+ * allocating: for callers that may not call cudaMalloc (their device memory
+ * belongs to a pool or a fixed budget, so they cannot create an engine, which
+ * allocates). No counterpart in the reference. Arguments: the engine's params
+ * and mesh structs, the caller's alfven array ([NB][3][N3][N2][N1], device)
+ * and a device double for the result. Scratch lives in a file-scope device
+ * array of 3 x 4096 minima (96 KiB on every GPU that loads the library, held
+ * until exit): meshes with more than 4096 blocks get PANGU_ETOOBIG. The first
+ * call on a device looks the array's address up (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture. All
+ * calls share the array: calls that overlap on the GPU (other streams or
+ * devices sharing a context) race, so serialise them. */
+int pangu_estimate_dt_noalloc(const pangu_params *params, const pangu_mesh *mesh,
+                              const double *alfven, double *dt_out, void *stream);
+
 /* Device dt policy applied after each cycle: dt = min(dt_factor*dt, dt_est). */
 int pangu_update_dt(pangu_engine *e, double *dt, const double *dt_est,
                     double dt_factor, void *stream);

@@ -12,6 +12,7 @@
 #include <cfloat>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -1250,6 +1251,81 @@ int pangu_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_
   if ((rc = run_bcs(e, mc1, s))) return rc;
   if (stage == 2 && dt_est && (rc = run_estimate_dt(e, mc1, dt_est, s))) return rc;
   return PANGU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// dt estimate without any allocation.
+//
+// Some callers cannot call cudaMalloc: an application whose device memory is
+// owned by a pool or a fixed budget (a Parthenon/Kokkos memory pool, or a
+// serving loop that admits jobs against an HBM budget) may not allocate on
+// the side, and cannot create a pangu_engine, which allocates its tables and
+// scratch. pangu_estimate_dt_noalloc serves them: it needs only the caller's
+// alfven array and output, and keeps its per-block scratch in the file-scope
+// device array below, which every GPU that loads this library holds until
+// the process exits.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kNoAllocMaxBlocks = 4096;  // 3 minima per block: 96 KiB
+constexpr int kNoAllocMaxDevices = 64;
+static __device__ __align__(256) unsigned long long g_noalloc_dtmin[3 * kNoAllocMaxBlocks];
+std::mutex g_noalloc_mutex;
+void *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+}  // namespace
+
+int pangu_estimate_dt_noalloc(const pangu_params *params, const pangu_mesh *mesh,
+                              const double *alfven, double *dt_out, void *stream) {
+  if (!params || !mesh || !alfven || !dt_out) return PANGU_EINVAL;
+  const pangu_mesh &m = *mesh;
+  if (m.nx1 < 1 || m.nx2 < 1 || m.nx3 < 1 || m.nbx1 < 1 || m.nbx2 < 1 || m.nbx3 < 1 || m.ng < 0)
+    return PANGU_EINVAL;
+  const long long nb = (long long)m.nbx1 * m.nbx2 * m.nbx3;
+  if (nb > kNoAllocMaxBlocks) return PANGU_ETOOBIG;
+  Dims d{};
+  d.o1 = m.nx1 > 1;
+  d.o2 = m.nx2 > 1;
+  d.o3 = m.nx3 > 1;
+  d.ndim = 1 + d.o2 + d.o3;
+  d.N1 = m.nx1 + 2 * m.ng * d.o1;
+  d.N2 = m.nx2 + 2 * m.ng * d.o2;
+  d.N3 = m.nx3 + 2 * m.ng * d.o3;
+  d.NB = (int)nb;
+  d.NF = pangu_num_fields(params);
+  d.is = m.ng * d.o1; d.ie = d.is + m.nx1 - 1;
+  d.js = m.ng * d.o2; d.je = d.js + m.nx2 - 1;
+  d.ks = m.ng * d.o3; d.ke = d.ks + m.nx3 - 1;
+  d.ncell = (long long)d.N1 * d.N2 * d.N3;
+  d.dx[0] = (m.x1max - m.x1min) / (double)(m.nbx1 * m.nx1);
+  d.dx[1] = (m.x2max - m.x2min) / (double)(m.nbx2 * m.nx2);
+  d.dx[2] = (m.x3max - m.x3min) / (double)(m.nbx3 * m.nx3);
+  // Device address of the scratch array, looked up once per device with that
+  // device current (the host-side name of a __device__ array is not a device
+  // address).
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return PANGU_ECUDA;
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return PANGU_EINVAL;
+  void *ptr = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+      if (cudaGetSymbolAddress(&g_noalloc_ptr[dev], g_noalloc_dtmin) != cudaSuccess) {
+        g_noalloc_ptr[dev] = nullptr;
+        return PANGU_ECUDA;
+      }
+    }
+    ptr = g_noalloc_ptr[dev];
+  }
+  unsigned long long *mins = static_cast<unsigned long long *>(ptr);
+  cudaStream_t s = S(stream);
+  // The array keeps the previous call's minima: reset them first.
+  k_dt_init<<<grid_for(3 * d.NB), kThreads, 0, s>>>(3 * d.NB, mins);
+  const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
+  const unsigned gx =
+      (unsigned)std::min<long long>((n / std::max(1, d.NB) + kThreads - 1) / kThreads, 592);
+  k_dt_reduce<<<dim3(std::max(1u, gx), d.NB), kThreads, 0, s>>>(d, params->cfl_number, alfven,
+                                                                 mins);
+  k_dt_finalize<<<1, 32, 0, s>>>(d.NB, mins, dt_out);
+  return check_launch();
 }
 
 int pangu_update_dt(pangu_engine *e, double *dt, const double *dt_est, double dt_factor,
