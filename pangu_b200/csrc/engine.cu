@@ -47,6 +47,10 @@ struct Dims {
   const double *t1;      // [NB][10][N1 + 1]
   const double *t2;      // [NB][12][N2 + 1]
   const double *origin;  // [NB][3]
+  // Static MKS/BL metric tables (built once per engine by k_build_tables):
+  // component planes of [NB][comp][N2][N1] (centres), [NB][comp][N2][N1+1]
+  // (x1 faces) and [NB][comp][N2+1][N1] (x2 faces); x3 faces use the centres.
+  const double *ctab, *f1tab, *f2tab;
 };
 
 struct pangu_engine {
@@ -54,6 +58,7 @@ struct pangu_engine {
   pangu_mesh m;
   Dims d;
   double *d_t1 = nullptr, *d_t2 = nullptr, *d_origin = nullptr;
+  double *d_ctab = nullptr, *d_f1tab = nullptr, *d_f2tab = nullptr;
   long long *d_xdst = nullptr, *d_xsrc = nullptr;
   long long nxch = 0;
   unsigned long long *d_cnt = nullptr;
@@ -125,37 +130,152 @@ __device__ __forceinline__ void gcov_at(const Dims &d, const pangu_params &p, in
   }
 }
 
+// ---------------------------------------------------------------------------
+// Static metric tables. The MKS and BL metrics depend on (x1, x2) only and not
+// on time, so ComputeMetricAtLocation (christoffel.h:53-62) and
+// ComputeChristoffelConnection (christoffel.h:74-148) are evaluated once per
+// (j, i) point by the dense reference arithmetic (k_build_tables) and stored:
+// the structurally non-zero entries of gcov and gcon (upper triangle), gdet,
+// sqrt|gdet|, the lapse 1/sqrt(-gcon00), a validity flag (0 where the
+// inversion is singular) and, at cell centres, the structurally non-zero
+// Christoffel symbols (symmetric in their lower indices). Loads reproduce
+// the dense values bit for bit.
+// ---------------------------------------------------------------------------
+struct TabLayout {
+  int nsym, nmet, nconn, ncen;
+  int sym[4][4];      // slot of g_rc (r, c symmetric), -1 if structurally zero
+  int conn[4][4][4];  // slot of Gamma^a_bc (b, c symmetric), -1 if zero
+};
+
+__host__ __device__ constexpr TabLayout tab_layout(int mt) {
+  TabLayout L{};
+  const Pattern pt = metric_pattern(mt);
+  int n = 0;
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) L.sym[r][c] = -1;
+  for (int r = 0; r < 4; ++r)
+    for (int c = r; c < 4; ++c)
+      if (pt.nz[r][c]) {
+        L.sym[r][c] = n;
+        L.sym[c][r] = n;
+        ++n;
+      }
+  L.nsym = n;
+  L.nmet = 2 * n + 4;
+  // derivative directions with non-zero metric derivatives
+  bool ddir[4] = {false, true, true, mt == CKS};
+  if (mt == MINKOWSKI) ddir[1] = ddir[2] = ddir[3] = false;
+  bool dg[4][4][4] = {};
+  for (int dd = 0; dd < 4; ++dd)
+    for (int r = 0; r < 4; ++r)
+      for (int c = 0; c < 4; ++c) dg[dd][r][c] = ddir[dd] && pt.nz[r][c];
+  int m = 0;
+  for (int a = 0; a < 4; ++a)
+    for (int j = 0; j < 4; ++j)
+      for (int k = 0; k < 4; ++k) L.conn[a][j][k] = -1;
+  for (int a = 0; a < 4; ++a)
+    for (int j = 0; j < 4; ++j)
+      for (int k = j; k < 4; ++k) {
+        bool nz = false;
+        for (int l = 0; l < 4; ++l)
+          nz = nz || (pt.nz[a][l] && (dg[j][l][k] || dg[k][l][j] || dg[l][j][k]));
+        if (nz) {
+          L.conn[a][j][k] = m;
+          L.conn[a][k][j] = m;
+          ++m;
+        }
+      }
+  L.nconn = m;
+  L.ncen = L.nmet + m;
+  return L;
+}
+
+template <int MT>
+__device__ __forceinline__ int load_geo(const double *__restrict__ tab, long long plane,
+                                        long long off, Geo &g) {
+  constexpr TabLayout L = tab_layout(MT);
+  double cov[L.nsym], con[L.nsym];
+#pragma unroll
+  for (int q = 0; q < L.nsym; ++q) {
+    cov[q] = __ldg(tab + off + q * plane);
+    con[q] = __ldg(tab + off + (L.nsym + q) * plane);
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      g.gcov[r][c] = L.sym[r][c] >= 0 ? cov[L.sym[r][c]] : 0.0;
+      g.gcon[r][c] = L.sym[r][c] >= 0 ? con[L.sym[r][c]] : 0.0;
+    }
+  g.gdet = __ldg(tab + off + (2 * L.nsym) * plane);
+  g.sg = __ldg(tab + off + (2 * L.nsym + 1) * plane);
+  g.alpha = __ldg(tab + off + (2 * L.nsym + 2) * plane);
+  return __ldg(tab + off + (2 * L.nsym + 3) * plane) != 0.0;
+}
+
+__device__ __forceinline__ void minkowski_geo(Geo &g) {
+  minkowski_gcov(g.gcov);
+  minkowski_gcov(g.gcon);
+  g.gdet = -1.0;
+  g.sg = 1.0;
+  g.alpha = 1.0;
+}
+
+// Dense reference arithmetic at an analytic point (CKS; table building).
+template <int MT>
+__device__ __forceinline__ int analytic_geo(const Dims &d, const pangu_params &p, int b, int i,
+                                            int q1, int j, int q2, const double x[4], Geo &g) {
+  gcov_at<MT>(d, p, b, i, q1, j, q2, x, g.gcov);
+  const int ok = gj_invert(g.gcov, g.gcon);
+  g.gdet = determinant(g.gcov);
+  g.sg = sqrt(fabs(g.gdet));
+  g.alpha = 1.0 / sqrt(-g.gcon[0][0]);
+  return ok;
+}
+
 // ComputeMetricAtLocation (christoffel.h:53-62) at cell centre (b, k, j, i).
 // Returns 0 if the metric is singular.
 template <int MT>
 __device__ __forceinline__ int cell_metric(const Dims &d, const pangu_params &p, int b, int k,
                                            int j, int i, Geo &g) {
-  double x[4] = {0.0, 0.0, 0.0, 0.0};
-  if (MT == CKS) {
-    x[1] = xc(d, b, 0, i);
-    x[2] = xc(d, b, 1, j);
-    x[3] = xc(d, b, 2, k);
+  if (MT == MKS || MT == BL) {
+    constexpr TabLayout L = tab_layout(MT);
+    const long long plane = (long long)d.N2 * d.N1;
+    return load_geo<MT>(d.ctab, plane, (long long)b * L.ncen * plane + (long long)j * d.N1 + i, g);
+  } else if (MT == CKS) {
+    const double x[4] = {0.0, xc(d, b, 0, i), xc(d, b, 1, j), xc(d, b, 2, k)};
+    return analytic_geo<MT>(d, p, b, i, 0, j, 0, x, g);
+  } else {
+    minkowski_geo(g);
+    return 1;
   }
-  gcov_at<MT>(d, p, b, i, 0, j, 0, x, g.gcov);
-  const int ok = gj_invert(g.gcov, g.gcon);
-  g.gdet = determinant(g.gcov);
-  return ok;
 }
 
 // Metric at the lower face of (b, k, j, i) along dir (1..3).
 template <int MT>
 __device__ __forceinline__ int face_metric(const Dims &d, const pangu_params &p, int dir, int b,
                                            int k, int j, int i, Geo &g) {
-  double x[4] = {0.0, 0.0, 0.0, 0.0};
-  if (MT == CKS) {
-    x[1] = dir == 1 ? xf(d, b, 0, i) : xc(d, b, 0, i);
-    x[2] = dir == 2 ? xf(d, b, 1, j) : xc(d, b, 1, j);
-    x[3] = dir == 3 ? xf(d, b, 2, k) : xc(d, b, 2, k);
+  if (MT == MKS || MT == BL) {
+    constexpr TabLayout L = tab_layout(MT);
+    if (dir == 1) {
+      const long long plane = (long long)d.N2 * (d.N1 + 1);
+      return load_geo<MT>(d.f1tab, plane,
+                          (long long)b * L.nmet * plane + (long long)j * (d.N1 + 1) + i, g);
+    } else if (dir == 2) {
+      const long long plane = (long long)(d.N2 + 1) * d.N1;
+      return load_geo<MT>(d.f2tab, plane, (long long)b * L.nmet * plane + (long long)j * d.N1 + i,
+                          g);
+    }
+    return cell_metric<MT>(d, p, b, k, j, i, g);  // independent of x3
+  } else if (MT == CKS) {
+    const double x[4] = {0.0, dir == 1 ? xf(d, b, 0, i) : xc(d, b, 0, i),
+                         dir == 2 ? xf(d, b, 1, j) : xc(d, b, 1, j),
+                         dir == 3 ? xf(d, b, 2, k) : xc(d, b, 2, k)};
+    return analytic_geo<MT>(d, p, b, i, 0, j, 0, x, g);
+  } else {
+    minkowski_geo(g);
+    return 1;
   }
-  gcov_at<MT>(d, p, b, i, dir == 1 ? 3 : 0, j, dir == 2 ? 3 : 0, x, g.gcov);
-  const int ok = gj_invert(g.gcov, g.gcon);
-  g.gdet = determinant(g.gcov);
-  return ok;
 }
 
 // Warp-aggregated increment of a hit counter.
@@ -228,7 +348,7 @@ __global__ void __launch_bounds__(kThreads) k_fix_primitive(Dims d, pangu_params
   load_prim(d, P, b, k, j, i, pc);
   const double rho = pc[RHO], ug = pc[ENY];
   State st;
-  calc_state(pc, g, st);
+  calc_state<MT>(pc, g, st);
   if (rho_floor < ug / sigma_max_safe) rho_floor = ug / sigma_max_safe;
   const double sigma = st.bsq / rho;
   if (sigma > p.sigma_max) rho_floor = st.bsq / sigma_max_safe;
@@ -239,8 +359,16 @@ __global__ void __launch_bounds__(kThreads) k_fix_primitive(Dims d, pangu_params
   if (hit_u) pu = eng_floor;
   double u1 = pc[UX1], u2 = pc[UX2], u3 = pc[UX3];
   const double umax2 = p.lorentz_max * p.lorentz_max - 1.0;
-  const double uvsq = g.gcov[1][1] * u1 * u1 + g.gcov[2][2] * u2 * u2 + g.gcov[3][3] * u3 * u3 +
-                      2.0 * (g.gcov[1][2] * u1 * u2 + g.gcov[1][3] * u1 * u3 + g.gcov[2][3] * u2 * u3);
+  // primitive_fixer.cc:131-134; structurally zero cross terms skipped
+  constexpr Pattern PT = metric_pattern(MT);
+  double uvsq = g.gcov[1][1] * u1 * u1 + g.gcov[2][2] * u2 * u2 + g.gcov[3][3] * u3 * u3;
+  if (PT.nz[1][2] || PT.nz[1][3] || PT.nz[2][3]) {
+    double cross = 0.0;
+    if (PT.nz[1][2]) cross = cross + g.gcov[1][2] * u1 * u2;
+    if (PT.nz[1][3]) cross = cross + g.gcov[1][3] * u1 * u3;
+    if (PT.nz[2][3]) cross = cross + g.gcov[2][3] * u2 * u3;
+    uvsq = uvsq + 2.0 * cross;
+  }
   const bool cap = umax2 > 0.0 && uvsq > umax2;
   if (cap) {
     const double f = sqrt(umax2 / kmax(uvsq, small));
@@ -287,99 +415,214 @@ __global__ void __launch_bounds__(kThreads) k_calc_cons(Dims d, pangu_params p, 
   double pc[NPRIM];
   load_prim(d, P, b, k, j, i, pc);
   State s;
-  calc_state(pc, g, s);
+  calc_state<MT>(pc, g, s);
   double f[NPRIM];
-  flux_from_state(p.adiabatic_index, pc, s, sqrt(fabs(g.gdet)), 0, f);
+  flux_from_state(p.adiabatic_index, pc, s, g.sg, 0, f);
 #pragma unroll
   for (int v = 0; v < NPRIM; ++v)
     if (d.pidx[v] >= 0) U[vidx(d, b, d.pidx[v], k, j, i)] = f[v];
 }
 
 // ---------------------------------------------------------------------------
-// CalculateLAXF / CalculateHLL, one direction (laxf.cc:78-181 and twins).
+// CalculateLAXF / CalculateHLL (laxf.cc:78-393, hll.cc:78-399).
+//
+// Each cell's reconstruction is computed once and shared by its two faces
+// (the reference calls MC/PPM4 twice per variable and face,
+// laxf.cc:86-105): x1 faces by warp shuffles, x2/x3 faces by marching along
+// the column. The Riemann flux is then assembled component by component
+// from the two states, in the reference's operation order.
 // ---------------------------------------------------------------------------
-template <int MT, int dir>
-__device__ __forceinline__ void k_flux_body(Dims d, pangu_params p, int k0, int k1,
-                                                   int j0, int j1, int i0, int i1, const double *P,
-                                                   double *F, double *alfven) {
-  int b, k, j, i;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (!box_index(t, d.NB, k0, k1, j0, j1, i0, i1, b, k, j, i)) return;
-  const int di = dir == 1, dj = dir == 2, dk = dir == 3;
-  const long long step = (long long)di + (long long)dj * d.N1 + (long long)dk * d.N1 * d.N2;
-  const bool use_mc = p.limiter == PANGU_LIMITER_MC;
-  double PL[NPRIM], PR[NPRIM];
-#pragma unroll
-  for (int s = 0; s < NPRIM; ++s) {
-    PL[s] = 0.0;
-    PR[s] = 0.0;
-    if (d.pidx[s] < 0) continue;
-    const double *q = P + vidx(d, b, d.pidx[s], k, j, i);
-    double dummy;
-    if (use_mc) {
-      const double qm2 = q[-2 * step], qm1 = q[-step], q0 = q[0], qp1 = q[step];
-      mc(qm2, qm1, q0, PL[s], dummy);
-      mc(qm1, q0, qp1, dummy, PR[s]);
-    } else {
-      const double qm3 = q[-3 * step], qm2 = q[-2 * step], qm1 = q[-step], q0 = q[0],
-                   qp1 = q[step], qp2 = q[2 * step];
-      ppm4(qm3, qm2, qm1, q0, qp1, PL[s], dummy);
-      ppm4(qm2, qm1, q0, qp1, qp2, dummy, PR[s]);
-    }
+
+// Reconstruction of one variable in cell q (stride s along the direction):
+// ql_ip1 = value at the upper face, qr_i = value at the lower face
+// (interpolater_mc.h:38-48, interpolater_ppm4.h:29-67).
+__device__ __forceinline__ void recon_cell(bool use_mc, const double *q, long long s,
+                                           double &ql_ip1, double &qr_i) {
+  if (use_mc) {
+    mc(q[-s], q[0], q[s], ql_ip1, qr_i);
+  } else {
+    ppm4(q[-2 * s], q[-s], q[0], q[s], q[2 * s], ql_ip1, qr_i);
   }
+}
+
+// One flux component from a state (contravariant_flux.h:12-39).
+template <int c>
+__device__ __forceinline__ double flux_component(double gam, const double P[NPRIM],
+                                                 const State &s, double sg, int dir) {
+  const double f_rho = P[RHO] * s.ucon[dir];
+  if (c == RHO) return f_rho * sg;
+  if (c == ENT) return (P[ENT] * f_rho) * sg;
+  if (c == KEL) return (P[KEL] * f_rho) * sg;
+  if (c >= BX1 && c <= BX3) {
+    const int m = c - BX1 + 1;
+    return SUB(MUL(s.bcon[m], s.ucon[dir]), MUL(s.bcon[dir], s.ucon[m])) * sg;
+  }
+  const double hh = P[RHO] + gam * P[ENY];
+  const double e_tot = hh + s.bsq;
+  const double p_tot = (gam - 1.) * P[ENY] + 0.5 * s.bsq;
+  const int m = (c == ENY) ? 0 : c - UX1 + 1;
+  const double t = e_tot * s.ucon[dir] * s.ucov[m] + p_tot * (dir == m) - s.bcon[dir] * s.bcov[m];
+  if (c == ENY) return (t + f_rho) * sg;
+  return t * sg;
+}
+
+// Riemann flux and fast speed at the lower face of (b, k, j, i) along DIR
+// from the left and right states.
+template <int MT, int DIR>
+__device__ __forceinline__ void face_flux(const Dims &d, const pangu_params &p, int b, int k, int j,
+                                          int i, const double PL[NPRIM], const double PR[NPRIM],
+                                          double *F, double *alfven) {
   Geo g;
   const long long fo = vidx(d, b, 0, k, j, i);
-  if (!face_metric<MT>(d, p, dir, b, k, j, i, g)) {
+  if (!face_metric<MT>(d, p, DIR, b, k, j, i, g)) {
     // Singular code metric (theta = 0 exactly on a polar face): zero flux,
     // zero speed (the reference reads an unwritten inverse here).
-    alfven[aidx(d, b, dir - 1, k, j, i)] = 0.0;
+    alfven[aidx(d, b, DIR - 1, k, j, i)] = 0.0;
 #pragma unroll
     for (int s = 0; s < NPRIM; ++s)
       if (d.pidx[s] >= 0) F[fo + d.pidx[s] * d.ncell] = 0.0;
     return;
   }
   const double gam = p.adiabatic_index;
-  const double sg = sqrt(fabs(g.gdet));
+  const double sg = g.sg;
   State sL, sR;
-  calc_state(PL, g, sL);
-  calc_state(PR, g, sR);
+  calc_state<MT>(PL, g, sL);
+  calc_state<MT>(PR, g, sR);
   double vmaxL, vminL, vmaxR, vminR;
-  fast_speed_from_state(gam, PL, g, sL, dir, vmaxL, vminL);
-  fast_speed_from_state(gam, PR, g, sR, dir, vmaxR, vminR);
+  fast_speed_from_state(gam, PL, g, sL, DIR, vmaxL, vminL);
+  fast_speed_from_state(gam, PR, g, sR, DIR, vmaxR, vminR);
   const double cmax = fabs(kmax(kmax(0., vmaxL), vmaxR));
   const double cmin = fabs(kmax(kmax(0., -vminL), -vminR));
   const double cms = kmax(cmax, cmin);
-  alfven[aidx(d, b, dir - 1, k, j, i)] = cms;
-  double UL[NPRIM], UR[NPRIM], FL[NPRIM], FR[NPRIM];
-  flux_from_state(gam, PL, sL, sg, 0, UL);
-  flux_from_state(gam, PR, sR, sg, 0, UR);
-  flux_from_state(gam, PL, sL, sg, dir, FL);
-  flux_from_state(gam, PR, sR, sg, dir, FR);
+  alfven[aidx(d, b, DIR - 1, k, j, i)] = cms;
   const bool hll = p.riemann_solver == PANGU_RIEMANN_HLL;
+#define PGD_FACE_COMPONENT(C)                                                         \
+  if (d.pidx[C] >= 0) {                                                               \
+    const double fl = flux_component<C>(gam, PL, sL, sg, DIR);                        \
+    const double fr = flux_component<C>(gam, PR, sR, sg, DIR);                        \
+    const double ul = flux_component<C>(gam, PL, sL, sg, 0);                          \
+    const double ur = flux_component<C>(gam, PR, sR, sg, 0);                          \
+    F[fo + d.pidx[C] * d.ncell] =                                                     \
+        hll ? (cmax * fl + cmin * fr - cmax * cmin * (ur - ul)) / (cmax + cmin + 1e-20) \
+            : 0.5 * (fl + fr - cms * (ur - ul));                                      \
+  }
+  PGD_FACE_COMPONENT(RHO)
+  PGD_FACE_COMPONENT(ENY)
+  PGD_FACE_COMPONENT(UX1)
+  PGD_FACE_COMPONENT(UX2)
+  PGD_FACE_COMPONENT(UX3)
+  PGD_FACE_COMPONENT(BX1)
+  PGD_FACE_COMPONENT(BX2)
+  PGD_FACE_COMPONENT(BX3)
+  PGD_FACE_COMPONENT(ENT)
+  PGD_FACE_COMPONENT(KEL)
+#undef PGD_FACE_COMPONENT
+}
+
+// x1 faces: a warp covers 31 consecutive faces of one row. Lane l
+// reconstructs cell c = f0 - 1 + l; face c takes its left state from lane
+// l - 1 (upper-face value of cell c - 1) and its right state from lane l.
+constexpr int kFacesPerWarp = 31;
+
+template <int MT>
+__global__ void __launch_bounds__(kThreads) k_flux_x1(Dims d, pangu_params p, int k0, int k1,
+                                                      int j0, int j1, int i0, int i1,
+                                                      const double *P, double *F,
+                                                      double *alfven) {
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int nf = i1 - i0 + 1;
+  const int nseg = (nf + kFacesPerWarp - 1) / kFacesPerWarp;
+  const long long nrow = (long long)(k1 - k0 + 1) * (j1 - j0 + 1);
+  if (warp >= nrow * d.NB * nseg) return;  // whole warps exit together
+  const int seg = (int)(warp % nseg);
+  const long long row = warp / nseg;
+  const int b = (int)(row / nrow);
+  const long long rr = row - (long long)b * nrow;
+  const int k = k0 + (int)(rr / (j1 - j0 + 1));
+  const int j = j0 + (int)(rr % (j1 - j0 + 1));
+  const int c = i0 - 1 + seg * kFacesPerWarp + lane;
+  const bool active = c <= i1;  // cell c is needed by face c (and c + 1)
+  const bool use_mc = p.limiter == PANGU_LIMITER_MC;
+  double PL[NPRIM], PR[NPRIM];
 #pragma unroll
   for (int s = 0; s < NPRIM; ++s) {
-    if (d.pidx[s] < 0) continue;
-    double fx;
-    if (hll)
-      fx = (cmax * FL[s] + cmin * FR[s] - cmax * cmin * (UR[s] - UL[s])) / (cmax + cmin + 1e-20);
-    else
-      fx = 0.5 * (FL[s] + FR[s] - cms * (UR[s] - UL[s]));
-    F[fo + d.pidx[s] * d.ncell] = fx;
+    double up = 0.0, lo = 0.0;
+    if (d.pidx[s] >= 0 && active)
+      recon_cell(use_mc, P + vidx(d, b, d.pidx[s], k, j, c), 1, up, lo);
+    PL[s] = __shfl_up_sync(0xffffffffu, up, 1);
+    PR[s] = lo;
+  }
+  if (lane == 0 || !active) return;
+  face_flux<MT, 1>(d, p, b, k, j, c, PL, PR, F, alfven);
+}
+
+// x2 / x3 faces: a thread marches over kMarch consecutive faces of one
+// column, carrying the upper-face value of the previous cell.
+constexpr int kMarch = 4;
+
+template <int MT, int DIR>
+__device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_params &p, int k0,
+                                                int k1, int j0, int j1, int i0, int i1,
+                                                const double *P, double *F, double *alfven) {
+  // the marching index is j (DIR 2) or k (DIR 3); the other two form the column
+  const int m0 = DIR == 2 ? j0 : k0, m1 = DIR == 2 ? j1 : k1;
+  const int a0 = DIR == 2 ? k0 : j0, a1 = DIR == 2 ? k1 : j1;  // outer transverse index
+  const int ni = i1 - i0 + 1, na = a1 - a0 + 1;
+  const int nruns = (m1 - m0 + 1 + kMarch - 1) / kMarch;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)d.NB * na * nruns * ni) return;
+  const int i = i0 + (int)(t % ni);
+  long long r = t / ni;
+  const int run = (int)(r % nruns);
+  r /= nruns;
+  const int a = a0 + (int)(r % na);
+  const int b = (int)(r / na);
+  const long long stride = DIR == 2 ? (long long)d.N1 : (long long)d.N1 * d.N2;
+  const bool use_mc = p.limiter == PANGU_LIMITER_MC;
+  const int f0 = m0 + run * kMarch;
+  const int f1 = min(f0 + kMarch - 1, m1);
+  double carry[NPRIM];
+  {
+    const int c = f0 - 1;
+    const int kk = DIR == 2 ? a : c, jj = DIR == 2 ? c : a;
+#pragma unroll
+    for (int s = 0; s < NPRIM; ++s) {
+      double up = 0.0, lo;
+      if (d.pidx[s] >= 0) recon_cell(use_mc, P + vidx(d, b, d.pidx[s], kk, jj, i), stride, up, lo);
+      carry[s] = up;
+    }
+  }
+  for (int f = f0; f <= f1; ++f) {
+    const int kk = DIR == 2 ? a : f, jj = DIR == 2 ? f : a;
+    double PR[NPRIM], up[NPRIM];
+#pragma unroll
+    for (int s = 0; s < NPRIM; ++s) {
+      up[s] = 0.0;
+      PR[s] = 0.0;
+      if (d.pidx[s] >= 0)
+        recon_cell(use_mc, P + vidx(d, b, d.pidx[s], kk, jj, i), stride, up[s], PR[s]);
+    }
+    face_flux<MT, DIR>(d, p, b, kk, jj, i, carry, PR, F, alfven);
+#pragma unroll
+    for (int s = 0; s < NPRIM; ++s) carry[s] = up[s];
   }
 }
 
-// Direction-specialised entry points (the direction indexes register arrays).
-#define PGD_FLUX_DIR(NAME, DIR)                                                              \
-  template <int MT>                                                                          \
-  __global__ void __launch_bounds__(kThreads)                                                \
-      NAME(Dims d, pangu_params p, int k0, int k1, int j0, int j1, int i0, int i1,            \
-           const double *P, double *F, double *alfven) {                                     \
-    k_flux_body<MT, DIR>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);                        \
-  }
-PGD_FLUX_DIR(k_flux1, 1)
-PGD_FLUX_DIR(k_flux2, 2)
-PGD_FLUX_DIR(k_flux3, 3)
-#undef PGD_FLUX_DIR
+template <int MT>
+__global__ void __launch_bounds__(kThreads) k_flux_march2(Dims d, pangu_params p, int k0, int k1,
+                                                          int j0, int j1, int i0, int i1,
+                                                          const double *P, double *F,
+                                                          double *alfven) {
+  flux_march_body<MT, 2>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
+}
+template <int MT>
+__global__ void __launch_bounds__(kThreads) k_flux_march3(Dims d, pangu_params p, int k0, int k1,
+                                                          int j0, int j1, int i0, int i1,
+                                                          const double *P, double *F,
+                                                          double *alfven) {
+  flux_march_body<MT, 3>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
+}
 
 // ---------------------------------------------------------------------------
 // ConstraintedTransport (constrained_transport.cc:13-130).
@@ -538,27 +781,103 @@ __global__ void __launch_bounds__(kThreads) k_source(Dims d, pangu_params p, con
   if (MT == MINKOWSKI) return;  // connection identically zero (christoffel.h:90)
   Geo g;
   cell_metric<MT>(d, p, b, k, j, i, g);
-  const double sg = sqrt(fabs(g.gdet));
-  double conn[4][4][4];
-  christoffel<MT>(d, p, b, k, j, i, g, conn);
+  const double sg = g.sg;
   double pc[NPRIM];
   load_prim(d, P, b, k, j, i, pc);
   State s;
-  calc_state(pc, g, s);
+  calc_state<MT>(pc, g, s);
   double T[4][4];
 #pragma unroll
   for (int r = 0; r < 4; ++r) emt_from_state(p.adiabatic_index, pc, s, r, T[r]);
   const double bdt = beta * (*dt);
+  if (MT == MKS || MT == BL) {
+    // Christoffel symbols from the centre table; structural zeros skipped
+    constexpr TabLayout L = tab_layout(MT);
+    const long long plane = (long long)d.N2 * d.N1;
+    const double *cn = d.ctab + (long long)b * L.ncen * plane + (long long)j * d.N1 + i +
+                       (long long)L.nmet * plane;
 #pragma unroll
-  for (int dir = 0; dir < 4; ++dir) {
-    double con = 0.0;
+    for (int dir = 0; dir < 4; ++dir) {
+      double con = 0.0;
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
+      for (int r = 0; r < 4; ++r)
 #pragma unroll
-      for (int c = 0; c < 4; ++c) con += T[r][c] * conn[c][dir][r];
-    const int v = dir == 0 ? d.pidx[ENY] : d.pidx[UX1] + dir - 1;
-    const long long q = vidx(d, b, v, k, j, i);
-    U[q] += con * sg * bdt;
+        for (int c = 0; c < 4; ++c)
+          if (L.conn[c][dir][r] >= 0) con += T[r][c] * __ldg(cn + L.conn[c][dir][r] * plane);
+      const int v = dir == 0 ? d.pidx[ENY] : d.pidx[UX1] + dir - 1;
+      const long long q = vidx(d, b, v, k, j, i);
+      U[q] += con * sg * bdt;
+    }
+  } else {
+    double conn[4][4][4];
+    christoffel<MT>(d, p, b, k, j, i, g, conn);
+#pragma unroll
+    for (int dir = 0; dir < 4; ++dir) {
+      double con = 0.0;
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) con += T[r][c] * conn[c][dir][r];
+      const int v = dir == 0 ? d.pidx[ENY] : d.pidx[UX1] + dir - 1;
+      const long long q = vidx(d, b, v, k, j, i);
+      U[q] += con * sg * bdt;
+    }
+  }
+}
+
+// Builds the static metric tables of an MKS or BL engine with the dense
+// reference arithmetic (one thread per table point).
+template <int MT>
+__global__ void __launch_bounds__(kThreads) k_build_tables(Dims d, pangu_params p, double *ctab,
+                                                           double *f1tab, double *f2tab) {
+  constexpr TabLayout L = tab_layout(MT);
+  const long long pc = (long long)d.N2 * d.N1, p1 = (long long)d.N2 * (d.N1 + 1),
+                  p2 = (long long)(d.N2 + 1) * d.N1;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long per = pc + p1 + p2;
+  if (t >= per * d.NB) return;
+  const int b = (int)(t / per);
+  t -= (long long)b * per;
+  int which, W;
+  long long plane;
+  double *tab;
+  int nc;
+  if (t < pc) {
+    which = 0, W = d.N1, plane = pc, tab = ctab, nc = L.ncen;
+  } else if (t < pc + p1) {
+    t -= pc;
+    which = 1, W = d.N1 + 1, plane = p1, tab = f1tab, nc = L.nmet;
+  } else {
+    t -= pc + p1;
+    which = 2, W = d.N1, plane = p2, tab = f2tab, nc = L.nmet;
+  }
+  const int j = (int)(t / W), i = (int)(t % W);
+  const double x[4] = {0.0, 0.0, 0.0, 0.0};
+  Geo g;
+  const int ok = analytic_geo<MT>(d, p, b, i, which == 1 ? 3 : 0, j, which == 2 ? 3 : 0, x, g);
+  double *o = tab + (long long)b * nc * plane + t;
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = r; c < 4; ++c)
+      if (L.sym[r][c] >= 0) {
+        o[L.sym[r][c] * plane] = g.gcov[r][c];
+        o[(L.nsym + L.sym[r][c]) * plane] = g.gcon[r][c];
+      }
+  o[(2 * L.nsym) * plane] = g.gdet;
+  o[(2 * L.nsym + 1) * plane] = g.sg;
+  o[(2 * L.nsym + 2) * plane] = g.alpha;
+  o[(2 * L.nsym + 3) * plane] = ok ? 1.0 : 0.0;
+  if (which == 0) {
+    double conn[4][4][4];
+    christoffel<MT>(d, p, b, 0, j, i, g, conn);
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+        for (int kk = jj; kk < 4; ++kk)
+          if (L.conn[a][jj][kk] >= 0) o[(L.nmet + L.conn[a][jj][kk]) * plane] = conn[a][jj][kk];
   }
 }
 
@@ -589,8 +908,8 @@ __global__ void __launch_bounds__(kThreads) k_recovery(Dims d, pangu_params p, d
   Geo g;
   cell_metric<MT>(d, p, b, k, j, i, g);
   if (!robuster) flag[fc] = 0;
-  const double sg = sqrt(fabs(g.gdet));
-  const double alpha = 1.0 / sqrt(-g.gcon[0][0]);
+  const double sg = g.sg;
+  const double alpha = g.alpha;
   const long long q = vidx(d, b, 0, k, j, i);
   const long long vs = d.ncell;
   double C[9], Pp[9];
@@ -625,14 +944,14 @@ __global__ void __launch_bounds__(kThreads) k_recovery(Dims d, pangu_params p, d
     if (st != 0) return;
   } else {
     Harm hs;
-    harm_setup(UH, g, hs);
-    int ok = invert_2d(UH, PH, gam, g, hs) == 0;
+    harm_setup<MT>(UH, g, hs);
+    int ok = invert_2d<MT>(UH, PH, gam, g, hs) == 0;
     count(cnt, PANGU_CNT_C2P_2D, ok);
     if (!ok) {
-      ok = invert_1dvsq(UH, PH, gam, g, hs) == 0;
+      ok = invert_1dvsq<MT>(UH, PH, gam, g, hs) == 0;
       count(cnt, PANGU_CNT_C2P_1DVSQ, ok);
       if (!ok) {
-        ok = invert_1d(UH, PH, gam, g, hs) == 0;
+        ok = invert_1d<MT>(UH, PH, gam, g, hs) == 0;
         count(cnt, PANGU_CNT_C2P_1D, ok);
         count(cnt, PANGU_CNT_C2P_FAIL, !ok);
       }
@@ -660,7 +979,7 @@ __global__ void __launch_bounds__(kThreads) k_heating(Dims d, pangu_params p, do
   double pc[NPRIM];
   load_prim(d, P, b, k, j, i, pc);
   State s;
-  calc_state(pc, g, s);
+  calc_state<MT>(pc, g, s);
   const long long q = vidx(d, b, 0, k, j, i);
   const long long vs = d.ncell;
   const double cr = U[q];
@@ -925,12 +1244,18 @@ int run_fluxes(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
       if (hll) { j0 = d.js; j1 = d.je; i0 = d.is; i1 = d.ie; }
     }
     double *F = dir == 1 ? md->flux1 : (dir == 2 ? md->flux2 : md->flux3);
-    const long long n = box_count(d.NB, k0, k1, j0, j1, i0, i1);
-    const unsigned g = grid_for(n);
 #define FLUX_ARGS d, e->p, k0, k1, j0, j1, i0, i1, md->prim, F, md->alfven
-    if (dir == 1) DISPATCH_MT(e->p.metric_type, k_flux1, g, s, FLUX_ARGS);
-    else if (dir == 2) DISPATCH_MT(e->p.metric_type, k_flux2, g, s, FLUX_ARGS);
-    else DISPATCH_MT(e->p.metric_type, k_flux3, g, s, FLUX_ARGS);
+    if (dir == 1) {
+      const int nseg = (i1 - i0 + 1 + kFacesPerWarp - 1) / kFacesPerWarp;
+      const long long warps = (long long)d.NB * (k1 - k0 + 1) * (j1 - j0 + 1) * nseg;
+      DISPATCH_MT(e->p.metric_type, k_flux_x1, grid_for(32 * warps), s, FLUX_ARGS);
+    } else {
+      const int m = dir == 2 ? (j1 - j0 + 1) : (k1 - k0 + 1);
+      const int na = dir == 2 ? (k1 - k0 + 1) : (j1 - j0 + 1);
+      const long long n = (long long)d.NB * na * ((m + kMarch - 1) / kMarch) * (i1 - i0 + 1);
+      if (dir == 2) DISPATCH_MT(e->p.metric_type, k_flux_march2, grid_for(n), s, FLUX_ARGS);
+      else DISPATCH_MT(e->p.metric_type, k_flux_march3, grid_for(n), s, FLUX_ARGS);
+    }
 #undef FLUX_ARGS
     ++e->launches;
     const int rc = check_launch();
@@ -1070,6 +1395,9 @@ int pangu_num_fields(const pangu_params *p) {
 int pangu_engine_destroy(pangu_engine *e) {
   if (!e) return PANGU_EINVAL;
   cudaFree(e->d_t1);
+  cudaFree(e->d_ctab);
+  cudaFree(e->d_f1tab);
+  cudaFree(e->d_f2tab);
   cudaFree(e->d_t2);
   cudaFree(e->d_origin);
   cudaFree(e->d_xdst);
@@ -1167,6 +1495,32 @@ int pangu_engine_create(const pangu_params *params, const pangu_mesh *mesh, pang
   d.t1 = e->d_t1;
   d.t2 = e->d_t2;
   d.origin = e->d_origin;
+  d.ctab = d.f1tab = d.f2tab = nullptr;
+  if (p.metric_type == PANGU_METRIC_MKS || p.metric_type == PANGU_METRIC_BL) {
+    const TabLayout L = p.metric_type == PANGU_METRIC_MKS ? tab_layout(MKS) : tab_layout(BL);
+    const size_t pc = (size_t)d.N2 * d.N1, p1 = (size_t)d.N2 * (d.N1 + 1),
+                 p2 = (size_t)(d.N2 + 1) * d.N1;
+    int rc2 = PANGU_OK;
+    rc2 |= dalloc(&e->d_ctab, (size_t)d.NB * L.ncen * pc);
+    rc2 |= dalloc(&e->d_f1tab, (size_t)d.NB * L.nmet * p1);
+    rc2 |= dalloc(&e->d_f2tab, (size_t)d.NB * L.nmet * p2);
+    if (rc2 != PANGU_OK) {
+      pangu_engine_destroy(e);
+      return PANGU_ENOMEM;
+    }
+    const long long n = (long long)d.NB * (pc + p1 + p2);
+    if (p.metric_type == PANGU_METRIC_MKS)
+      k_build_tables<MKS><<<grid_for(n), kThreads>>>(d, p, e->d_ctab, e->d_f1tab, e->d_f2tab);
+    else
+      k_build_tables<BL><<<grid_for(n), kThreads>>>(d, p, e->d_ctab, e->d_f1tab, e->d_f2tab);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+      pangu_engine_destroy(e);
+      return PANGU_ECUDA;
+    }
+    d.ctab = e->d_ctab;
+    d.f1tab = e->d_f1tab;
+    d.f2tab = e->d_f2tab;
+  }
   *out = e;
   return PANGU_OK;
 }

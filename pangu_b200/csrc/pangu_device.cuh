@@ -35,6 +35,8 @@ struct Geo {
   double gcov[4][4];
   double gcon[4][4];
   double gdet;
+  double sg;     // sqrt(|gdet|), as every reference task computes it
+  double alpha;  // 1 / sqrt(-gcon[0][0]), as state_calculation.h:24 computes it
 };
 
 // Coordinate values along x1 and x2 that fully determine the MKS / BL
@@ -201,6 +203,152 @@ PGD double determinant(const double m[4][4]) {
 }
 
 // ---------------------------------------------------------------------------
+// Structural zeros of the code metrics. The MKS and BL metrics couple only
+// (t, r, phi) with theta apart, and the Minkowski metric is diagonal; their
+// zero entries are exact zeros by construction (ks_code_gcov, bl_code_gcov).
+// Operations on a structural zero change at most the sign of a zero result,
+// so skipping them leaves every non-zero value bit-identical to the dense
+// computation of the reference.
+// ---------------------------------------------------------------------------
+struct Pattern {
+  bool nz[4][4];
+};
+__host__ __device__ constexpr Pattern metric_pattern(int mt) {
+  Pattern p{};
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) {
+      if (mt == MKS) {
+        const bool tr = (r != 2), tc = (c != 2);
+        p.nz[r][c] = (tr && tc) || (r == 2 && c == 2);
+      } else if (mt == BL) {
+        p.nz[r][c] = (r == c) || (r == 0 && c == 3) || (r == 3 && c == 0);
+      } else if (mt == MINKOWSKI) {
+        p.nz[r][c] = (r == c);
+      } else {
+        p.nz[r][c] = true;
+      }
+    }
+  return p;
+}
+
+// Fill pattern of the Gauss-Jordan elimination of tensor_algebra.h:71-124:
+// a[i][r][c] is true when entry (r, c) of the augmented matrix may be
+// non-zero before pivot step i. After step i, column i of every other row is
+// exactly zero (x - x * 1).
+struct GJPlan {
+  bool a[4][4][8];
+};
+__host__ __device__ constexpr GJPlan gj_plan(int mt) {
+  GJPlan P{};
+  bool cur[4][8] = {};
+  const Pattern pt = metric_pattern(mt);
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) {
+      cur[r][c] = pt.nz[r][c];
+      cur[r][c + 4] = (r == c);
+    }
+  for (int i = 0; i < 4; ++i) {
+    for (int r = 0; r < 4; ++r)
+      for (int c = 0; c < 8; ++c) P.a[i][r][c] = cur[r][c];
+    bool prow[8] = {};
+    for (int c = 0; c < 8; ++c) prow[c] = cur[i][c];
+    for (int j = 0; j < 4; ++j) {
+      if (j == i || !cur[j][i]) continue;
+      for (int c = 0; c < 8; ++c) cur[j][c] = cur[j][c] || prow[c];
+      cur[j][i] = false;
+    }
+  }
+  return P;
+}
+
+// Gauss-Jordan inverse restricted to the fill pattern of metric type MT.
+// A pivot that is exactly zero needs the reference's row swap: the dense
+// routine then redoes the inversion from scratch.
+template <int MT>
+PGD int gj_invert_s(const double m[4][4], double inv[4][4]) {
+  constexpr GJPlan P = gj_plan(MT);
+  double aug[4][8];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      aug[i][j] = m[i][j];
+      aug[i][j + 4] = (i == j) ? 1.0 : 0.0;
+    }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const double piv = aug[i][i];
+    if (piv == 0.0) return gj_invert(m, inv);
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+      if (P.a[i][i][c]) aug[i][c] = DIV(aug[i][c], piv);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if (j == i || !P.a[i][j][i]) continue;
+      const double f = aug[j][i];
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        if (P.a[i][i][c]) aug[j][c] = SUB(aug[j][c], MUL(f, aug[i][c]));
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) inv[i][j] = aug[i][j + 4];
+  return 1;
+}
+
+// The cofactor determinant of tensor_algebra.h:39-69 with the structural
+// zeros of MT folded away at compile time: Zr stands for a value known to be
+// a (signed) zero, and the operator overloads return what the dense
+// arithmetic returns for it (x - 0 = x, 0 - x = -x, 0 * x = 0).
+struct Zr {};
+PGD double op_mul(double a, double b) { return MUL(a, b); }
+PGD Zr op_mul(Zr, double) { return {}; }
+PGD Zr op_mul(double, Zr) { return {}; }
+PGD Zr op_mul(Zr, Zr) { return {}; }
+PGD double op_sub(double a, double b) { return SUB(a, b); }
+PGD double op_sub(double a, Zr) { return a; }
+PGD double op_sub(Zr, double b) { return -b; }
+PGD Zr op_sub(Zr, Zr) { return {}; }
+PGD double op_add(double a, double b) { return ADD(a, b); }
+PGD double op_add(double a, Zr) { return a; }
+PGD double op_add(Zr, double b) { return b; }
+PGD Zr op_add(Zr, Zr) { return {}; }
+PGD double to_double(double a) { return a; }
+PGD double to_double(Zr) { return 0.0; }
+
+template <int MT, int r, int c>
+PGD auto el(const double (&m)[4][4]) {
+  if constexpr (metric_pattern(MT).nz[r][c]) {
+    return m[r][c];
+  } else {
+    return Zr{};
+  }
+}
+
+template <int MT>
+PGD double determinant_s(const double (&m)[4][4]) {
+#define E(r, c) el<MT, r, c>(m)
+#define D2(a, b, c, d) op_sub(op_mul(a, b), op_mul(c, d))
+  const auto t0 = op_mul(E(0, 0), op_add(op_sub(op_mul(E(1, 1), D2(E(2, 2), E(3, 3), E(2, 3), E(3, 2))),
+                                                op_mul(E(1, 2), D2(E(2, 1), E(3, 3), E(2, 3), E(3, 1)))),
+                                         op_mul(E(1, 3), D2(E(2, 1), E(3, 2), E(2, 2), E(3, 1)))));
+  const auto t1 = op_mul(E(0, 1), op_add(op_sub(op_mul(E(1, 0), D2(E(2, 2), E(3, 3), E(2, 3), E(3, 2))),
+                                                op_mul(E(1, 2), D2(E(2, 0), E(3, 3), E(2, 3), E(3, 0)))),
+                                         op_mul(E(1, 3), D2(E(2, 0), E(3, 2), E(2, 2), E(3, 0)))));
+  const auto t2 = op_mul(E(0, 2), op_add(op_sub(op_mul(E(1, 0), D2(E(2, 1), E(3, 3), E(2, 3), E(3, 1))),
+                                                op_mul(E(1, 1), D2(E(2, 0), E(3, 3), E(2, 3), E(3, 0)))),
+                                         op_mul(E(1, 3), D2(E(2, 0), E(3, 1), E(2, 1), E(3, 0)))));
+  const auto t3 = op_mul(E(0, 3), op_add(op_sub(op_mul(E(1, 0), D2(E(2, 1), E(3, 2), E(2, 2), E(3, 1))),
+                                                op_mul(E(1, 1), D2(E(2, 0), E(3, 2), E(2, 2), E(3, 0)))),
+                                         op_mul(E(1, 2), D2(E(2, 0), E(3, 1), E(2, 1), E(3, 0)))));
+#undef D2
+#undef E
+  return to_double(op_sub(op_add(op_sub(t0, t1), t2), t3));
+}
+
+// ---------------------------------------------------------------------------
 // physics/ (state_calculation.h, energy_momentum_tensor.h,
 // contravariant_flux.h, fast_magnetosonic_speed.h)
 // ---------------------------------------------------------------------------
@@ -208,22 +356,30 @@ struct State {
   double ucon[4], ucov[4], bcon[4], bcov[4], bsq;
 };
 
+template <int MT>
 PGD void calc_state(const double P[NPRIM], const Geo &g, State &s) {
-  const double alpha = 1.0 / sqrt(-g.gcon[0][0]);
-  const double u1 = P[UX1], u2 = P[UX2], u3 = P[UX3];
-  const double sq = u1 * g.gcov[1][1] * u1 + u1 * g.gcov[1][2] * u2 + u1 * g.gcov[1][3] * u3 +
-                    u2 * g.gcov[2][1] * u1 + u2 * g.gcov[2][2] * u2 + u2 * g.gcov[2][3] * u3 +
-                    u3 * g.gcov[3][1] * u1 + u3 * g.gcov[3][2] * u2 + u3 * g.gcov[3][3] * u3;
+  constexpr Pattern PT = metric_pattern(MT);
+  const double alpha = g.alpha;
+  const double u[3] = {P[UX1], P[UX2], P[UX3]};
+  // 1 + gamma_ij u^i u^j, summed left to right over (i, j) as square3 does
+  // (tensor_algebra.h:18-37); structurally zero terms are skipped.
+  double sq = 0.0;
+#pragma unroll
+  for (int i = 1; i < 4; ++i)
+#pragma unroll
+    for (int j = 1; j < 4; ++j)
+      if (PT.nz[i][j]) sq = sq + u[i - 1] * g.gcov[i][j] * u[j - 1];
   const double lor = sqrt(1.0 + sq);
   s.ucon[0] = lor / alpha;
-  s.ucon[1] = u1 - s.ucon[0] * g.gcon[0][1] * alpha * alpha;
-  s.ucon[2] = u2 - s.ucon[0] * g.gcon[0][2] * alpha * alpha;
-  s.ucon[3] = u3 - s.ucon[0] * g.gcon[0][3] * alpha * alpha;
+#pragma unroll
+  for (int i = 1; i < 4; ++i)
+    s.ucon[i] = PT.nz[0][i] ? u[i - 1] - s.ucon[0] * g.gcon[0][i] * alpha * alpha : u[i - 1];
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
     double v = 0.0;
 #pragma unroll
-    for (int c = 0; c < 4; ++c) v += g.gcov[r][c] * s.ucon[c];
+    for (int c = 0; c < 4; ++c)
+      if (PT.nz[r][c]) v += g.gcov[r][c] * s.ucon[c];
     s.ucov[r] = v;
   }
   s.bcon[0] = P[BX1] * s.ucov[1] + P[BX2] * s.ucov[2] + P[BX3] * s.ucov[3];
@@ -234,7 +390,8 @@ PGD void calc_state(const double P[NPRIM], const Geo &g, State &s) {
   for (int r = 0; r < 4; ++r) {
     double v = 0.0;
 #pragma unroll
-    for (int c = 0; c < 4; ++c) v += g.gcov[r][c] * s.bcon[c];
+    for (int c = 0; c < 4; ++c)
+      if (PT.nz[r][c]) v += g.gcov[r][c] * s.bcon[c];
     s.bcov[r] = v;
   }
   s.bsq = s.bcon[0] * s.bcov[0] + s.bcon[1] * s.bcov[1] + s.bcon[2] * s.bcov[2] +
@@ -366,7 +523,11 @@ struct Harm {
   double Bsq, QdotB, QdotBsq, Qdotn, Qsq, Qtsq, D;
 };
 
+// Bcon[0] = 0 and the structural zeros of the metric contribute signed
+// zeros only; they are skipped.
+template <int MT>
 PGD void harm_setup(const double U[9], const Geo &g, Harm &s) {
+  constexpr Pattern PT = metric_pattern(MT);
   s.Bcon[0] = 0.;
   s.Bcon[1] = U[BX1];
   s.Bcon[2] = U[BX2];
@@ -376,7 +537,8 @@ PGD void harm_setup(const double U[9], const Geo &g, Harm &s) {
   for (int i = 0; i < 4; i++) {
     double v = 0.0;
 #pragma unroll
-    for (int j = 0; j < 4; j++) v += g.gcov[i][j] * s.Bcon[j];
+    for (int j = 1; j < 4; j++)
+      if (PT.nz[i][j]) v += g.gcov[i][j] * s.Bcon[j];
     Bcov[i] = v;
   }
   const double Qcov[4] = {U[ENY], U[UX1], U[UX2], U[UX3]};
@@ -384,38 +546,44 @@ PGD void harm_setup(const double U[9], const Geo &g, Harm &s) {
   for (int i = 0; i < 4; i++) {
     double v = 0.0;
 #pragma unroll
-    for (int j = 0; j < 4; j++) v += g.gcon[i][j] * Qcov[j];
+    for (int j = 0; j < 4; j++)
+      if (PT.nz[i][j]) v += g.gcon[i][j] * Qcov[j];
     s.Qcon[i] = v;
   }
   s.Bsq = s.Bcon[1] * Bcov[1] + s.Bcon[2] * Bcov[2] + s.Bcon[3] * Bcov[3];
-  s.QdotB = Qcov[0] * s.Bcon[0] + Qcov[1] * s.Bcon[1] + Qcov[2] * s.Bcon[2] + Qcov[3] * s.Bcon[3];
+  s.QdotB = Qcov[1] * s.Bcon[1] + Qcov[2] * s.Bcon[2] + Qcov[3] * s.Bcon[3];
   s.QdotBsq = s.QdotB * s.QdotB;
   const double lapse = sqrt(-1.0 / g.gcon[0][0]);
   const double n0 = -lapse;
 #pragma unroll
-  for (int i = 0; i < 4; i++) s.ncon[i] = g.gcon[i][0] * n0;
+  for (int i = 0; i < 4; i++) s.ncon[i] = PT.nz[i][0] ? g.gcon[i][0] * n0 : 0.0;
   s.Qdotn = s.Qcon[0] * n0;
   s.Qsq = Qcov[0] * s.Qcon[0] + Qcov[1] * s.Qcon[1] + Qcov[2] * s.Qcon[2] + Qcov[3] * s.Qcon[3];
   s.Qtsq = s.Qsq + s.Qdotn * s.Qdotn;
   s.D = U[RHO];
 }
 
+template <int MT>
 PGD bool harm_utsq(const double prim[9], const Geo &g, double &utsq) {
+  constexpr Pattern PT = metric_pattern(MT);
   const double u[3] = {prim[UX1], prim[UX2], prim[UX3]};
   double v = 0.;
 #pragma unroll
   for (int i = 1; i < 4; i++)
 #pragma unroll
-    for (int j = 1; j < 4; j++) v += g.gcov[i][j] * u[i - 1] * u[j - 1];
+    for (int j = 1; j < 4; j++)
+      if (PT.nz[i][j]) v += g.gcov[i][j] * u[i - 1] * u[j - 1];
   if ((v < 0.) && (fabs(v) < 1.0e-13)) v = fabs(v);
   utsq = v;
   return !(v < 0. || v > UTSQ_TOO_BIG);
 }
 
+template <int MT>
 PGD void harm_velocity(const Harm &s, double Gamma, double W, double prim[9]) {
+  constexpr Pattern PT = metric_pattern(MT);
 #pragma unroll
   for (int i = 1; i < 4; i++) {
-    const double qt = s.Qcon[i] + s.ncon[i] * s.Qdotn;
+    const double qt = PT.nz[i][0] ? s.Qcon[i] + s.ncon[i] * s.Qdotn : s.Qcon[i];
     prim[UX1 + i - 1] = Gamma / (W + s.Bsq) * (qt + s.QdotB * s.Bcon[i] / W);
   }
 }
@@ -432,10 +600,11 @@ PGD bool w_too_small(double W, double Bsq, double QdotBsq, double Qtsq) {
 
 // Scheme2D::invert (scheme_2d.h:257-404) with general_newton_raphson
 // (:158-255) and func_vsq (:99-156).
+template <int MT>
 PGD int invert_2d(const double U[9], double prim[9], double g, const Geo &geo,
                   const Harm &s) {
   double utsq;
-  if (!harm_utsq(prim, geo, utsq)) return 2;
+  if (!harm_utsq<MT>(prim, geo, utsq)) return 2;
   const double gammasq = 1. + utsq;
   double Gamma = sqrt(gammasq);
   double rho0 = s.D / Gamma;
@@ -513,7 +682,7 @@ PGD int invert_2d(const double U[9], double prim[9], double g, const Geo &geo,
   prim[RHO] = rho0;
   prim[ENY] = uu;
   prim[ENT] = (g - 1.) * uu * pgm::pow(rho0, -g);
-  harm_velocity(s, Gamma, W, prim);
+  harm_velocity<MT>(s, Gamma, W, prim);
   return 0;
 }
 
@@ -527,12 +696,13 @@ PGD double w_of_vsq(double D, double K, double vsq, double g, double &p, double 
   return ((rho + uu + p) / gtmp);
 }
 
+template <int MT>
 PGD int invert_1dvsq(const double U[9], double prim[9], double g, const Geo &geo,
                      const Harm &s) {
   (void)U;
   const double K = prim[ENT];
   double utsq;
-  if (!harm_utsq(prim, geo, utsq)) return 2;
+  if (!harm_utsq<MT>(prim, geo, utsq)) return 2;
   const double gammasq = 1. + utsq;
   double x = 1. - 1. / gammasq;
   const double Bsq = s.Bsq, QdotBsq = s.QdotBsq, Qtsq = s.Qtsq, D = s.D;
@@ -582,16 +752,17 @@ PGD int invert_1dvsq(const double U[9], double prim[9], double g, const Geo &geo
   prim[RHO] = rho0;
   prim[ENY] = uu;
   prim[ENT] = (g - 1.) * uu * pgm::pow(rho0, -g);
-  harm_velocity(s, Gamma, Wf, prim);
+  harm_velocity<MT>(s, Gamma, Wf, prim);
   return 0;
 }
 
 // Scheme1D::invert (scheme_1d.h:411-568) with func_1d_orig2 (:376-409).
+template <int MT>
 PGD int invert_1d(const double U[9], double prim[9], double g, const Geo &geo, const Harm &s) {
   (void)U;
   const double K = prim[ENT];
   double utsq;
-  if (!harm_utsq(prim, geo, utsq)) return 2;
+  if (!harm_utsq<MT>(prim, geo, utsq)) return 2;
   const double uvsq = 1. + utsq;
   double Gamma = sqrt(uvsq);
   const double Bsq = s.Bsq, QdotBsq = s.QdotBsq, Qtsq = s.Qtsq, D = s.D;
@@ -653,7 +824,7 @@ PGD int invert_1d(const double U[9], double prim[9], double g, const Geo &geo, c
   prim[RHO] = rho0;
   prim[ENY] = uu;
   prim[ENT] = (g - 1.) * uu * pgm::pow(rho0, -g);
-  harm_velocity(s, Gamma, W, prim);
+  harm_velocity<MT>(s, Gamma, W, prim);
   return 0;
 }
 
