@@ -523,9 +523,10 @@ __device__ __forceinline__ void face_flux(const Dims &d, const pangu_params &p, 
 // reconstructs cell c = f0 - 1 + l; face c takes its left state from lane
 // l - 1 (upper-face value of cell c - 1) and its right state from lane l.
 constexpr int kFacesPerWarp = 31;
+constexpr int kFluxThreads = 128;  // flux kernels use ~160 registers: 3 CTAs of 4 warps per SM
 
 template <int MT>
-__global__ void __launch_bounds__(kThreads) k_flux_x1(Dims d, pangu_params p, int k0, int k1,
+__global__ void __launch_bounds__(kFluxThreads) k_flux_x1(Dims d, pangu_params p, int k0, int k1,
                                                       int j0, int j1, int i0, int i1,
                                                       const double *P, double *F,
                                                       double *alfven) {
@@ -610,14 +611,14 @@ __device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_param
 }
 
 template <int MT>
-__global__ void __launch_bounds__(kThreads) k_flux_march2(Dims d, pangu_params p, int k0, int k1,
+__global__ void __launch_bounds__(kFluxThreads) k_flux_march2(Dims d, pangu_params p, int k0, int k1,
                                                           int j0, int j1, int i0, int i1,
                                                           const double *P, double *F,
                                                           double *alfven) {
   flux_march_body<MT, 2>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
 }
 template <int MT>
-__global__ void __launch_bounds__(kThreads) k_flux_march3(Dims d, pangu_params p, int k0, int k1,
+__global__ void __launch_bounds__(kFluxThreads) k_flux_march3(Dims d, pangu_params p, int k0, int k1,
                                                           int j0, int j1, int i0, int i1,
                                                           const double *P, double *F,
                                                           double *alfven) {
@@ -884,10 +885,73 @@ __global__ void __launch_bounds__(kThreads) k_build_tables(Dims d, pangu_params 
 // ---------------------------------------------------------------------------
 // Recovery (invertor.cc:18-210).
 // ---------------------------------------------------------------------------
+// Warp-aggregated append of `value` to list[*count] for the lanes with pred.
+__device__ __forceinline__ void append(int *count, long long *list, bool pred, long long value) {
+  const unsigned mask = __activemask();
+  const unsigned hits = __ballot_sync(mask, pred);
+  if (!hits) return;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(count, __popc(hits));
+  base = __shfl_sync(mask, base, leader);
+  if (pred) list[base + __popc(hits & ((1u << lane) - 1u))] = value;
+}
+
+// The HARM-normalised conserved state and the stale primitive guess of one
+// cell (invertor.cc:100-174); writes the magnetic primitives
+// (invertor.cc:137-147).
+template <int MT>
+__device__ __forceinline__ void c2p_inputs(const Dims &d, const pangu_params &p, double *P,
+                                           const double *U, int b, int k, int j, int i,
+                                           const Geo &g, double UH[9], double PH[9],
+                                           bool write_b) {
+  const long long q = vidx(d, b, 0, k, j, i);
+  const long long vs = d.ncell;
+  double C[9];
+#pragma unroll
+  for (int s = 0; s < 9; ++s) {
+    C[s] = d.pidx[s] >= 0 ? U[q + d.pidx[s] * vs] : 0.0;
+    PH[s] = d.pidx[s] >= 0 ? P[q + d.pidx[s] * vs] : 0.0;
+  }
+  const double isg = 1.0 / g.sg;
+  const double aisg = g.alpha * isg;
+  if (p.enable_B && write_b) {
+    P[q + d.pidx[BX1] * vs] = C[BX1] * isg;
+    P[q + d.pidx[BX2] * vs] = C[BX2] * isg;
+    P[q + d.pidx[BX3] * vs] = C[BX3] * isg;
+  }
+  UH[RHO] = aisg * C[RHO];
+  UH[ENY] = aisg * (C[ENY] - C[RHO]);
+  UH[UX1] = aisg * C[UX1];
+  UH[UX2] = aisg * C[UX2];
+  UH[UX3] = aisg * C[UX3];
+  UH[BX1] = aisg * C[BX1];
+  UH[BX2] = aisg * C[BX2];
+  UH[BX3] = aisg * C[BX3];
+  UH[ENT] = aisg * C[ENT];
+}
+
+__device__ __forceinline__ void c2p_write(const Dims &d, double *P, int b, int k, int j, int i,
+                                          const double PH[9]) {
+  const long long q = vidx(d, b, 0, k, j, i);
+  const long long vs = d.ncell;
+  P[q] = PH[RHO];
+  P[q + vs] = PH[ENY];
+  P[q + 2 * vs] = PH[UX1];
+  P[q + 3 * vs] = PH[UX2];
+  P[q + 4 * vs] = PH[UX3];
+}
+
+// Recovery, first pass: Kastaun (robuster), or Scheme2D of the chain. Cells
+// where Scheme2D fails are appended to `retry` (their primitives are left
+// untouched) and finished by k_recovery_retry, so the long 1Dvsq/1D Newton
+// loops of a few cells do not hold whole warps of converged cells.
 template <int MT>
 __global__ void __launch_bounds__(kThreads) k_recovery(Dims d, pangu_params p, double *P,
                                                        const double *U, double *flag,
-                                                       unsigned long long *cnt) {
+                                                       unsigned long long *cnt, int *nretry,
+                                                       long long *retry) {
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
@@ -907,36 +971,8 @@ __global__ void __launch_bounds__(kThreads) k_recovery(Dims d, pangu_params p, d
   }
   Geo g;
   cell_metric<MT>(d, p, b, k, j, i, g);
-  if (!robuster) flag[fc] = 0;
-  const double sg = g.sg;
-  const double alpha = g.alpha;
-  const long long q = vidx(d, b, 0, k, j, i);
-  const long long vs = d.ncell;
-  double C[9], Pp[9];
-#pragma unroll
-  for (int s = 0; s < 9; ++s) {
-    C[s] = d.pidx[s] >= 0 ? U[q + d.pidx[s] * vs] : 0.0;
-    Pp[s] = d.pidx[s] >= 0 ? P[q + d.pidx[s] * vs] : 0.0;
-  }
-  const double isg = 1.0 / sg;
-  const double aisg = alpha * isg;
-  if (p.enable_B) {
-    P[q + d.pidx[BX1] * vs] = C[BX1] * isg;
-    P[q + d.pidx[BX2] * vs] = C[BX2] * isg;
-    P[q + d.pidx[BX3] * vs] = C[BX3] * isg;
-  }
   double UH[9], PH[9];
-  UH[RHO] = aisg * C[RHO];
-  UH[ENY] = aisg * (C[ENY] - C[RHO]);
-  UH[UX1] = aisg * C[UX1];
-  UH[UX2] = aisg * C[UX2];
-  UH[UX3] = aisg * C[UX3];
-  UH[BX1] = aisg * C[BX1];
-  UH[BX2] = aisg * C[BX2];
-  UH[BX3] = aisg * C[BX3];
-  UH[ENT] = aisg * C[ENT];
-#pragma unroll
-  for (int s = 0; s < 9; ++s) PH[s] = Pp[s];
+  c2p_inputs<MT>(d, p, P, U, b, k, j, i, g, UH, PH, true);
   const double gam = p.adiabatic_index;
   if (robuster) {
     const int st = invert_kastaun(UH, PH, gam, g);
@@ -945,24 +981,49 @@ __global__ void __launch_bounds__(kThreads) k_recovery(Dims d, pangu_params p, d
   } else {
     Harm hs;
     harm_setup<MT>(UH, g, hs);
-    int ok = invert_2d<MT>(UH, PH, gam, g, hs) == 0;
+    const bool ok = invert_2d<MT>(UH, PH, gam, g, hs) == 0;
     count(cnt, PANGU_CNT_C2P_2D, ok);
-    if (!ok) {
-      ok = invert_1dvsq<MT>(UH, PH, gam, g, hs) == 0;
-      count(cnt, PANGU_CNT_C2P_1DVSQ, ok);
-      if (!ok) {
-        ok = invert_1d<MT>(UH, PH, gam, g, hs) == 0;
-        count(cnt, PANGU_CNT_C2P_1D, ok);
-        count(cnt, PANGU_CNT_C2P_FAIL, !ok);
-      }
-    }
-    flag[fc] = ok;
+    append(nretry, retry, !ok, fc);
+    flag[fc] = ok ? 1.0 : 0.0;
+    if (!ok) return;
   }
-  P[q] = PH[RHO];
-  P[q + vs] = PH[ENY];
-  P[q + 2 * vs] = PH[UX1];
-  P[q + 3 * vs] = PH[UX2];
-  P[q + 4 * vs] = PH[UX3];
+  c2p_write(d, P, b, k, j, i, PH);
+}
+
+// Recovery, second pass over the cells Scheme2D failed: Scheme1Dvsq, then
+// Scheme1D (invertor.cc:185-197).
+template <int MT>
+__global__ void __launch_bounds__(kThreads) k_recovery_retry(Dims d, pangu_params p, double *P,
+                                                             const double *U, double *flag,
+                                                             unsigned long long *cnt,
+                                                             const int *nretry,
+                                                             const long long *retry) {
+  const int n = *nretry;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long fc = retry[t];
+    const int b = (int)(fc / d.ncell);
+    long long c = fc - (long long)b * d.ncell;
+    const int k = (int)(c / ((long long)d.N2 * d.N1));
+    c -= (long long)k * d.N2 * d.N1;
+    const int j = (int)(c / d.N1), i = (int)(c % d.N1);
+    Geo g;
+    cell_metric<MT>(d, p, b, k, j, i, g);
+    double UH[9], PH[9];
+    c2p_inputs<MT>(d, p, P, U, b, k, j, i, g, UH, PH, false);
+    const double gam = p.adiabatic_index;
+    Harm hs;
+    harm_setup<MT>(UH, g, hs);
+    bool ok = invert_1dvsq<MT>(UH, PH, gam, g, hs) == 0;
+    count(cnt, PANGU_CNT_C2P_1DVSQ, ok);
+    if (!ok) {
+      ok = invert_1d<MT>(UH, PH, gam, g, hs) == 0;
+      count(cnt, PANGU_CNT_C2P_1D, ok);
+      count(cnt, PANGU_CNT_C2P_FAIL, !ok);
+    }
+    flag[fc] = ok ? 1.0 : 0.0;
+    c2p_write(d, P, b, k, j, i, PH);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1061,43 +1122,64 @@ __global__ void __launch_bounds__(kThreads) k_fixrec_write(Dims d, const int *co
 }
 
 // ---------------------------------------------------------------------------
-// Physical boundary conditions on one face.
+// Physical boundary conditions (outflow / reflecting) of all faces in one
+// pass. Applying the faces in the order ix1, ox1, ix2, ox2, ix3, ox3, each over
+// its full transverse range, leaves every ghost cell equal to one interior
+// (or exchanged) cell, reached by applying each direction's rule in turn to
+// the index, with the reflections' sign flips composed. The kernel computes
+// that composition directly; its sources are never written by it.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_bc_face(Dims d, int face, int kind, int b_sel_dim,
-                                                      int b_sel_val, int nbx1, int nbx2,
-                                                      int enable_B, double *P, double *flag) {
-  const int dir = face / 2, outer = face % 2;
-  int N[3] = {d.N1, d.N2, d.N3};
-  const int s[3] = {d.is, d.js, d.ks}, e[3] = {d.ie, d.je, d.ke};
-  const int ng = outer ? (N[dir] - 1 - e[dir]) : s[dir];
-  int ext[3] = {N[0], N[1], N[2]};
-  ext[dir] = ng;
-  const long long per = (long long)ext[0] * ext[1] * ext[2];
+struct BCInfo {
+  int kind[6];   // per face: PANGU_BC_OUTFLOW / REFLECTING, or -1 (periodic / inactive)
+  int nb[3];     // block lattice
+};
+
+__global__ void __launch_bounds__(kThreads) k_bcs(Dims d, BCInfo bc, int enable_B, double *P,
+                                                  double *flag) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= per * d.NB) return;
-  const int b = (int)(t / per);
-  const int bl[3] = {b % nbx1, (b / nbx1) % nbx2, b / (nbx1 * nbx2)};
-  if (bl[b_sel_dim] != b_sel_val) return;
-  long long r = t - (long long)b * per;
+  if (t >= (long long)d.NB * d.ncell) return;
+  const int b = (int)(t / d.ncell);
+  long long c = t - (long long)b * d.ncell;
   int idx[3];
-  idx[0] = (int)(r % ext[0]);
-  r /= ext[0];
-  idx[1] = (int)(r % ext[1]);
-  idx[2] = (int)(r / ext[1]);
-  idx[dir] = outer ? (e[dir] + 1 + idx[dir]) : idx[dir];
-  const int x = idx[dir];
-  int sidx[3] = {idx[0], idx[1], idx[2]};
-  if (kind == PANGU_BC_OUTFLOW) sidx[dir] = outer ? e[dir] : s[dir];
-  else sidx[dir] = outer ? (2 * e[dir] + 1 - x) : (2 * s[dir] - 1 - x);
+  idx[2] = (int)(c / ((long long)d.N2 * d.N1));
+  c -= (long long)idx[2] * d.N2 * d.N1;
+  idx[1] = (int)(c / d.N1);
+  idx[0] = (int)(c % d.N1);
+  const int bl[3] = {b % bc.nb[0], (b / bc.nb[0]) % bc.nb[1], b / (bc.nb[0] * bc.nb[1])};
+  const int st[3] = {d.is, d.js, d.ks}, en[3] = {d.ie, d.je, d.ke};
+  int src[3] = {idx[0], idx[1], idx[2]};
+  int flip[3] = {0, 0, 0};
+  bool ghost = false;
+#pragma unroll
+  for (int dir = 0; dir < 3; ++dir) {
+    const int x = src[dir];
+    int kind = -1, outer = 0;
+    if (x < st[dir] && bl[dir] == 0) {
+      kind = bc.kind[2 * dir];
+    } else if (x > en[dir] && bl[dir] == bc.nb[dir] - 1) {
+      kind = bc.kind[2 * dir + 1];
+      outer = 1;
+    }
+    if (kind < 0) continue;
+    ghost = true;
+    if (kind == PANGU_BC_OUTFLOW) {
+      src[dir] = outer ? en[dir] : st[dir];
+    } else {
+      src[dir] = outer ? (2 * en[dir] + 1 - x) : (2 * st[dir] - 1 - x);
+      flip[dir] ^= 1;
+    }
+  }
+  if (!ghost) return;
   const long long dc = cidx(d, b, idx[2], idx[1], idx[0]);
-  const long long sc = cidx(d, b, sidx[2], sidx[1], sidx[0]);
-  const long long base = (long long)b * d.NF * d.ncell - (long long)b * d.ncell;
+  const long long sc = cidx(d, b, src[2], src[1], src[0]);
+  const long long base = (long long)b * (d.NF - 1) * d.ncell;
   for (int v = 0; v < d.NF; ++v) {
     double val = P[base + sc + v * d.ncell];
-    if (kind == PANGU_BC_REFLECTING) {
+#pragma unroll
+    for (int dir = 0; dir < 3; ++dir) {
       const bool vel = v == d.pidx[UX1] + dir;
       const bool mag = enable_B && v == d.pidx[BX1] + dir;
-      if (vel || mag) val = -val;
+      if (flip[dir] && (vel || mag)) val = -val;
     }
     P[base + dc + v * d.ncell] = val;
   }
@@ -1207,6 +1289,20 @@ inline long long box_count(int NB, int k0, int k1, int j0, int j1, int i0, int i
     }                                                                       \
   } while (0)
 
+#define DISPATCH_MT_T(mt, KERNEL, grid, threads, stream, ...)                                 \
+  do {                                                                                       \
+    switch (mt) {                                                                            \
+      case PANGU_METRIC_MKS: KERNEL<MKS><<<grid, threads, 0, stream>>>(__VA_ARGS__); break;   \
+      case PANGU_METRIC_BL: KERNEL<BL><<<grid, threads, 0, stream>>>(__VA_ARGS__); break;     \
+      case PANGU_METRIC_CKS: KERNEL<CKS><<<grid, threads, 0, stream>>>(__VA_ARGS__); break;   \
+      default: KERNEL<MINKOWSKI><<<grid, threads, 0, stream>>>(__VA_ARGS__); break;           \
+    }                                                                                        \
+  } while (0)
+
+inline unsigned grid_flux(long long n) {
+  return (unsigned)std::max<long long>(1, (n + kFluxThreads - 1) / kFluxThreads);
+}
+
 bool pack_ok(const pangu_engine *e, const pangu_pack *md) {
   if (!e || !md || !md->prim || !md->cons || !md->flux1 || !md->alfven || !md->efield) return false;
   if (e->d.ndim >= 2 && !md->flux2) return false;
@@ -1248,13 +1344,15 @@ int run_fluxes(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
     if (dir == 1) {
       const int nseg = (i1 - i0 + 1 + kFacesPerWarp - 1) / kFacesPerWarp;
       const long long warps = (long long)d.NB * (k1 - k0 + 1) * (j1 - j0 + 1) * nseg;
-      DISPATCH_MT(e->p.metric_type, k_flux_x1, grid_for(32 * warps), s, FLUX_ARGS);
+      DISPATCH_MT_T(e->p.metric_type, k_flux_x1, grid_flux(32 * warps), kFluxThreads, s, FLUX_ARGS);
     } else {
       const int m = dir == 2 ? (j1 - j0 + 1) : (k1 - k0 + 1);
       const int na = dir == 2 ? (k1 - k0 + 1) : (j1 - j0 + 1);
       const long long n = (long long)d.NB * na * ((m + kMarch - 1) / kMarch) * (i1 - i0 + 1);
-      if (dir == 2) DISPATCH_MT(e->p.metric_type, k_flux_march2, grid_for(n), s, FLUX_ARGS);
-      else DISPATCH_MT(e->p.metric_type, k_flux_march3, grid_for(n), s, FLUX_ARGS);
+      if (dir == 2)
+        DISPATCH_MT_T(e->p.metric_type, k_flux_march2, grid_flux(n), kFluxThreads, s, FLUX_ARGS);
+      else
+        DISPATCH_MT_T(e->p.metric_type, k_flux_march3, grid_flux(n), kFluxThreads, s, FLUX_ARGS);
     }
 #undef FLUX_ARGS
     ++e->launches;
@@ -1311,9 +1409,15 @@ int run_source(pangu_engine *e, const pangu_pack *md, double beta, const double 
 int run_recovery(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
   const Dims &d = e->d;
   const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
+  if (cudaMemsetAsync(e->d_fail_count, 0, sizeof(int), s) != cudaSuccess) return PANGU_ECUDA;
   DISPATCH_MT(e->p.metric_type, k_recovery, grid_for(n), s, d, e->p, md->prim, md->cons, md->flag,
-              e->d_cnt);
+              e->d_cnt, e->d_fail_count, e->d_fail_list);
   ++e->launches;
+  if (e->p.recovery == PANGU_RECOVERY_CHAINER) {
+    DISPATCH_MT(e->p.metric_type, k_recovery_retry, 2 * 148, s, d, e->p, md->prim, md->cons,
+                md->flag, e->d_cnt, e->d_fail_count, e->d_fail_list);
+    ++e->launches;
+  }
   return check_launch();
 }
 
@@ -1344,22 +1448,21 @@ int run_fix_recovery(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
 int run_bcs(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
   const Dims &d = e->d;
   const int act[3] = {d.o1, d.o2, d.o3};
-  const int N[3] = {d.N1, d.N2, d.N3};
-  const int nb[3] = {e->m.nbx1, e->m.nbx2, e->m.nbx3};
+  BCInfo bc;
+  bool any = false;
   for (int face = 0; face < 6; ++face) {
-    const int dir = face / 2, outer = face % 2;
     const int kind = e->m.bc[face];
-    if (!act[dir] || kind == PANGU_BC_PERIODIC) continue;
-    long long ext = (long long)N[0] * N[1] * N[2] / N[dir] * e->m.ng;
-    const long long n = ext * d.NB;
-    k_bc_face<<<grid_for(n), kThreads, 0, s>>>(d, face, kind, dir, outer ? nb[dir] - 1 : 0,
-                                               e->m.nbx1, e->m.nbx2, e->p.enable_B, md->prim,
-                                               md->flag);
-    ++e->launches;
-    const int rc = check_launch();
-    if (rc) return rc;
+    bc.kind[face] = (act[face / 2] && kind != PANGU_BC_PERIODIC) ? kind : -1;
+    any = any || bc.kind[face] >= 0;
   }
-  return PANGU_OK;
+  if (!any) return PANGU_OK;
+  bc.nb[0] = e->m.nbx1;
+  bc.nb[1] = e->m.nbx2;
+  bc.nb[2] = e->m.nbx3;
+  k_bcs<<<grid_for((long long)d.NB * d.ncell), kThreads, 0, s>>>(d, bc, e->p.enable_B, md->prim,
+                                                                md->flag);
+  ++e->launches;
+  return check_launch();
 }
 
 int run_estimate_dt(pangu_engine *e, const pangu_pack *md, double *dt_out, cudaStream_t s) {
