@@ -62,7 +62,8 @@ def config(extra=None):
     c = {"workload": WORKLOAD, "nx1": NX1, "nx2": NX2, "meshblocks": 1, "limiter": "ppm4",
          "riemann_solver": "laxf", "recovery": "chainer", "electron_heating": True,
          "metric": "mks a=0.9375 h=0.7", "job_steps": JOB_STEPS,
-         "l2": "flushed (256 MiB write) before every timed step"}
+         "l2": "flushed (256 MiB write) before every timed step",
+         "launch": "one CUDA graph replay per RK2 step"}
     if extra:
         c.update(extra)
     return c
@@ -166,6 +167,13 @@ def run_engine(args):
     for _ in range(args.warmup):
         sim.step()
     torch.cuda.synchronize()
+    if not args.no_graph:
+        # one RK2 cycle per CUDA graph replay; the capture runs no kernel
+        launches_per_step = sim.engine.launches()
+        sim.capture()
+        launches_per_step = sim.engine.launches() - launches_per_step
+        sim.step()  # the first replay is part of the warm-up
+        torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
 
@@ -181,6 +189,8 @@ def run_engine(args):
             ends[s].record()
         torch.cuda.synchronize()
     launches = sim.engine.launches() - launches0
+    if not args.no_graph:
+        launches = launches_per_step * args.steps
     total_ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
     if world > 1:
         t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
@@ -406,6 +416,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-budget", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="launch every kernel from the host instead of replaying a CUDA graph")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -526,7 +526,7 @@ constexpr int kFacesPerWarp = 31;
 constexpr int kFluxThreads = 128;  // flux kernels use ~160 registers: 3 CTAs of 4 warps per SM
 
 template <int MT>
-__global__ void __launch_bounds__(kFluxThreads) k_flux_x1(Dims d, pangu_params p, int k0, int k1,
+__global__ void __launch_bounds__(kFluxThreads, 4) k_flux_x1(Dims d, pangu_params p, int k0, int k1,
                                                       int j0, int j1, int i0, int i1,
                                                       const double *P, double *F,
                                                       double *alfven) {
@@ -611,14 +611,14 @@ __device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_param
 }
 
 template <int MT>
-__global__ void __launch_bounds__(kFluxThreads) k_flux_march2(Dims d, pangu_params p, int k0, int k1,
+__global__ void __launch_bounds__(kFluxThreads, 4) k_flux_march2(Dims d, pangu_params p, int k0, int k1,
                                                           int j0, int j1, int i0, int i1,
                                                           const double *P, double *F,
                                                           double *alfven) {
   flux_march_body<MT, 2>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
 }
 template <int MT>
-__global__ void __launch_bounds__(kFluxThreads) k_flux_march3(Dims d, pangu_params p, int k0, int k1,
+__global__ void __launch_bounds__(kFluxThreads, 4) k_flux_march3(Dims d, pangu_params p, int k0, int k1,
                                                           int j0, int j1, int i0, int i1,
                                                           const double *P, double *F,
                                                           double *alfven) {
@@ -948,7 +948,7 @@ __device__ __forceinline__ void c2p_write(const Dims &d, double *P, int b, int k
 // untouched) and finished by k_recovery_retry, so the long 1Dvsq/1D Newton
 // loops of a few cells do not hold whole warps of converged cells.
 template <int MT>
-__global__ void __launch_bounds__(kThreads) k_recovery(Dims d, pangu_params p, double *P,
+__global__ void __launch_bounds__(kThreads, 3) k_recovery(Dims d, pangu_params p, double *P,
                                                        const double *U, double *flag,
                                                        unsigned long long *cnt, int *nretry,
                                                        long long *retry) {

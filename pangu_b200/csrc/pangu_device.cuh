@@ -708,14 +708,18 @@ PGD int invert_1dvsq(const double U[9], double prim[9], double g, const Geo &geo
   const double Bsq = s.Bsq, QdotBsq = s.QdotBsq, Qtsq = s.Qtsq, D = s.D;
   double f = 1., df = 1., errx = 1., W = 0., W_old;
   int i_extra = 0, doing_extra = 0;
+  // W_of_vsq at the current x: func_1d_gnr evaluates it at the start of each
+  // iteration (scheme_1d_vsq.h:100) at the point where the previous
+  // iteration's convergence test evaluated it (:174); the value is reused.
+  double pA, rhoA, uuA;
+  double WA = w_of_vsq(D, K, x, g, pA, rhoA, uuA);
   for (int n_iter = 0;; ++n_iter) {
-    double rho, p, uu;
     {
       const double vsq = x;
-      const double Wv = w_of_vsq(D, K, vsq, g, p, rho, uu);
+      const double Wv = WA;
       const double Wsq = Wv * Wv;
       const double W3 = Wv * Wsq;
-      const double dWdvsq = ((g * (2. - g) * p + (g - 1.) * rho) /
+      const double dWdvsq = ((g * (2. - g) * pA + (g - 1.) * rhoA) /
                              (2. * (g - 1.) * (1. - vsq) * (1. - vsq)));
       const double ft = (Bsq + Wv);
       const double resid = Qtsq - vsq * ft * ft + QdotBsq * (Bsq + 2. * Wv) / Wsq;
@@ -729,7 +733,8 @@ PGD int invert_1dvsq(const double U[9], double prim[9], double g, const Geo &geo
       x = (x < -1.e-10) ? (0.5 * xo) : x;
       x = fabs(x);
       W_old = W;
-      W = w_of_vsq(D, K, x, g, p, rho, uu);
+      W = w_of_vsq(D, K, x, g, pA, rhoA, uuA);
+      WA = W;
       errx = (W == 0.) ? fabs(W - W_old) : fabs((W - W_old) / W);
       errx += (x == 0.) ? fabs(x - xo) : fabs((x - xo) / x);
     }
@@ -745,8 +750,7 @@ PGD int invert_1dvsq(const double U[9], double prim[9], double g, const Geo &geo
   if (retval != 0) return retval * 100 + 1;
   const double vsq = x;
   if ((vsq >= 1.) || (vsq < 0.)) return 4;
-  double p, rho0, uu;
-  const double Wf = w_of_vsq(D, K, vsq, g, p, rho0, uu);
+  const double Wf = WA, rho0 = rhoA, uu = uuA;  // W_of_vsq(D, K, vsq) of :321
   const double Gamma = 1. / sqrt(1. - vsq);
   if ((rho0 <= 0.) || (uu <= 0.)) return 5;
   prim[RHO] = rho0;

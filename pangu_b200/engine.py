@@ -225,6 +225,7 @@ class Simulation:
         self.dt = torch.full((1,), self.dt_init, dtype=torch.float64, device=dev)
         self.dt_est = torch.zeros(1, dtype=torch.float64, device=dev)
         self.cycle = 0
+        self._graph = None
 
     def set_primitives(self, prim: np.ndarray):
         """Loads initial primitives (interior values; ghosts are filled here:
@@ -240,12 +241,32 @@ class Simulation:
     def stage(self, st: int, dt_est=None):
         self.engine.stage(st, self.base, self.one, RK2_BETA[st % 2], self.dt, dt_est)
 
-    def step(self, fixed_dt: bool = False):
-        """One rk2 cycle; afterwards dt = min(dt_factor * dt, estimate)."""
+    def _step_launches(self, fixed_dt: bool):
         self.stage(1)
         self.stage(2, self.dt_est)
         if not fixed_dt:
             self.engine.update_dt(self.dt, self.dt_est, self.dt_factor)
+
+    def capture(self):
+        """Captures one RK2 cycle (both stages and the device dt policy) as a
+        CUDA graph; later step() calls replay it. Every launch of the cycle is
+        stream ordered and reads dt from device memory, so one graph serves
+        every step."""
+        import torch
+        s = torch.cuda.Stream(self.engine.device)
+        s.wait_stream(torch.cuda.current_stream(self.engine.device))
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            self._step_launches(False)
+        torch.cuda.current_stream(self.engine.device).wait_stream(s)
+        self._graph = g
+
+    def step(self, fixed_dt: bool = False):
+        """One rk2 cycle; afterwards dt = min(dt_factor * dt, estimate)."""
+        if self._graph is not None and not fixed_dt:
+            self._graph.replay()
+        else:
+            self._step_launches(fixed_dt)
         self.cycle += 1
 
     def primitives(self) -> np.ndarray:
