@@ -44,6 +44,7 @@ extern "C" {
 #define PANGU_ENOMEM (-3)     /* engine-internal allocation failed             */
 #define PANGU_ENGHOST (-4)    /* ghost width too small for the limiter         */
 #define PANGU_ETOOBIG (-5)    /* size above a documented maximum               */
+#define PANGU_EFULL (-6)      /* pool has no free slot or job id               */
 
 /* ---- option enumerations (string values of the reference's params) ---- */
 #define PANGU_RIEMANN_LAXF 0  /* <core>/riemann_solver = laxf */
@@ -178,7 +179,8 @@ int pangu_constrained_transport(pangu_engine *e, const pangu_pack *md,
                                 void *stream);
 /* mc1.cons = mc_init.cons - (beta*dt) * div(mc0 fluxes) over the interior
  * (Parthenon FluxDivergence + UpdateIndependentData, ideal_grmhd.cc:73-76).
- * dt is a DEVICE pointer to one double so a captured graph stays valid. */
+ * dt is a DEVICE pointer so a captured graph stays valid: dt[job] per job
+ * (dt[0] for an engine made by pangu_engine_create). */
 int pangu_flux_divergence_update(pangu_engine *e, const pangu_pack *mc_init,
                                  const pangu_pack *mc0, const pangu_pack *mc1,
                                  double beta, const double *dt, void *stream);
@@ -196,7 +198,7 @@ int pangu_fix_recovery(pangu_engine *e, const pangu_pack *md, void *stream);
 int pangu_apply_boundary_conditions(pangu_engine *e, const pangu_pack *md,
                                     void *stream);
 /* dt estimate from the alfven field (timestep_estimation.cc:13-102),
- * written to the DEVICE double *dt_out. */
+ * written to the DEVICE array dt_out[job] of every active job. */
 int pangu_estimate_dt(pangu_engine *e, const pangu_pack *md, double *dt_out,
                       void *stream);
 
@@ -224,16 +226,49 @@ int pangu_stage(pangu_engine *e, int stage, const pangu_pack *base,
 int pangu_estimate_dt_noalloc(const pangu_params *params, const pangu_mesh *mesh,
                               const double *alfven, double *dt_out, void *stream);
 
-/* Device dt policy applied after each cycle: dt = min(dt_factor*dt, dt_est). */
+/* Device dt policy applied after each cycle, per active job:
+ * dt[job] = min(dt_factor*dt[job], dt_est[job]). */
 int pangu_update_dt(pangu_engine *e, double *dt, const double *dt_est,
                     double dt_factor, void *stream);
 
-/* Counters accumulated since the last reset (host copy, synchronous). */
+/* Counters accumulated since the last reset, summed over jobs (host copy,
+ * synchronous). */
 int pangu_counters(pangu_engine *e, uint64_t out[PANGU_NCOUNTERS]);
 int pangu_reset_counters(pangu_engine *e, void *stream);
 
 /* Number of CUDA kernels this handle has launched so far (host-side count). */
 long long pangu_launches(const pangu_engine *e);
+
+/* ---- block pool: many jobs stepped by the same launches ---------------- */
+/* No counterpart in the reference, which runs one mesh per process. A pool
+ * engine owns a block table over `capacity_blocks` slots of the block shape
+ * in `block` (nx1..nx3, ng; its other fields are ignored). Jobs -- meshes of
+ * such blocks with their own lattice, extents, BCs and metric spin a and h --
+ * are attached into free slots and detached when done; every task and
+ * pangu_stage call then processes all attached jobs' blocks in one launch per
+ * kernel, reading dt[job] and writing dt_est[job]. The caller owns the
+ * containers: packs sized for `capacity_blocks` blocks, slot-major. Results
+ * are identical to running each job alone with pangu_engine_create.
+ * attach/detach synchronise the device and change the launch domain, so a
+ * CUDA graph captured before them must be captured again. */
+int pangu_pool_create(const pangu_params *params, const pangu_mesh *block,
+                      int32_t capacity_blocks, int32_t max_jobs, pangu_engine **out);
+/* Places a job (mesh: the pool's nx and ng, any nbx/extents/bc) in free slots
+ * (lowest first). slots_out[b] receives the slot of the job's block b (lattice
+ * order, x1 fastest); job_out its id, which indexes dt/dt_est.
+ * PANGU_EFULL when no id or too few slots are free. */
+int pangu_job_attach(pangu_engine *e, const pangu_mesh *mesh, double a, double h,
+                     int32_t *job_out, int32_t *slots_out);
+/* After the caller wrote a job's interior primitives into its slots of base:
+ * fills its ghosts (exchange, then physical BCs) and copies base into one for
+ * its slots, as Parthenon does after the problem generator. */
+int pangu_job_start(pangu_engine *e, int32_t job, const pangu_pack *base,
+                    const pangu_pack *one, void *stream);
+int pangu_job_detach(pangu_engine *e, int32_t job);
+/* Counters of one job since its attach (host copy, synchronous). */
+int pangu_job_counters(pangu_engine *e, int32_t job, uint64_t out[PANGU_NCOUNTERS]);
+/* Blocks in the launch domain (all attached jobs). */
+int pangu_active_blocks(const pangu_engine *e);
 
 #ifdef __cplusplus
 }

@@ -9,6 +9,7 @@ PANGU_ECUDA = -2
 PANGU_ENOMEM = -3
 PANGU_ENGHOST = -4
 PANGU_ETOOBIG = -5
+PANGU_EFULL = -6
 
 RIEMANN = {"laxf": 0, "hll": 1}
 LIMITER = {"ppm4": 0, "mc": 1}

@@ -43,30 +43,58 @@ struct Dims {
   int o1, o2, o3, ndim;
   long long ncell;  // N1 * N2 * N3
   int pidx[NPRIM];  // pack index of each slot, -1 if absent
-  double dx[3];
-  const double *t1;      // [NB][10][N1 + 1]
-  const double *t2;      // [NB][12][N2 + 1]
-  const double *origin;  // [NB][3]
+  double dx[3];          // cell widths where bdx is null (handle-free dt estimate)
+  // Block table. The launch domain is NB active blocks; active block bb lives
+  // in pool slot slot[bb] (identity when null). Arrays below marked [slot]
+  // are indexed by pool slot.
+  const int *slot;          // [NB]
+  const int *slot_job;      // [slot] owning job id (job 0 when null)
+  const double *bdx;        // [slot][3] cell widths of the owning job's mesh
+  const signed char *bcf;   // [slot][6] PANGU_BC_OUTFLOW/REFLECTING per face, -1 none
+  const double *t1;      // [slot][10][N1 + 1]
+  const double *t2;      // [slot][12][N2 + 1]
+  const double *origin;  // [slot][3]
   // Static MKS/BL metric tables (built once per engine by k_build_tables):
   // component planes of [NB][comp][N2][N1] (centres), [NB][comp][N2][N1+1]
   // (x1 faces) and [NB][comp][N2+1][N1] (x2 faces); x3 faces use the centres.
   const double *ctab, *f1tab, *f2tab;
 };
 
+// A job: one mesh of equal meshblocks, placed in pool slots.
+struct PoolJob {
+  bool live = false;
+  pangu_mesh m{};
+  pangu_params p{};                 // the pool's params with the job's metric a, h
+  std::vector<int> slots;           // slot of the job's block b (lattice order)
+  std::vector<int64_t> xdst, xsrc;  // exchange map in slot cell offsets
+  bool any_bc = false;              // some face is outflow / reflecting
+};
+
 struct pangu_engine {
   pangu_params p;
-  pangu_mesh m;
-  Dims d;
+  pangu_mesh m;  // block shape (nx, ng); for a single-mesh engine the whole mesh
+  Dims d;        // d.NB = active blocks; d.slot = d_active
+  int capacity = 0, max_jobs = 0;
+  std::vector<PoolJob> jobs;
+  std::vector<char> slot_used;
+  int njobs_active = 0;
+  bool any_bc = false;
+  std::vector<long long> xoff;  // per job id: offset of its entries in the exchange map
+  int *d_active = nullptr;      // [capacity] active block -> slot
+  int *d_slot_job = nullptr;    // [capacity]
+  int *d_jr = nullptr;          // [max_jobs][3] job id, first and end active block
+  double *d_bdx = nullptr;      // [capacity][3]
+  signed char *d_bcf = nullptr; // [capacity][6]
   double *d_t1 = nullptr, *d_t2 = nullptr, *d_origin = nullptr;
   double *d_ctab = nullptr, *d_f1tab = nullptr, *d_f2tab = nullptr;
   long long *d_xdst = nullptr, *d_xsrc = nullptr;
-  long long nxch = 0;
-  unsigned long long *d_cnt = nullptr;
+  long long nxch = 0, xch_cap = 0;
+  unsigned long long *d_cnt = nullptr;  // [max_jobs][PANGU_NCOUNTERS]
   int *d_fail_count = nullptr;
   long long *d_fail_list = nullptr;
   double *d_fail_vals = nullptr;
   long long fail_cap = 0;
-  unsigned long long *d_dtmin = nullptr;
+  unsigned long long *d_dtmin = nullptr;  // [capacity][3]
   long long launches = 0;  // kernels launched through this handle
 };
 
@@ -74,6 +102,16 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kT1Rows = 10;  // rows of the x1 table (host_tables.cc)
+
+__device__ __forceinline__ int slot_of(const Dims &d, int bb) {
+  return d.slot ? __ldg(d.slot + bb) : bb;
+}
+__device__ __forceinline__ int job_of(const Dims &d, int b) {
+  return d.slot_job ? __ldg(d.slot_job + b) : 0;
+}
+__device__ __forceinline__ double dx_of(const Dims &d, int b, int dir) {
+  return d.bdx ? __ldg(d.bdx + 3 * b + dir) : d.dx[dir];
+}
 
 __device__ __forceinline__ long long vidx(const Dims &d, int b, int v, int k, int j, int i) {
   return (((long long)b * d.NF + v) * d.N3 + k) * (long long)d.N2 * d.N1 + (long long)j * d.N1 + i;
@@ -93,10 +131,10 @@ __device__ __forceinline__ void load_prim(const Dims &d, const double *P, int b,
 
 // Cell-centre coordinate (origin + (idx + 1/2) dx, rounded step by step).
 __device__ __forceinline__ double xc(const Dims &d, int b, int dir, int idx) {
-  return ADD(d.origin[3 * b + dir], MUL((double)idx + 0.5, d.dx[dir]));
+  return ADD(d.origin[3 * b + dir], MUL((double)idx + 0.5, dx_of(d, b, dir)));
 }
 __device__ __forceinline__ double xf(const Dims &d, int b, int dir, int idx) {
-  return ADD(d.origin[3 * b + dir], MUL((double)idx, d.dx[dir]));
+  return ADD(d.origin[3 * b + dir], MUL((double)idx, dx_of(d, b, dir)));
 }
 
 // Map point of the x1/x2 tables: q1/q2 select centre (0), +delta (1),
@@ -278,11 +316,16 @@ __device__ __forceinline__ int face_metric(const Dims &d, const pangu_params &p,
   }
 }
 
-// Warp-aggregated increment of a hit counter.
-__device__ __forceinline__ void count(unsigned long long *cnt, int which, bool pred) {
+// Warp-aggregated increment of a hit counter of `job` (counters are
+// [job][PANGU_NCOUNTERS]); a warp may straddle blocks of several jobs.
+__device__ __forceinline__ void count(unsigned long long *cnt, int job, int which, bool pred) {
   const unsigned mask = __activemask();
   const unsigned hits = __ballot_sync(mask, pred);
-  if (hits && (threadIdx.x & 31) == (__ffs(mask) - 1)) atomicAdd(&cnt[which], (unsigned long long)__popc(hits));
+  if (!hits) return;
+  const unsigned peers = __match_any_sync(mask, job);
+  const unsigned mine = hits & peers;
+  if (mine && (threadIdx.x & 31) == (__ffs(peers) - 1))
+    atomicAdd(&cnt[job * PANGU_NCOUNTERS + which], (unsigned long long)__popc(mine));
 }
 
 // Decomposes a flat index over the box [k0,k1] x [j0,j1] x [i0,i1] of every
@@ -316,6 +359,7 @@ __global__ void __launch_bounds__(kThreads) k_fix_primitive(Dims d, pangu_params
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, 0, d.N3 - 1, 0, d.N2 - 1, 0, d.N1 - 1, b, k, j, i)) return;
+  b = slot_of(d, b);
   const double gam = p.adiabatic_index;
   constexpr double small = 1.0e-20;
   const double sigma_max_safe = kmax(p.sigma_max, small);
@@ -396,9 +440,9 @@ __global__ void __launch_bounds__(kThreads) k_fix_primitive(Dims d, pangu_params
   P[q + 4 * vs] = u3;
   P[q + d.pidx[ENT] * vs] = ent;
   if (p.enable_heating) P[q + d.pidx[KEL] * vs] = kel;
-  count(cnt, PANGU_CNT_RHO_FLOOR, hit_r);
-  count(cnt, PANGU_CNT_ENG_FLOOR, hit_u);
-  count(cnt, PANGU_CNT_LORENTZ_CAP, cap);
+  count(cnt, job_of(d, b), PANGU_CNT_RHO_FLOOR, hit_r);
+  count(cnt, job_of(d, b), PANGU_CNT_ENG_FLOOR, hit_u);
+  count(cnt, job_of(d, b), PANGU_CNT_LORENTZ_CAP, cap);
 }
 
 // ---------------------------------------------------------------------------
@@ -410,6 +454,7 @@ __global__ void __launch_bounds__(kThreads) k_calc_cons(Dims d, pangu_params p, 
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
+  b = slot_of(d, b);
   Geo g;
   cell_metric<MT>(d, p, b, k, j, i, g);
   double pc[NPRIM];
@@ -538,8 +583,9 @@ __global__ void __launch_bounds__(kFluxThreads, 4) k_flux_x1(Dims d, pangu_param
   if (warp >= nrow * d.NB * nseg) return;  // whole warps exit together
   const int seg = (int)(warp % nseg);
   const long long row = warp / nseg;
-  const int b = (int)(row / nrow);
-  const long long rr = row - (long long)b * nrow;
+  const int bb = (int)(row / nrow);
+  const long long rr = row - (long long)bb * nrow;
+  const int b = slot_of(d, bb);
   const int k = k0 + (int)(rr / (j1 - j0 + 1));
   const int j = j0 + (int)(rr % (j1 - j0 + 1));
   const int c = i0 - 1 + seg * kFacesPerWarp + lane;
@@ -578,7 +624,7 @@ __device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_param
   const int run = (int)(r % nruns);
   r /= nruns;
   const int a = a0 + (int)(r % na);
-  const int b = (int)(r / na);
+  const int b = slot_of(d, (int)(r / na));
   const long long stride = DIR == 2 ? (long long)d.N1 : (long long)d.N1 * d.N2;
   const bool use_mc = p.limiter == PANGU_LIMITER_MC;
   const int f0 = m0 + run * kMarch;
@@ -634,6 +680,7 @@ __global__ void __launch_bounds__(kThreads) k_ct_emf(Dims d, const double *F1, c
   const int o1 = d.N1 > 1, o2 = d.N2 > 1, o3 = d.N3 > 1;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, d.ks, d.ke + o3, d.js, d.je + o2, d.is, d.ie + o1, b, k, j, i)) return;
+  b = slot_of(d, b);
   const long long sj = d.N1, sk = (long long)d.N1 * d.N2;
   double e1 = 0.0, e2 = 0.0, e3 = 0.0;
   if (o2 && o3) {
@@ -662,6 +709,7 @@ __global__ void __launch_bounds__(kThreads) k_ct_faces(Dims d, int dir, double *
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int ei = dir == 1 ? o1 : 0, ej = dir == 2 ? o2 : 0, ek = dir == 3 ? o3 : 0;
   if (!box_index(t, d.NB, d.ks, d.ke + ek, d.js, d.je + ej, d.is, d.ie + ei, b, k, j, i)) return;
+  b = slot_of(d, b);
   const long long sj = d.N1, sk = (long long)d.N1 * d.N2;
   const long long e0 = aidx(d, b, 0, k, j, i), e1 = aidx(d, b, 1, k, j, i),
                   e2 = aidx(d, b, 2, k, j, i);
@@ -690,10 +738,13 @@ __global__ void __launch_bounds__(kThreads) k_flux_div_update(Dims d, const doub
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB * d.NF, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
-  // b here runs over (block, variable) pairs; vidx with NF=1 view.
-  const long long q = ((long long)b * d.N3 + k) * (long long)d.N2 * d.N1 + (long long)j * d.N1 + i;
-  const double A1 = MUL(d.dx[1], d.dx[2]), A2 = MUL(d.dx[0], d.dx[2]), A3 = MUL(d.dx[0], d.dx[1]);
-  const double V = MUL(MUL(d.dx[0], d.dx[1]), d.dx[2]);
+  // b here runs over (active block, variable) pairs
+  const int v = b % d.NF;
+  b = slot_of(d, b / d.NF);
+  const long long q = vidx(d, b, v, k, j, i);
+  const double dx0 = dx_of(d, b, 0), dx1 = dx_of(d, b, 1), dx2 = dx_of(d, b, 2);
+  const double A1 = MUL(dx1, dx2), A2 = MUL(dx0, dx2), A3 = MUL(dx0, dx1);
+  const double V = MUL(MUL(dx0, dx1), dx2);
   double du = SUB(MUL(A1, F1[q + 1]), MUL(A1, F1[q]));
   if (d.ndim >= 2) du = ADD(du, SUB(MUL(A2, F2[q + d.N1]), MUL(A2, F2[q])));
   if (d.ndim == 3) {
@@ -701,7 +752,7 @@ __global__ void __launch_bounds__(kThreads) k_flux_div_update(Dims d, const doub
     du = ADD(du, SUB(MUL(A3, F3[q + sk]), MUL(A3, F3[q])));
   }
   const double dudt = DIV(-du, V);
-  const double bdt = MUL(beta, *dt);
+  const double bdt = MUL(beta, dt[job_of(d, b)]);
   Uout[q] = ADD(Uinit[q], MUL(bdt, dudt));
 }
 
@@ -779,6 +830,7 @@ __global__ void __launch_bounds__(kThreads) k_source(Dims d, pangu_params p, con
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
+  b = slot_of(d, b);
   if (MT == MINKOWSKI) return;  // connection identically zero (christoffel.h:90)
   Geo g;
   cell_metric<MT>(d, p, b, k, j, i, g);
@@ -790,7 +842,7 @@ __global__ void __launch_bounds__(kThreads) k_source(Dims d, pangu_params p, con
   double T[4][4];
 #pragma unroll
   for (int r = 0; r < 4; ++r) emt_from_state(p.adiabatic_index, pc, s, r, T[r]);
-  const double bdt = beta * (*dt);
+  const double bdt = beta * dt[job_of(d, b)];
   if (MT == MKS || MT == BL) {
     // Christoffel symbols from the centre table; structural zeros skipped
     constexpr TabLayout L = tab_layout(MT);
@@ -837,8 +889,9 @@ __global__ void __launch_bounds__(kThreads) k_build_tables(Dims d, pangu_params 
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long per = pc + p1 + p2;
   if (t >= per * d.NB) return;
-  const int b = (int)(t / per);
-  t -= (long long)b * per;
+  const int bb = (int)(t / per);
+  t -= (long long)bb * per;
+  const int b = slot_of(d, bb);
   int which, W;
   long long plane;
   double *tab;
@@ -955,6 +1008,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_recovery(Dims d, pangu_params p
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
+  b = slot_of(d, b);
   const bool robuster = p.recovery == PANGU_RECOVERY_ROBUSTER;
   const long long fc = cidx(d, b, k, j, i);
   if (MT == CKS) {
@@ -963,7 +1017,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_recovery(Dims d, pangu_params p
     const double rad2 = x * x + y * y + z * z;
     const double sa = (rad2 - a2) * (rad2 - a2) + 4.0 * a2 * z * z;
     const bool exc = sqrt(0.5 * (rad2 - a2 + sqrt(sa))) < p.r_excise;
-    count(cnt, PANGU_CNT_EXCISED, exc);
+    count(cnt, job_of(d, b), PANGU_CNT_EXCISED, exc);
     if (exc) {
       if (!robuster) flag[fc] = 0;
       return;
@@ -976,13 +1030,13 @@ __global__ void __launch_bounds__(kThreads, 3) k_recovery(Dims d, pangu_params p
   const double gam = p.adiabatic_index;
   if (robuster) {
     const int st = invert_kastaun(UH, PH, gam, g);
-    count(cnt, PANGU_CNT_KASTAUN_FAIL, st != 0);
+    count(cnt, job_of(d, b), PANGU_CNT_KASTAUN_FAIL, st != 0);
     if (st != 0) return;
   } else {
     Harm hs;
     harm_setup<MT>(UH, g, hs);
     const bool ok = invert_2d<MT>(UH, PH, gam, g, hs) == 0;
-    count(cnt, PANGU_CNT_C2P_2D, ok);
+    count(cnt, job_of(d, b), PANGU_CNT_C2P_2D, ok);
     append(nretry, retry, !ok, fc);
     flag[fc] = ok ? 1.0 : 0.0;
     if (!ok) return;
@@ -1015,11 +1069,11 @@ __global__ void __launch_bounds__(kThreads) k_recovery_retry(Dims d, pangu_param
     Harm hs;
     harm_setup<MT>(UH, g, hs);
     bool ok = invert_1dvsq<MT>(UH, PH, gam, g, hs) == 0;
-    count(cnt, PANGU_CNT_C2P_1DVSQ, ok);
+    count(cnt, job_of(d, b), PANGU_CNT_C2P_1DVSQ, ok);
     if (!ok) {
       ok = invert_1d<MT>(UH, PH, gam, g, hs) == 0;
-      count(cnt, PANGU_CNT_C2P_1D, ok);
-      count(cnt, PANGU_CNT_C2P_FAIL, !ok);
+      count(cnt, job_of(d, b), PANGU_CNT_C2P_1D, ok);
+      count(cnt, job_of(d, b), PANGU_CNT_C2P_FAIL, !ok);
     }
     flag[fc] = ok ? 1.0 : 0.0;
     c2p_write(d, P, b, k, j, i, PH);
@@ -1035,6 +1089,7 @@ __global__ void __launch_bounds__(kThreads) k_heating(Dims d, pangu_params p, do
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
+  b = slot_of(d, b);
   Geo g;
   cell_metric<MT>(d, p, b, k, j, i, g);
   double pc[NPRIM];
@@ -1060,6 +1115,7 @@ __global__ void __launch_bounds__(kThreads) k_fixrec_scan(Dims d, pangu_params p
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
+  b = slot_of(d, b);
   const long long fc = cidx(d, b, k, j, i);
   if (flag[fc] != 0) return;
   if (p.metric_type == PANGU_METRIC_CKS) {
@@ -1117,8 +1173,8 @@ __global__ void __launch_bounds__(kThreads) k_fixrec_write(Dims d, const int *co
     for (int v = 0; v < d.NF; ++v) P[(b * d.NF + v) * d.ncell + c] = vals[t * d.NF + v];
     for (int v = 2; v < 5; ++v) P[(b * d.NF + v) * d.ncell + c] = 0.;
     flag[fc] = 1;
+    count(cnt, job_of(d, (int)b), PANGU_CNT_FIXRECOVERY, true);
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&cnt[PANGU_CNT_FIXRECOVERY], (unsigned long long)n);
 }
 
 // ---------------------------------------------------------------------------
@@ -1129,23 +1185,19 @@ __global__ void __launch_bounds__(kThreads) k_fixrec_write(Dims d, const int *co
 // the index, with the reflections' sign flips composed. The kernel computes
 // that composition directly; its sources are never written by it.
 // ---------------------------------------------------------------------------
-struct BCInfo {
-  int kind[6];   // per face: PANGU_BC_OUTFLOW / REFLECTING, or -1 (periodic / inactive)
-  int nb[3];     // block lattice
-};
-
-__global__ void __launch_bounds__(kThreads) k_bcs(Dims d, BCInfo bc, int enable_B, double *P,
+__global__ void __launch_bounds__(kThreads) k_bcs(Dims d, int enable_B, double *P,
                                                   double *flag) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)d.NB * d.ncell) return;
-  const int b = (int)(t / d.ncell);
-  long long c = t - (long long)b * d.ncell;
+  const int bb = (int)(t / d.ncell);
+  long long c = t - (long long)bb * d.ncell;
+  const int b = slot_of(d, bb);
   int idx[3];
   idx[2] = (int)(c / ((long long)d.N2 * d.N1));
   c -= (long long)idx[2] * d.N2 * d.N1;
   idx[1] = (int)(c / d.N1);
   idx[0] = (int)(c % d.N1);
-  const int bl[3] = {b % bc.nb[0], (b / bc.nb[0]) % bc.nb[1], b / (bc.nb[0] * bc.nb[1])};
+  const signed char *bcf = d.bcf + 6 * b;  // -1 unless the face is a physical boundary
   const int st[3] = {d.is, d.js, d.ks}, en[3] = {d.ie, d.je, d.ke};
   int src[3] = {idx[0], idx[1], idx[2]};
   int flip[3] = {0, 0, 0};
@@ -1154,10 +1206,10 @@ __global__ void __launch_bounds__(kThreads) k_bcs(Dims d, BCInfo bc, int enable_
   for (int dir = 0; dir < 3; ++dir) {
     const int x = src[dir];
     int kind = -1, outer = 0;
-    if (x < st[dir] && bl[dir] == 0) {
-      kind = bc.kind[2 * dir];
-    } else if (x > en[dir] && bl[dir] == bc.nb[dir] - 1) {
-      kind = bc.kind[2 * dir + 1];
+    if (x < st[dir]) {
+      kind = bcf[2 * dir];
+    } else if (x > en[dir]) {
+      kind = bcf[2 * dir + 1];
       outer = 1;
     }
     if (kind < 0) continue;
@@ -1202,12 +1254,13 @@ __global__ void __launch_bounds__(kThreads) k_dt_reduce(Dims d, double cfl,
                                                         const double *alfven,
                                                         unsigned long long *mins) {
   __shared__ unsigned long long red[3][kThreads / 32];
-  const int b = blockIdx.y;
+  const int b = slot_of(d, blockIdx.y);
   const int ni = d.ie - d.is + 1, nj = d.je - d.js + 1, nk = d.ke - d.ks + 1;
   const long long per = (long long)ni * nj * nk;
   const unsigned long long big = (unsigned long long)__double_as_longlong(DBL_MAX);
   unsigned long long m[3] = {big, big, big};
-  const double cdx[3] = {MUL(cfl, d.dx[0]), MUL(cfl, d.dx[1]), MUL(cfl, d.dx[2])};
+  const double cdx[3] = {MUL(cfl, dx_of(d, b, 0)), MUL(cfl, dx_of(d, b, 1)),
+                         MUL(cfl, dx_of(d, b, 2))};
   const int act[3] = {d.N1 > 1, d.N2 > 1, d.N3 > 1};
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < per;
        t += (long long)gridDim.x * blockDim.x) {
@@ -1244,23 +1297,35 @@ __global__ void __launch_bounds__(kThreads) k_dt_reduce(Dims d, double cfl,
   }
 }
 
-__global__ void k_dt_finalize(int NB, const unsigned long long *mins, double *dt_out) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  double gmin = DBL_MAX;
-  for (int b = 0; b < NB; ++b) {
-    const double m0 = __longlong_as_double((long long)mins[3 * b + 0]);
-    const double m1 = __longlong_as_double((long long)mins[3 * b + 1]);
-    const double m2 = __longlong_as_double((long long)mins[3 * b + 2]);
-    const double bdt = 1.0 / (1.0 / m0 + 1.0 / m1 + 1.0 / m2);
-    if (bdt < gmin) gmin = bdt;
+// One thread per job: the minimum over the job's blocks, active entries
+// jr[3q+1] .. jr[3q+2]-1 of job jr[3q] (the whole domain as job 0 when jr is
+// null), written to dt_out[job].
+__global__ void k_dt_finalize(Dims d, int njobs, const int *jr, const unsigned long long *mins,
+                              double *dt_out) {
+  if (blockIdx.x != 0) return;
+  for (int q = threadIdx.x; q < njobs; q += blockDim.x) {
+    const int job = jr ? jr[3 * q] : 0;
+    const int s0 = jr ? jr[3 * q + 1] : 0, s1 = jr ? jr[3 * q + 2] : d.NB;
+    double gmin = DBL_MAX;
+    for (int bb = s0; bb < s1; ++bb) {
+      const int b = slot_of(d, bb);
+      const double m0 = __longlong_as_double((long long)mins[3 * b + 0]);
+      const double m1 = __longlong_as_double((long long)mins[3 * b + 1]);
+      const double m2 = __longlong_as_double((long long)mins[3 * b + 2]);
+      const double bdt = 1.0 / (1.0 / m0 + 1.0 / m1 + 1.0 / m2);
+      if (bdt < gmin) gmin = bdt;
+    }
+    dt_out[job] = gmin;
   }
-  *dt_out = gmin;
 }
 
-__global__ void k_update_dt(double *dt, const double *dt_est, double factor) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    const double grown = factor * (*dt);
-    *dt = (*dt_est < grown) ? *dt_est : grown;
+__global__ void k_update_dt(int njobs, const int *jr, double *dt, const double *dt_est,
+                            double factor) {
+  if (blockIdx.x != 0) return;
+  for (int q = threadIdx.x; q < njobs; q += blockDim.x) {
+    const int job = jr ? jr[3 * q] : 0;
+    const double grown = factor * dt[job];
+    dt[job] = (dt_est[job] < grown) ? dt_est[job] : grown;
   }
 }
 
@@ -1388,12 +1453,17 @@ int run_update(pangu_engine *e, const pangu_pack *mi, const pangu_pack *m0, cons
   return check_launch();
 }
 
-int run_exchange(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
-  if (e->nxch == 0) return PANGU_OK;
-  k_exchange<<<grid_for(e->nxch), kThreads, 0, s>>>(e->d, e->nxch, e->d_xdst, e->d_xsrc,
-                                                    md->prim, md->flag);
+int run_exchange_range(pangu_engine *e, const pangu_pack *md, long long off, long long n,
+                       cudaStream_t s) {
+  if (n == 0) return PANGU_OK;
+  k_exchange<<<grid_for(n), kThreads, 0, s>>>(e->d, n, e->d_xdst + off, e->d_xsrc + off, md->prim,
+                                              md->flag);
   ++e->launches;
   return check_launch();
+}
+
+int run_exchange(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
+  return run_exchange_range(e, md, 0, e->nxch, s);
 }
 
 int run_source(pangu_engine *e, const pangu_pack *md, double beta, const double *dt,
@@ -1445,34 +1515,27 @@ int run_fix_recovery(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
   return check_launch();
 }
 
-int run_bcs(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
-  const Dims &d = e->d;
-  const int act[3] = {d.o1, d.o2, d.o3};
-  BCInfo bc;
-  bool any = false;
-  for (int face = 0; face < 6; ++face) {
-    const int kind = e->m.bc[face];
-    bc.kind[face] = (act[face / 2] && kind != PANGU_BC_PERIODIC) ? kind : -1;
-    any = any || bc.kind[face] >= 0;
-  }
-  if (!any) return PANGU_OK;
-  bc.nb[0] = e->m.nbx1;
-  bc.nb[1] = e->m.nbx2;
-  bc.nb[2] = e->m.nbx3;
-  k_bcs<<<grid_for((long long)d.NB * d.ncell), kThreads, 0, s>>>(d, bc, e->p.enable_B, md->prim,
+// Physical BCs of the blocks of d (all active blocks, or one job's).
+int run_bcs(pangu_engine *e, const Dims &d, bool any_bc, const pangu_pack *md, cudaStream_t s) {
+  if (!any_bc || d.NB == 0) return PANGU_OK;
+  k_bcs<<<grid_for((long long)d.NB * d.ncell), kThreads, 0, s>>>(d, e->p.enable_B, md->prim,
                                                                 md->flag);
   ++e->launches;
   return check_launch();
 }
 
+int run_bcs(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
+  return run_bcs(e, e->d, e->any_bc, md, s);
+}
+
 int run_estimate_dt(pangu_engine *e, const pangu_pack *md, double *dt_out, cudaStream_t s) {
   const Dims &d = e->d;
-  k_dt_init<<<grid_for(3 * d.NB), kThreads, 0, s>>>(3 * d.NB, e->d_dtmin);
+  k_dt_init<<<grid_for(3 * e->capacity), kThreads, 0, s>>>(3 * e->capacity, e->d_dtmin);
   const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
   const unsigned gx = (unsigned)std::min<long long>((n / std::max(1, d.NB) + kThreads - 1) / kThreads, 592);
   k_dt_reduce<<<dim3(std::max(1u, gx), d.NB), kThreads, 0, s>>>(d, e->p.cfl_number, md->alfven,
                                                                  e->d_dtmin);
-  k_dt_finalize<<<1, 32, 0, s>>>(d.NB, e->d_dtmin, dt_out);
+  k_dt_finalize<<<1, 128, 0, s>>>(d, e->njobs_active, e->d_jr, e->d_dtmin, dt_out);
   e->launches += 3;
   return check_launch();
 }
@@ -1497,6 +1560,11 @@ int pangu_num_fields(const pangu_params *p) {
 
 int pangu_engine_destroy(pangu_engine *e) {
   if (!e) return PANGU_EINVAL;
+  cudaFree(e->d_active);
+  cudaFree(e->d_slot_job);
+  cudaFree(e->d_jr);
+  cudaFree(e->d_bdx);
+  cudaFree(e->d_bcf);
   cudaFree(e->d_t1);
   cudaFree(e->d_ctab);
   cudaFree(e->d_f1tab);
@@ -1514,45 +1582,59 @@ int pangu_engine_destroy(pangu_engine *e) {
   return PANGU_OK;
 }
 
-int pangu_engine_create(const pangu_params *params, const pangu_mesh *mesh, pangu_engine **out) {
-  if (!params || !mesh || !out) return PANGU_EINVAL;
-  *out = nullptr;
-  const pangu_params &p = *params;
-  const pangu_mesh &m = *mesh;
-  if (m.nx1 < 1 || m.nx2 < 1 || m.nx3 < 1 || m.nbx1 < 1 || m.nbx2 < 1 || m.nbx3 < 1 || m.ng < 0)
-    return PANGU_EINVAL;
+}  // extern "C"
+
+namespace {
+
+int validate_params(const pangu_params &p) {
   if (p.riemann_solver < 0 || p.riemann_solver > 1 || p.limiter < 0 || p.limiter > 1 ||
       p.recovery < 0 || p.recovery > 1 || p.metric_type < 0 || p.metric_type > 3 || p.model < 0 ||
       p.model > 5)
     return PANGU_EINVAL;
+  return PANGU_OK;
+}
+
+// Block shape checks shared by single meshes, pools and jobs.
+int validate_shape(const pangu_params &p, const pangu_mesh &m) {
+  if (m.nx1 < 1 || m.nx2 < 1 || m.nx3 < 1 || m.ng < 0) return PANGU_EINVAL;
   const int need_ng = p.limiter == PANGU_LIMITER_PPM4 ? 3 : 2;
   if (m.ng < need_ng) return PANGU_ENGHOST;
   const int act[3] = {m.nx1 > 1, m.nx2 > 1, m.nx3 > 1};
   const int nx[3] = {m.nx1, m.nx2, m.nx3};
   for (int dd = 0; dd < 3; ++dd)
     if (act[dd] && nx[dd] < m.ng) return PANGU_EINVAL;
+  return PANGU_OK;
+}
+
+int validate_mesh(const pangu_params &p, const pangu_mesh &m) {
+  if (m.nbx1 < 1 || m.nbx2 < 1 || m.nbx3 < 1) return PANGU_EINVAL;
   for (int f = 0; f < 6; ++f)
     if (m.bc[f] < 0 || m.bc[f] > 2) return PANGU_EINVAL;
-  pangu_engine *e = new (std::nothrow) pangu_engine;
-  if (!e) return PANGU_ENOMEM;
-  e->p = p;
-  e->m = m;
-  pgh::Layout L = pgh::make_layout(p, m);
+  return validate_shape(p, m);
+}
+
+// Allocates an empty pool of `capacity` block slots for up to `max_jobs`
+// jobs with the block shape of e->m.
+int pool_init(pangu_engine *e, int capacity, int max_jobs) {
+  const pangu_params &p = e->p;
+  pangu_mesh one = e->m;
+  one.nbx1 = one.nbx2 = one.nbx3 = 1;
+  const pgh::Layout L = pgh::make_layout(p, one);
   Dims &d = e->d;
+  d = Dims{};
   d.N1 = L.N[0];
   d.N2 = L.N[1];
   d.N3 = L.N[2];
   d.NF = L.NF;
-  d.NB = L.NB;
-  d.o1 = act[0];
-  d.o2 = act[1];
-  d.o3 = act[2];
+  d.NB = 0;
+  d.o1 = L.act[0];
+  d.o2 = L.act[1];
+  d.o3 = L.act[2];
   d.ndim = 1 + d.o2 + d.o3;
-  d.is = L.st[0]; d.ie = d.is + m.nx1 - 1;
-  d.js = L.st[1]; d.je = d.js + m.nx2 - 1;
-  d.ks = L.st[2]; d.ke = d.ks + m.nx3 - 1;
+  d.is = L.st[0]; d.ie = d.is + e->m.nx1 - 1;
+  d.js = L.st[1]; d.je = d.js + e->m.nx2 - 1;
+  d.ks = L.st[2]; d.ke = d.ks + e->m.nx3 - 1;
   d.ncell = (long long)d.N1 * d.N2 * d.N3;
-  for (int dd = 0; dd < 3; ++dd) d.dx[dd] = L.dx[dd];
   int n = 0;
   for (int s = 0; s < NPRIM; ++s) d.pidx[s] = -1;
   d.pidx[RHO] = n++; d.pidx[ENY] = n++;
@@ -1561,75 +1643,300 @@ int pangu_engine_create(const pangu_params *params, const pangu_mesh *mesh, pang
   d.pidx[ENT] = n++;
   if (p.enable_heating) d.pidx[KEL] = n++;
 
-  std::vector<double> t1, t2;
-  pgh::build_tables(p, L, t1, t2);
-  std::vector<int64_t> xdst, xsrc;
-  pgh::build_exchange(m, L, xdst, xsrc);
-  e->nxch = (long long)xdst.size();
-  e->fail_cap = (long long)d.NB * m.nx1 * m.nx2 * m.nx3;
+  e->capacity = capacity;
+  e->max_jobs = max_jobs;
+  e->jobs.assign(max_jobs, PoolJob{});
+  e->slot_used.assign(capacity, 0);
+  e->xoff.assign(max_jobs, 0);
+  const size_t W1 = d.N1 + 1, W2 = d.N2 + 1;
+  e->fail_cap = (long long)capacity * e->m.nx1 * e->m.nx2 * e->m.nx3;
   int rc = PANGU_OK;
-  rc |= dalloc(&e->d_t1, t1.size());
-  rc |= dalloc(&e->d_t2, t2.size());
-  rc |= dalloc(&e->d_origin, L.origin.size());
-  rc |= dalloc(&e->d_xdst, xdst.size());
-  rc |= dalloc(&e->d_xsrc, xsrc.size());
-  rc |= dalloc(&e->d_cnt, PANGU_NCOUNTERS);
+  rc |= dalloc(&e->d_active, capacity);
+  rc |= dalloc(&e->d_slot_job, capacity);
+  rc |= dalloc(&e->d_jr, 3 * (size_t)max_jobs);
+  rc |= dalloc(&e->d_bdx, 3 * (size_t)capacity);
+  rc |= dalloc(&e->d_bcf, 6 * (size_t)capacity);
+  rc |= dalloc(&e->d_t1, (size_t)capacity * kT1Rows * W1);
+  rc |= dalloc(&e->d_t2, (size_t)capacity * 12 * W2);
+  rc |= dalloc(&e->d_origin, 3 * (size_t)capacity);
+  rc |= dalloc(&e->d_cnt, (size_t)max_jobs * PANGU_NCOUNTERS);
   rc |= dalloc(&e->d_fail_count, 1);
   rc |= dalloc(&e->d_fail_list, (size_t)e->fail_cap);
   rc |= dalloc(&e->d_fail_vals, (size_t)e->fail_cap * d.NF);
-  rc |= dalloc(&e->d_dtmin, 3 * (size_t)d.NB);
-  if (rc != PANGU_OK) {
-    pangu_engine_destroy(e);
-    return PANGU_ENOMEM;
+  rc |= dalloc(&e->d_dtmin, 3 * (size_t)capacity);
+  if (p.metric_type == PANGU_METRIC_MKS || p.metric_type == PANGU_METRIC_BL) {
+    const TabLayout T = p.metric_type == PANGU_METRIC_MKS ? tab_layout(MKS) : tab_layout(BL);
+    const size_t pc = (size_t)d.N2 * d.N1, p1 = (size_t)d.N2 * (d.N1 + 1),
+                 p2 = (size_t)(d.N2 + 1) * d.N1;
+    rc |= dalloc(&e->d_ctab, (size_t)capacity * T.ncen * pc);
+    rc |= dalloc(&e->d_f1tab, (size_t)capacity * T.nmet * p1);
+    rc |= dalloc(&e->d_f2tab, (size_t)capacity * T.nmet * p2);
   }
-  bool ok = cudaMemcpy(e->d_t1, t1.data(), t1.size() * 8, cudaMemcpyHostToDevice) == cudaSuccess;
-  ok &= cudaMemcpy(e->d_t2, t2.data(), t2.size() * 8, cudaMemcpyHostToDevice) == cudaSuccess;
-  ok &= cudaMemcpy(e->d_origin, L.origin.data(), L.origin.size() * 8, cudaMemcpyHostToDevice) ==
-        cudaSuccess;
-  if (!xdst.empty()) {
-    ok &= cudaMemcpy(e->d_xdst, xdst.data(), xdst.size() * 8, cudaMemcpyHostToDevice) == cudaSuccess;
-    ok &= cudaMemcpy(e->d_xsrc, xsrc.data(), xsrc.size() * 8, cudaMemcpyHostToDevice) == cudaSuccess;
-  }
-  ok &= cudaMemset(e->d_cnt, 0, PANGU_NCOUNTERS * sizeof(unsigned long long)) == cudaSuccess;
-  if (!ok) {
-    pangu_engine_destroy(e);
-    return PANGU_ECUDA;
-  }
+  if (rc != PANGU_OK) return PANGU_ENOMEM;
+  bool ok = cudaMemset(e->d_cnt, 0, (size_t)max_jobs * PANGU_NCOUNTERS * 8) == cudaSuccess;
+  ok &= cudaMemset(e->d_slot_job, 0, (size_t)capacity * sizeof(int)) == cudaSuccess;
+  ok &= cudaMemset(e->d_bcf, 0xff, 6 * (size_t)capacity) == cudaSuccess;  // -1: no BC
+  if (!ok) return PANGU_ECUDA;
+  d.slot = e->d_active;
+  d.slot_job = e->d_slot_job;
+  d.bdx = e->d_bdx;
+  d.bcf = e->d_bcf;
   d.t1 = e->d_t1;
   d.t2 = e->d_t2;
   d.origin = e->d_origin;
-  d.ctab = d.f1tab = d.f2tab = nullptr;
-  if (p.metric_type == PANGU_METRIC_MKS || p.metric_type == PANGU_METRIC_BL) {
-    const TabLayout L = p.metric_type == PANGU_METRIC_MKS ? tab_layout(MKS) : tab_layout(BL);
-    const size_t pc = (size_t)d.N2 * d.N1, p1 = (size_t)d.N2 * (d.N1 + 1),
-                 p2 = (size_t)(d.N2 + 1) * d.N1;
-    int rc2 = PANGU_OK;
-    rc2 |= dalloc(&e->d_ctab, (size_t)d.NB * L.ncen * pc);
-    rc2 |= dalloc(&e->d_f1tab, (size_t)d.NB * L.nmet * p1);
-    rc2 |= dalloc(&e->d_f2tab, (size_t)d.NB * L.nmet * p2);
-    if (rc2 != PANGU_OK) {
-      pangu_engine_destroy(e);
-      return PANGU_ENOMEM;
+  d.ctab = e->d_ctab;
+  d.f1tab = e->d_f1tab;
+  d.f2tab = e->d_f2tab;
+  return PANGU_OK;
+}
+
+// Active block list (jobs in id order, each job's blocks in lattice order),
+// per-job ranges and the concatenated exchange map, uploaded synchronously.
+int pool_rebuild(pangu_engine *e) {
+  std::vector<int> active, jr;
+  std::vector<int64_t> xd, xs;
+  e->any_bc = false;
+  for (int q = 0; q < e->max_jobs; ++q) {
+    const PoolJob &J = e->jobs[q];
+    if (!J.live) continue;
+    jr.push_back(q);
+    jr.push_back((int)active.size());
+    active.insert(active.end(), J.slots.begin(), J.slots.end());
+    jr.push_back((int)active.size());
+    e->xoff[q] = (long long)xd.size();
+    xd.insert(xd.end(), J.xdst.begin(), J.xdst.end());
+    xs.insert(xs.end(), J.xsrc.begin(), J.xsrc.end());
+    e->any_bc = e->any_bc || J.any_bc;
+  }
+  if ((long long)xd.size() > e->xch_cap) {
+    cudaFree(e->d_xdst);
+    cudaFree(e->d_xsrc);
+    e->d_xdst = e->d_xsrc = nullptr;
+    e->xch_cap = 0;
+    if (dalloc(&e->d_xdst, xd.size()) || dalloc(&e->d_xsrc, xs.size())) return PANGU_ENOMEM;
+    e->xch_cap = (long long)xd.size();
+  }
+  bool ok = true;
+  if (!active.empty())
+    ok &= cudaMemcpy(e->d_active, active.data(), active.size() * sizeof(int),
+                     cudaMemcpyHostToDevice) == cudaSuccess;
+  if (!jr.empty())
+    ok &= cudaMemcpy(e->d_jr, jr.data(), jr.size() * sizeof(int), cudaMemcpyHostToDevice) ==
+          cudaSuccess;
+  if (!xd.empty()) {
+    ok &= cudaMemcpy(e->d_xdst, xd.data(), xd.size() * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+    ok &= cudaMemcpy(e->d_xsrc, xs.data(), xs.size() * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+  }
+  if (!ok) return PANGU_ECUDA;
+  e->d.NB = (int)active.size();
+  e->nxch = (long long)xd.size();
+  e->njobs_active = (int)(jr.size() / 3);
+  return PANGU_OK;
+}
+
+// Places a job's blocks in free slots (lowest first) and builds their
+// coordinate tables, metric tables, BC faces and exchange map.
+int pool_attach(pangu_engine *e, const pangu_mesh &m, double a, double h, int *job_out,
+                int32_t *slots_out) {
+  if (m.nx1 != e->m.nx1 || m.nx2 != e->m.nx2 || m.nx3 != e->m.nx3 || m.ng != e->m.ng)
+    return PANGU_EINVAL;
+  int rc = validate_mesh(e->p, m);
+  if (rc) return rc;
+  const long long nbl = (long long)m.nbx1 * m.nbx2 * m.nbx3;
+  int job = -1;
+  for (int q = 0; q < e->max_jobs && job < 0; ++q)
+    if (!e->jobs[q].live) job = q;
+  if (job < 0) return PANGU_EFULL;
+  std::vector<int> slots;
+  for (int sl = 0; sl < e->capacity && (long long)slots.size() < nbl; ++sl)
+    if (!e->slot_used[sl]) slots.push_back(sl);
+  if ((long long)slots.size() < nbl) return PANGU_EFULL;
+  if (cudaDeviceSynchronize() != cudaSuccess) return PANGU_ECUDA;
+
+  PoolJob J;
+  J.m = m;
+  J.p = e->p;
+  J.p.a = a;
+  J.p.h = h;
+  J.slots = slots;
+  const pgh::Layout L = pgh::make_layout(J.p, m);
+  std::vector<double> t1, t2;
+  pgh::build_tables(J.p, L, t1, t2);
+  std::vector<int64_t> xd, xs;
+  pgh::build_exchange(m, L, xd, xs);
+  const Dims &d = e->d;
+  const long long nc = d.ncell;
+  for (size_t q = 0; q < xd.size(); ++q) {
+    xd[q] = (int64_t)slots[xd[q] / nc] * nc + xd[q] % nc;
+    xs[q] = (int64_t)slots[xs[q] / nc] * nc + xs[q] % nc;
+  }
+  J.xdst.swap(xd);
+  J.xsrc.swap(xs);
+  const size_t W1 = d.N1 + 1, W2 = d.N2 + 1;
+  const size_t r1 = (size_t)kT1Rows * W1, r2 = 12 * W2;
+  const int nbv[3] = {m.nbx1, m.nbx2, m.nbx3};
+  const int act[3] = {d.o1, d.o2, d.o3};
+  bool ok = true;
+  for (long long b = 0; b < nbl; ++b) {
+    const int sl = slots[b];
+    const int bl[3] = {(int)(b % m.nbx1), (int)((b / m.nbx1) % m.nbx2),
+                       (int)(b / ((long long)m.nbx1 * m.nbx2))};
+    signed char bcf[6];
+    for (int f = 0; f < 6; ++f) {
+      const int dir = f / 2;
+      const bool edge = (f % 2 == 0) ? bl[dir] == 0 : bl[dir] == nbv[dir] - 1;
+      bcf[f] = (act[dir] && edge && m.bc[f] != PANGU_BC_PERIODIC) ? (signed char)m.bc[f] : -1;
+      J.any_bc = J.any_bc || bcf[f] >= 0;
     }
-    const long long n = (long long)d.NB * (pc + p1 + p2);
-    if (p.metric_type == PANGU_METRIC_MKS)
-      k_build_tables<MKS><<<grid_for(n), kThreads>>>(d, p, e->d_ctab, e->d_f1tab, e->d_f2tab);
-    else
-      k_build_tables<BL><<<grid_for(n), kThreads>>>(d, p, e->d_ctab, e->d_f1tab, e->d_f2tab);
-    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
-      pangu_engine_destroy(e);
-      return PANGU_ECUDA;
+    ok &= cudaMemcpy(e->d_t1 + sl * r1, &t1[b * r1], r1 * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+    ok &= cudaMemcpy(e->d_t2 + sl * r2, &t2[b * r2], r2 * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+    ok &= cudaMemcpy(e->d_origin + 3 * sl, &L.origin[3 * b], 24, cudaMemcpyHostToDevice) ==
+          cudaSuccess;
+    ok &= cudaMemcpy(e->d_bdx + 3 * sl, L.dx, 24, cudaMemcpyHostToDevice) == cudaSuccess;
+    ok &= cudaMemcpy(e->d_bcf + 6 * sl, bcf, 6, cudaMemcpyHostToDevice) == cudaSuccess;
+    ok &= cudaMemcpy(e->d_slot_job + sl, &job, sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
+  }
+  ok &= cudaMemset(e->d_cnt + (size_t)job * PANGU_NCOUNTERS, 0, PANGU_NCOUNTERS * 8) == cudaSuccess;
+  if (!ok) return PANGU_ECUDA;
+  if (e->p.metric_type == PANGU_METRIC_MKS || e->p.metric_type == PANGU_METRIC_BL) {
+    // static metric tables of the job's slots, with the job's a and h
+    int *d_slots = nullptr;
+    if (dalloc(&d_slots, slots.size())) return PANGU_ENOMEM;
+    ok = cudaMemcpy(d_slots, slots.data(), slots.size() * sizeof(int), cudaMemcpyHostToDevice) ==
+         cudaSuccess;
+    Dims dj = d;
+    dj.slot = d_slots;
+    dj.NB = (int)nbl;
+    const long long n = (long long)dj.NB * ((long long)d.N2 * d.N1 + (long long)d.N2 * (d.N1 + 1) +
+                                            (long long)(d.N2 + 1) * d.N1);
+    if (ok) {
+      if (e->p.metric_type == PANGU_METRIC_MKS)
+        k_build_tables<MKS><<<grid_for(n), kThreads>>>(dj, J.p, e->d_ctab, e->d_f1tab, e->d_f2tab);
+      else
+        k_build_tables<BL><<<grid_for(n), kThreads>>>(dj, J.p, e->d_ctab, e->d_f1tab, e->d_f2tab);
+      ok = cudaGetLastError() == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess;
     }
-    d.ctab = e->d_ctab;
-    d.f1tab = e->d_f1tab;
-    d.f2tab = e->d_f2tab;
+    cudaFree(d_slots);
+    if (!ok) return PANGU_ECUDA;
+  }
+  J.live = true;
+  for (int sl : slots) e->slot_used[sl] = 1;
+  e->jobs[job] = std::move(J);
+  rc = pool_rebuild(e);
+  if (rc) return rc;
+  *job_out = job;
+  if (slots_out)
+    for (long long b = 0; b < nbl; ++b) slots_out[b] = slots[b];
+  return PANGU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pangu_engine_create(const pangu_params *params, const pangu_mesh *mesh, pangu_engine **out) {
+  if (!params || !mesh || !out) return PANGU_EINVAL;
+  *out = nullptr;
+  int rc = validate_params(*params);
+  if (!rc) rc = validate_mesh(*params, *mesh);
+  if (rc) return rc;
+  pangu_engine *e = new (std::nothrow) pangu_engine;
+  if (!e) return PANGU_ENOMEM;
+  e->p = *params;
+  e->m = *mesh;
+  const int nb = mesh->nbx1 * mesh->nbx2 * mesh->nbx3;
+  rc = pool_init(e, nb, 1);
+  int job = -1;
+  if (!rc) rc = pool_attach(e, *mesh, params->a, params->h, &job, nullptr);
+  if (rc) {
+    pangu_engine_destroy(e);
+    return rc;
   }
   *out = e;
   return PANGU_OK;
 }
 
+int pangu_pool_create(const pangu_params *params, const pangu_mesh *block, int32_t capacity_blocks,
+                      int32_t max_jobs, pangu_engine **out) {
+  if (!params || !block || !out || capacity_blocks < 1 || max_jobs < 1) return PANGU_EINVAL;
+  *out = nullptr;
+  int rc = validate_params(*params);
+  if (!rc) rc = validate_shape(*params, *block);
+  if (rc) return rc;
+  pangu_engine *e = new (std::nothrow) pangu_engine;
+  if (!e) return PANGU_ENOMEM;
+  e->p = *params;
+  e->m = *block;
+  rc = pool_init(e, capacity_blocks, max_jobs);
+  if (rc) {
+    pangu_engine_destroy(e);
+    return rc;
+  }
+  *out = e;
+  return PANGU_OK;
+}
+
+int pangu_job_attach(pangu_engine *e, const pangu_mesh *mesh, double a, double h, int32_t *job_out,
+                     int32_t *slots_out) {
+  if (!e || !mesh || !job_out) return PANGU_EINVAL;
+  if (e->p.metric_type == PANGU_METRIC_CKS && (a != e->p.a || h != e->p.h)) return PANGU_EINVAL;
+  int job = -1;
+  const int rc = pool_attach(e, *mesh, a, h, &job, slots_out);
+  if (rc) return rc;
+  *job_out = job;
+  return PANGU_OK;
+}
+
+int pangu_job_start(pangu_engine *e, int32_t job, const pangu_pack *base, const pangu_pack *one,
+                    void *stream) {
+  if (!pack_ok(e, base) || !pack_ok(e, one) || job < 0 || job >= e->max_jobs ||
+      !e->jobs[job].live)
+    return PANGU_EINVAL;
+  cudaStream_t s = S(stream);
+  const PoolJob &J = e->jobs[job];
+  int first = 0;
+  for (int q = 0; q < job; ++q)
+    if (e->jobs[q].live) first += (int)e->jobs[q].slots.size();
+  Dims dj = e->d;
+  dj.slot = e->d_active + first;
+  dj.NB = (int)J.slots.size();
+  int rc = run_exchange_range(e, base, e->xoff[job], (long long)J.xdst.size(), s);
+  if (!rc) rc = run_bcs(e, dj, J.any_bc, base, s);
+  if (rc) return rc;
+  const size_t blk = (size_t)e->d.NF * e->d.ncell;
+  for (int sl : J.slots) {
+    if (cudaMemcpyAsync(one->prim + sl * blk, base->prim + sl * blk, blk * 8,
+                        cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(one->cons + sl * blk, base->cons + sl * blk, blk * 8,
+                        cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+      return PANGU_ECUDA;
+  }
+  return PANGU_OK;
+}
+
+int pangu_job_detach(pangu_engine *e, int32_t job) {
+  if (!e || job < 0 || job >= e->max_jobs || !e->jobs[job].live) return PANGU_EINVAL;
+  if (cudaDeviceSynchronize() != cudaSuccess) return PANGU_ECUDA;
+  for (int sl : e->jobs[job].slots) e->slot_used[sl] = 0;
+  e->jobs[job] = PoolJob{};
+  return pool_rebuild(e);
+}
+
+int pangu_job_counters(pangu_engine *e, int32_t job, uint64_t out[PANGU_NCOUNTERS]) {
+  if (!e || !out || job < 0 || job >= e->max_jobs) return PANGU_EINVAL;
+  unsigned long long tmp[PANGU_NCOUNTERS];
+  if (cudaMemcpy(tmp, e->d_cnt + (size_t)job * PANGU_NCOUNTERS, sizeof(tmp),
+                 cudaMemcpyDeviceToHost) != cudaSuccess)
+    return PANGU_ECUDA;
+  for (int i = 0; i < PANGU_NCOUNTERS; ++i) out[i] = tmp[i];
+  return PANGU_OK;
+}
+
+int pangu_active_blocks(const pangu_engine *e) { return e ? e->d.NB : PANGU_EINVAL; }
+
 #define GUARD(e, md)                      \
-  if (!pack_ok(e, md)) return PANGU_EINVAL;
+  if (!pack_ok(e, md)) return PANGU_EINVAL; \
+  if (e->d.NB == 0) return PANGU_OK;
 
 int pangu_fix_primitive(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
@@ -1652,6 +1959,7 @@ int pangu_flux_divergence_update(pangu_engine *e, const pangu_pack *mc_init, con
                                  const pangu_pack *mc1, double beta, const double *dt,
                                  void *stream) {
   if (!pack_ok(e, mc_init) || !pack_ok(e, mc0) || !pack_ok(e, mc1) || !dt) return PANGU_EINVAL;
+  if (e->d.NB == 0) return PANGU_OK;
   return run_update(e, mc_init, mc0, mc1, beta, dt, S(stream));
 }
 int pangu_exchange_ghosts(pangu_engine *e, const pangu_pack *md, void *stream) {
@@ -1691,6 +1999,7 @@ int pangu_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_
                 double beta, const double *dt, double *dt_est, void *stream) {
   if (!pack_ok(e, base) || !pack_ok(e, one) || !dt || (stage != 1 && stage != 2))
     return PANGU_EINVAL;
+  if (e->d.NB == 0) return PANGU_OK;
   cudaStream_t s = S(stream);
   const pangu_pack *mc0 = stage == 1 ? base : one;
   const pangu_pack *mc1 = stage == 1 ? one : base;
@@ -1781,24 +2090,28 @@ int pangu_estimate_dt_noalloc(const pangu_params *params, const pangu_mesh *mesh
       (unsigned)std::min<long long>((n / std::max(1, d.NB) + kThreads - 1) / kThreads, 592);
   k_dt_reduce<<<dim3(std::max(1u, gx), d.NB), kThreads, 0, s>>>(d, params->cfl_number, alfven,
                                                                  mins);
-  k_dt_finalize<<<1, 32, 0, s>>>(d.NB, mins, dt_out);
+  k_dt_finalize<<<1, 32, 0, s>>>(d, 1, nullptr, mins, dt_out);
   return check_launch();
 }
 
 int pangu_update_dt(pangu_engine *e, double *dt, const double *dt_est, double dt_factor,
                     void *stream) {
   if (!e || !dt || !dt_est) return PANGU_EINVAL;
-  k_update_dt<<<1, 32, 0, S(stream)>>>(dt, dt_est, dt_factor);
+  if (e->njobs_active == 0) return PANGU_OK;
+  k_update_dt<<<1, 128, 0, S(stream)>>>(e->njobs_active, e->d_jr, dt, dt_est, dt_factor);
   ++e->launches;
   return check_launch();
 }
 
 int pangu_counters(pangu_engine *e, uint64_t out[PANGU_NCOUNTERS]) {
   if (!e || !out) return PANGU_EINVAL;
-  unsigned long long tmp[PANGU_NCOUNTERS];
-  if (cudaMemcpy(tmp, e->d_cnt, sizeof(tmp), cudaMemcpyDeviceToHost) != cudaSuccess)
+  std::vector<unsigned long long> tmp((size_t)e->max_jobs * PANGU_NCOUNTERS);
+  if (cudaMemcpy(tmp.data(), e->d_cnt, tmp.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
     return PANGU_ECUDA;
-  for (int i = 0; i < PANGU_NCOUNTERS; ++i) out[i] = tmp[i];
+  for (int i = 0; i < PANGU_NCOUNTERS; ++i) {
+    out[i] = 0;
+    for (int q = 0; q < e->max_jobs; ++q) out[i] += tmp[(size_t)q * PANGU_NCOUNTERS + i];
+  }
   return PANGU_OK;
 }
 
@@ -1806,7 +2119,7 @@ long long pangu_launches(const pangu_engine *e) { return e ? e->launches : PANGU
 
 int pangu_reset_counters(pangu_engine *e, void *stream) {
   if (!e) return PANGU_EINVAL;
-  return cudaMemsetAsync(e->d_cnt, 0, PANGU_NCOUNTERS * sizeof(unsigned long long), S(stream)) ==
+  return cudaMemsetAsync(e->d_cnt, 0, (size_t)e->max_jobs * PANGU_NCOUNTERS * 8, S(stream)) ==
                  cudaSuccess
              ? PANGU_OK
              : PANGU_ECUDA;

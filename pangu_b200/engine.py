@@ -30,7 +30,8 @@ class EngineError(RuntimeError):
 _ERRORS = {abi.PANGU_EINVAL: "invalid argument", abi.PANGU_ECUDA: "CUDA error",
            abi.PANGU_ENOMEM: "out of device memory",
            abi.PANGU_ENGHOST: "ghost width too small for the limiter",
-           abi.PANGU_ETOOBIG: "size above the supported maximum"}
+           abi.PANGU_ETOOBIG: "size above the supported maximum",
+           abi.PANGU_EFULL: "no free pool slot or job id"}
 
 
 def _check(rc, what):
@@ -69,6 +70,14 @@ def lib():
     L.pangu_reset_counters.argtypes = [_P, _P]
     L.pangu_launches.argtypes = [_P]
     L.pangu_launches.restype = C.c_longlong
+    L.pangu_pool_create.argtypes = [C.POINTER(abi.Params), C.POINTER(abi.Mesh), C.c_int32,
+                                    C.c_int32, C.POINTER(_P)]
+    L.pangu_job_attach.argtypes = [_P, C.POINTER(abi.Mesh), C.c_double, C.c_double,
+                                   C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    L.pangu_job_start.argtypes = [_P, C.c_int32, _PK, _PK, _P]
+    L.pangu_job_detach.argtypes = [_P, C.c_int32]
+    L.pangu_job_counters.argtypes = [_P, C.c_int32, C.POINTER(C.c_uint64)]
+    L.pangu_active_blocks.argtypes = [_P]
     _lib = L
     return L
 
@@ -115,18 +124,24 @@ class DeviceContainer:
 class Engine:
     """An engine handle for one parameter set and mesh."""
 
-    def __init__(self, params: abi.Params, mesh: abi.Mesh, device=0):
+    def __init__(self, params: abi.Params, mesh: abi.Mesh, device=0, pool=None):
+        """pool=None: one mesh (pangu_engine_create). pool=(capacity_blocks,
+        max_jobs): an empty block pool of mesh's block shape."""
         torch = _torch()
         self.device = torch.device("cuda", device)
         self.L = lib()
         self.params, self.mesh = params, mesh
         h = _P()
         with torch.cuda.device(self.device):
-            _check(self.L.pangu_engine_create(C.byref(params), C.byref(mesh), C.byref(h)),
-                   "pangu_engine_create")
+            if pool is None:
+                _check(self.L.pangu_engine_create(C.byref(params), C.byref(mesh), C.byref(h)),
+                       "pangu_engine_create")
+            else:
+                _check(self.L.pangu_pool_create(C.byref(params), C.byref(mesh), int(pool[0]),
+                                                int(pool[1]), C.byref(h)), "pangu_pool_create")
         self.h = h
         self.nf = self.L.pangu_num_fields(C.byref(params))
-        self.nb = mesh.nbx1 * mesh.nbx2 * mesh.nbx3
+        self.nb = mesh.nbx1 * mesh.nbx2 * mesh.nbx3 if pool is None else int(pool[0])
         act = [mesh.nx1 > 1, mesh.nx2 > 1, mesh.nx3 > 1]
         n = [mesh.nx1, mesh.nx2, mesh.nx3]
         self.shape = tuple(n[d] + 2 * mesh.ng * act[d] for d in (2, 1, 0))
@@ -197,6 +212,30 @@ class Engine:
 
     def reset_counters(self):
         _check(self.L.pangu_reset_counters(self.h, self.stream()), "pangu_reset_counters")
+
+    # ---- block pool --------------------------------------------------------
+    def attach(self, mesh: abi.Mesh, a: float, h: float):
+        job = C.c_int32()
+        nbl = mesh.nbx1 * mesh.nbx2 * mesh.nbx3
+        slots = (C.c_int32 * nbl)()
+        _check(self.L.pangu_job_attach(self.h, C.byref(mesh), a, h, C.byref(job), slots),
+               "pangu_job_attach")
+        return job.value, list(slots)
+
+    def job_start(self, job, base, one):
+        _check(self.L.pangu_job_start(self.h, job, base.pack, one.pack, self.stream()),
+               "pangu_job_start")
+
+    def detach(self, job):
+        _check(self.L.pangu_job_detach(self.h, job), "pangu_job_detach")
+
+    def job_counters(self, job):
+        out = (C.c_uint64 * abi.NCOUNTERS)()
+        _check(self.L.pangu_job_counters(self.h, job, out), "pangu_job_counters")
+        return np.array(list(out), dtype=np.uint64)
+
+    def active_blocks(self) -> int:
+        return int(self.L.pangu_active_blocks(self.h))
 
 
 # rk2 of Parthenon's low-storage integrator: beta[stage % 2] with
@@ -271,3 +310,98 @@ class Simulation:
 
     def primitives(self) -> np.ndarray:
         return self.base.prim.cpu().numpy()
+
+
+class Pool:
+    """Many jobs of one block shape and parameter set (metric spin a and h may
+    differ per job) stepped together: every kernel of a stage is one launch
+    over the blocks of all attached jobs, through the engine's block table,
+    and a whole RK2 cycle of the pool is one CUDA graph replay.
+
+    ``template`` supplies the shared parameters and the block shape
+    (<parthenon/meshblock> nx*, nghost). Jobs are attached between cycles.
+    """
+
+    # params that may differ between the jobs of a pool
+    PER_JOB = ("a", "h")
+
+    def __init__(self, template: ParameterInput, capacity_blocks: int, max_jobs: int, device=0):
+        torch = _torch()
+        self.params = params_struct(process_packages(template))
+        block = mesh_struct(template)
+        block.nbx1 = block.nbx2 = block.nbx3 = 1
+        self.engine = Engine(self.params, block, device, pool=(capacity_blocks, max_jobs))
+        self.base, self.one = self.engine.new_containers()
+        dev = self.engine.device
+        self.dt = torch.zeros(max_jobs, dtype=torch.float64, device=dev)
+        self.dt_est = torch.zeros(max_jobs, dtype=torch.float64, device=dev)
+        self.dt_factor = template.get_or_add_real("parthenon/time", "dt_factor", 2.0)
+        self.capacity, self.max_jobs = capacity_blocks, max_jobs
+        self.jobs = {}      # job id -> slots
+        self._graph = None
+
+    def free_blocks(self) -> int:
+        return self.capacity - sum(len(s) for s in self.jobs.values())
+
+    def _check_compatible(self, p: abi.Params):
+        for name, _ in abi.Params._fields_:
+            if name in self.PER_JOB:
+                continue
+            if getattr(p, name) != getattr(self.params, name):
+                raise EngineError(f"job parameter {name} differs from the pool's")
+
+    def attach(self, pin: ParameterInput, prim: np.ndarray) -> int:
+        """Attaches a job with interior primitives ``prim`` ([block][var][k][j][i],
+        numpy or a device tensor), fills its ghosts and sets dt[job] = dt_init."""
+        torch = _torch()
+        p = params_struct(process_packages(pin))
+        self._check_compatible(p)
+        mesh = mesh_struct(pin)
+        job, slots = self.engine.attach(mesh, p.a, p.h)
+        idx = torch.tensor(slots, dtype=torch.long, device=self.engine.device)
+        src = torch.as_tensor(prim, device=self.engine.device, dtype=torch.float64)
+        self.base.prim.index_copy_(0, idx, src)
+        self.base.cons.index_fill_(0, idx, 0.0)
+        self.base.flag.index_fill_(0, idx, 0.0)
+        self.dt[job] = pin.get_or_add_real("parthenon/time", "dt_init", 1e-5)
+        self.engine.job_start(job, self.base, self.one)
+        self.jobs[job] = slots
+        self._graph = None
+        return job
+
+    def primitives(self, job) -> np.ndarray:
+        torch = _torch()
+        idx = torch.tensor(self.jobs[job], dtype=torch.long, device=self.engine.device)
+        return self.base.prim.index_select(0, idx).cpu().numpy()
+
+    def detach(self, job) -> np.ndarray:
+        """Detaches a job and returns its primitives."""
+        out = self.primitives(job)
+        self.engine.detach(job)
+        del self.jobs[job]
+        self._graph = None
+        return out
+
+    def _cycle(self):
+        e = self.engine
+        e.stage(1, self.base, self.one, RK2_BETA[1], self.dt)
+        e.stage(2, self.base, self.one, RK2_BETA[0], self.dt, self.dt_est)
+        e.update_dt(self.dt, self.dt_est, self.dt_factor)
+
+    def step(self, graph: bool = True):
+        """One RK2 cycle of every attached job."""
+        if not self.jobs:
+            return
+        if not graph:
+            self._cycle()
+            return
+        if self._graph is None:
+            import torch
+            s = torch.cuda.Stream(self.engine.device)
+            s.wait_stream(torch.cuda.current_stream(self.engine.device))
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=s):
+                self._cycle()
+            torch.cuda.current_stream(self.engine.device).wait_stream(s)
+            self._graph = g
+        self._graph.replay()
