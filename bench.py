@@ -143,6 +143,16 @@ def task_bytes(nf, n_int, n_ent, ndim):
     }
 
 
+def max_over_ranks(value, dist, device):
+    """Max of a per-rank time over all ranks: a multi-GPU run is as fast as
+    its slowest rank. The only collective of the benchmark (jobs are
+    independent, one per GPU; nothing crosses ranks on the data path)."""
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.item()
+
+
 def run_engine(args):
     import torch
     import torch.distributed as dist
@@ -193,9 +203,7 @@ def run_engine(args):
         launches = launches_per_step * args.steps
     total_ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
     if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = t.item()
+        total_ms = max_over_ranks(total_ms, dist, dev)
         dist.barrier()
     clocks = clk.summary()
     ms_per_step = total_ms / args.steps
@@ -204,9 +212,7 @@ def run_engine(args):
     # ---- end to end through the public API with host-resident state -------
     e2e = e2e_run(sim, torch, dev, min(args.steps, 100))
     if world > 1:
-        t = torch.tensor([e2e["ms"]], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e["ms"] = t.item()
+        e2e["ms"] = max_over_ranks(e2e["ms"], dist, dev)
 
     # ---- per-task breakdown and the dominant kernel's roofline ---------
     tasks = task_times(sim, torch, flush) if rank == 0 else {}

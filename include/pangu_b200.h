@@ -65,6 +65,15 @@ extern "C" {
 #define PANGU_HEAT_WERNER 3
 #define PANGU_HEAT_ROWAN 4
 #define PANGU_HEAT_SHARMA 5
+/* Arithmetic of the engine (no reference counterpart; the reference is
+ * FP64 throughout). MIXED stores primitives in FP32 (the pack's prim pointer
+ * then addresses floats) and runs reconstruction, Riemann flux and electron
+ * heating in FP32; conserved variables, the update, the source term, C2P, the
+ * metric and CT stay FP64. The conserved magnetic field is then evolved only
+ * by the FP64 CT update: CalculateConservative leaves it unchanged, and
+ * pangu_job_start computes it once from the initial primitives. */
+#define PANGU_PRECISION_FP64 0
+#define PANGU_PRECISION_MIXED 1
 /* Parthenon <parthenon/mesh> ix*_bc / ox*_bc */
 #define PANGU_BC_PERIODIC 0
 #define PANGU_BC_OUTFLOW 1
@@ -85,7 +94,7 @@ typedef struct pangu_params {
   int32_t enable_B;           /* false */
   int32_t recovery;           /* PANGU_RECOVERY_* (chainer) */
   int32_t enable_heating;     /* false */
-  int32_t reserved0;
+  int32_t precision;          /* PANGU_PRECISION_* (fp64); not a reference key */
   double sigma_max;           /* 50 */
   double lorentz_max;         /* 50 */
   /* <electron> */
@@ -249,7 +258,9 @@ long long pangu_launches(const pangu_engine *e);
  * kernel, reading dt[job] and writing dt_est[job]. The caller owns the
  * containers: packs sized for `capacity_blocks` blocks, slot-major. Results
  * are identical to running each job alone with pangu_engine_create.
- * attach/detach synchronise the device and change the launch domain, so a
+ * attach/detach need no work of this engine in flight (they rewrite the
+ * block table with blocking copies on the legacy default stream, and never
+ * synchronise the device or allocate); they change the launch domain, so a
  * CUDA graph captured before them must be captured again. */
 int pangu_pool_create(const pangu_params *params, const pangu_mesh *block,
                       int32_t capacity_blocks, int32_t max_jobs, pangu_engine **out);
@@ -261,7 +272,8 @@ int pangu_job_attach(pangu_engine *e, const pangu_mesh *mesh, double a, double h
                      int32_t *job_out, int32_t *slots_out);
 /* After the caller wrote a job's interior primitives into its slots of base:
  * fills its ghosts (exchange, then physical BCs) and copies base into one for
- * its slots, as Parthenon does after the problem generator. */
+ * its slots, as Parthenon does after the problem generator. With
+ * pangu_engine_create the mesh is job 0. */
 int pangu_job_start(pangu_engine *e, int32_t job, const pangu_pack *base,
                     const pangu_pack *one, void *stream);
 int pangu_job_detach(pangu_engine *e, int32_t job);
@@ -269,6 +281,46 @@ int pangu_job_detach(pangu_engine *e, int32_t job);
 int pangu_job_counters(pangu_engine *e, int32_t job, uint64_t out[PANGU_NCOUNTERS]);
 /* Blocks in the launch domain (all attached jobs). */
 int pangu_active_blocks(const pangu_engine *e);
+
+/* ---- serving: continuous batching over block pools --------------------- */
+/* No counterpart in the reference. A server owns one block pool per job
+ * class (parameter set + block shape), each with its containers, dt arrays,
+ * stream and captured RK2-cycle graph, allocated against an HBM budget when
+ * the class is added. pangu_server_run admits every submitted job once its
+ * arrival time (seconds after the run starts) has passed and its class pool
+ * has room (first fit in arrival order), steps the admitted jobs of each
+ * class one RK2 cycle per tick of that class (classes tick independently on
+ * their own streams, so their kernels overlap), copies each job's primitives
+ * back and detaches it after its last cycle. A job's result is identical to
+ * running it alone. */
+typedef struct pangu_server pangu_server;
+typedef struct pangu_server_stats {
+  int64_t jobs, ticks;
+  double wall_s;             /* host time of the whole run                   */
+  double zone_cycles;        /* interior cells x cycles, summed over jobs    */
+  double zone_cycles_per_s;  /* zone_cycles / wall_s                         */
+  double p50_s, p99_s;       /* job latency (completion - arrival)           */
+  uint64_t hbm_bytes;        /* device memory held by the classes' arenas    */
+} pangu_server_stats;
+int pangu_server_create(uint64_t hbm_budget_bytes, pangu_server **out);
+int pangu_server_destroy(pangu_server *s);
+/* PANGU_ENOMEM when the class's arena does not fit in the remaining budget. */
+int pangu_server_add_class(pangu_server *s, const pangu_params *params,
+                           const pangu_mesh *block, int32_t capacity_blocks,
+                           int32_t max_jobs, double dt_factor, int32_t *class_out);
+/* prim_host: the job's initial primitives, FP64 [block][var][k][j][i] over
+ * every cell of each block (ghosts are filled at admission). Copied. */
+int pangu_server_submit(pangu_server *s, int32_t cls, const pangu_mesh *mesh,
+                        double a, double h, double dt_init, int64_t cycles,
+                        double arrival_s, const double *prim_host, int32_t *ticket_out);
+/* Runs until every submitted job is done. Blocks the calling thread. */
+int pangu_server_run(pangu_server *s);
+/* A finished job: primitives (FP64, layout of submit), times {arrival,
+ * admission, completion} in seconds, and its counters. Any pointer may be
+ * NULL. */
+int pangu_server_result(pangu_server *s, int32_t ticket, double *prim_out,
+                        double *times_out, uint64_t counters_out[PANGU_NCOUNTERS]);
+int pangu_server_get_stats(const pangu_server *s, pangu_server_stats *out);
 
 #ifdef __cplusplus
 }

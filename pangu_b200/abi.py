@@ -12,6 +12,7 @@ PANGU_ETOOBIG = -5
 PANGU_EFULL = -6
 
 RIEMANN = {"laxf": 0, "hll": 1}
+PRECISION = {"fp64": 0, "mixed": 1}
 LIMITER = {"ppm4": 0, "mc": 1}
 RECOVERY = {"chainer": 0, "robuster": 1}
 METRIC = {"minkowski": 0, "bl": 1, "cks": 2, "mks": 3}
@@ -48,7 +49,7 @@ class Params(C.Structure):
         ("enable_B", C.c_int32),
         ("recovery", C.c_int32),
         ("enable_heating", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("precision", C.c_int32),
         ("sigma_max", C.c_double),
         ("lorentz_max", C.c_double),
         ("model", C.c_int32),
@@ -88,4 +89,13 @@ class Pack(C.Structure):
         ("prim", C.c_void_p), ("cons", C.c_void_p),
         ("flux1", C.c_void_p), ("flux2", C.c_void_p), ("flux3", C.c_void_p),
         ("alfven", C.c_void_p), ("efield", C.c_void_p), ("flag", C.c_void_p),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("jobs", C.c_int64), ("ticks", C.c_int64),
+        ("wall_s", C.c_double), ("zone_cycles", C.c_double),
+        ("zone_cycles_per_s", C.c_double), ("p50_s", C.c_double), ("p99_s", C.c_double),
+        ("hbm_bytes", C.c_uint64),
     ]

@@ -2,9 +2,11 @@
 
     python -m pangu_b200.build [--force] [--verbose]
 
-Produces ``pangu_b200/_lib/libpangu_b200.so`` from ``csrc/engine.cu`` (nvcc,
-``-gencode arch=compute_100a,code=sm_100a``) and ``csrc/host_tables.cc``
-(g++). Host code that evaluates the coordinate map is compiled with
+Produces ``pangu_b200/_lib/libpangu_b200.so`` from the CUDA sources of
+``csrc/`` (nvcc, ``-gencode arch=compute_100a,code=sm_100a``) and
+``csrc/host_tables.cc`` (g++). The exact FP64 build (engine.cu) uses
+``--fmad=false``; the mixed-precision one (engine_mixed.cu) allows
+contraction. Host code that evaluates the coordinate map is compiled with
 ``-ffp-contract=off`` so its rounding matches a plain C++ build.
 """
 from __future__ import annotations
@@ -24,6 +26,10 @@ INCLUDE = os.path.join(ROOT, "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "--fmad=false",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-Xcompiler", "-O2"]
+
+
+# Translation units of the mixed-precision form: FMA contraction allowed.
+MIXED_SOURCES = ("engine_mixed.cu",)
 
 
 def sources():
@@ -55,12 +61,15 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     obj_dir = os.path.join(LIBDIR, "obj")
     os.makedirs(obj_dir, exist_ok=True)
-    objs = []
+    objs, jobs = [], []
     for name in sorted(os.listdir(CSRC)):
         src = os.path.join(CSRC, name)
         if name.endswith(".cu"):
             obj = os.path.join(obj_dir, name + ".o")
-            cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-I", INCLUDE, "-I", CSRC, "-c", src, "-o", obj]
+            flags = NVCC_FLAGS
+            if name in MIXED_SOURCES:
+                flags = [f if f != "--fmad=false" else "--fmad=true" for f in flags]
+            cmd = [nvcc(), *ARCH, *flags, "-I", INCLUDE, "-I", CSRC, "-c", src, "-o", obj]
             if verbose:
                 cmd += ["-Xptxas", "-v"]
         elif name.endswith(".cc"):
@@ -71,8 +80,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
             continue
         if verbose:
             print(" ".join(cmd), flush=True)
-        subprocess.check_call(cmd)
+        jobs.append((subprocess.Popen(cmd), cmd))
         objs.append(obj)
+    for proc, cmd in jobs:  # translation units compile in parallel
+        if proc.wait() != 0:
+            raise subprocess.CalledProcessError(proc.returncode, cmd)
     tmp = LIB + ".tmp"
     cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
     subprocess.check_call(cmd)

@@ -6,1547 +6,42 @@
 // consecutive i so that loads and stores are coalesced in every sweep
 // direction (the reference's X2/X3 loops put a strided index innermost,
 // laxf.cc:185-189, 291-295).
-#include <cuda_runtime.h>
+#include "engine_impl.cuh"
 
-#include <algorithm>
-#include <cfloat>
-#include <cstdint>
-#include <cstring>
-#include <mutex>
-#include <new>
-#include <vector>
-
-#include "pangu_b200.h"
-#include "pangu_device.cuh"
+#define PGK_NS pgk64
+#define PGK_MIXED 0
+#include "kernels.cuh"
+#undef PGK_NS
 
 using namespace pgd;
-
-namespace pgh {
-struct Layout {
-  int N[3], st[3], nx[3], act[3], nb[3], NB, ng, NF;
-  double dx[3];
-  std::vector<double> origin;
-};
-Layout make_layout(const pangu_params &p, const pangu_mesh &m);
-void build_tables(const pangu_params &p, const Layout &L, std::vector<double> &t1,
-                  std::vector<double> &t2);
-void build_exchange(const pangu_mesh &m, const Layout &L, std::vector<int64_t> &dst,
-                    std::vector<int64_t> &src);
-}  // namespace pgh
-
-// ---------------------------------------------------------------------------
-// geometry passed to every kernel by value
-// ---------------------------------------------------------------------------
-struct Dims {
-  int N1, N2, N3, NF, NB;
-  int is, ie, js, je, ks, ke;
-  int o1, o2, o3, ndim;
-  long long ncell;  // N1 * N2 * N3
-  int pidx[NPRIM];  // pack index of each slot, -1 if absent
-  double dx[3];          // cell widths where bdx is null (handle-free dt estimate)
-  // Block table. The launch domain is NB active blocks; active block bb lives
-  // in pool slot slot[bb] (identity when null). Arrays below marked [slot]
-  // are indexed by pool slot.
-  const int *slot;          // [NB]
-  const int *slot_job;      // [slot] owning job id (job 0 when null)
-  const double *bdx;        // [slot][3] cell widths of the owning job's mesh
-  const signed char *bcf;   // [slot][6] PANGU_BC_OUTFLOW/REFLECTING per face, -1 none
-  const double *t1;      // [slot][10][N1 + 1]
-  const double *t2;      // [slot][12][N2 + 1]
-  const double *origin;  // [slot][3]
-  // Static MKS/BL metric tables (built once per engine by k_build_tables):
-  // component planes of [NB][comp][N2][N1] (centres), [NB][comp][N2][N1+1]
-  // (x1 faces) and [NB][comp][N2+1][N1] (x2 faces); x3 faces use the centres.
-  const double *ctab, *f1tab, *f2tab;
-};
-
-// A job: one mesh of equal meshblocks, placed in pool slots.
-struct PoolJob {
-  bool live = false;
-  pangu_mesh m{};
-  pangu_params p{};                 // the pool's params with the job's metric a, h
-  std::vector<int> slots;           // slot of the job's block b (lattice order)
-  std::vector<int64_t> xdst, xsrc;  // exchange map in slot cell offsets
-  bool any_bc = false;              // some face is outflow / reflecting
-};
-
-struct pangu_engine {
-  pangu_params p;
-  pangu_mesh m;  // block shape (nx, ng); for a single-mesh engine the whole mesh
-  Dims d;        // d.NB = active blocks; d.slot = d_active
-  int capacity = 0, max_jobs = 0;
-  std::vector<PoolJob> jobs;
-  std::vector<char> slot_used;
-  int njobs_active = 0;
-  bool any_bc = false;
-  std::vector<long long> xoff;  // per job id: offset of its entries in the exchange map
-  int *d_active = nullptr;      // [capacity] active block -> slot
-  int *d_slot_job = nullptr;    // [capacity]
-  int *d_jr = nullptr;          // [max_jobs][3] job id, first and end active block
-  double *d_bdx = nullptr;      // [capacity][3]
-  signed char *d_bcf = nullptr; // [capacity][6]
-  double *d_t1 = nullptr, *d_t2 = nullptr, *d_origin = nullptr;
-  double *d_ctab = nullptr, *d_f1tab = nullptr, *d_f2tab = nullptr;
-  long long *d_xdst = nullptr, *d_xsrc = nullptr;
-  long long nxch = 0, xch_cap = 0;
-  unsigned long long *d_cnt = nullptr;  // [max_jobs][PANGU_NCOUNTERS]
-  int *d_fail_count = nullptr;
-  long long *d_fail_list = nullptr;
-  double *d_fail_vals = nullptr;
-  long long fail_cap = 0;
-  unsigned long long *d_dtmin = nullptr;  // [capacity][3]
-  long long launches = 0;  // kernels launched through this handle
-};
-
-namespace {
-
-constexpr int kThreads = 256;
-constexpr int kT1Rows = 10;  // rows of the x1 table (host_tables.cc)
-
-__device__ __forceinline__ int slot_of(const Dims &d, int bb) {
-  return d.slot ? __ldg(d.slot + bb) : bb;
-}
-__device__ __forceinline__ int job_of(const Dims &d, int b) {
-  return d.slot_job ? __ldg(d.slot_job + b) : 0;
-}
-__device__ __forceinline__ double dx_of(const Dims &d, int b, int dir) {
-  return d.bdx ? __ldg(d.bdx + 3 * b + dir) : d.dx[dir];
-}
-
-__device__ __forceinline__ long long vidx(const Dims &d, int b, int v, int k, int j, int i) {
-  return (((long long)b * d.NF + v) * d.N3 + k) * (long long)d.N2 * d.N1 + (long long)j * d.N1 + i;
-}
-__device__ __forceinline__ long long cidx(const Dims &d, int b, int k, int j, int i) {
-  return ((long long)b * d.N3 + k) * (long long)d.N2 * d.N1 + (long long)j * d.N1 + i;
-}
-__device__ __forceinline__ long long aidx(const Dims &d, int b, int c, int k, int j, int i) {
-  return (((long long)b * 3 + c) * d.N3 + k) * (long long)d.N2 * d.N1 + (long long)j * d.N1 + i;
-}
-
-__device__ __forceinline__ void load_prim(const Dims &d, const double *P, int b, int k, int j,
-                                          int i, double out[NPRIM]) {
-#pragma unroll
-  for (int s = 0; s < NPRIM; ++s) out[s] = d.pidx[s] >= 0 ? P[vidx(d, b, d.pidx[s], k, j, i)] : 0.0;
-}
-
-// Cell-centre coordinate (origin + (idx + 1/2) dx, rounded step by step).
-__device__ __forceinline__ double xc(const Dims &d, int b, int dir, int idx) {
-  return ADD(d.origin[3 * b + dir], MUL((double)idx + 0.5, dx_of(d, b, dir)));
-}
-__device__ __forceinline__ double xf(const Dims &d, int b, int dir, int idx) {
-  return ADD(d.origin[3 * b + dir], MUL((double)idx, dx_of(d, b, dir)));
-}
-
-// Map point of the x1/x2 tables: q1/q2 select centre (0), +delta (1),
-// -delta (2) or face (3).
-__device__ __forceinline__ MapPt map_pt(const Dims &d, int b, int i, int q1, int j, int q2) {
-  const int W1 = d.N1 + 1, W2 = d.N2 + 1;
-  const double *T1 = d.t1 + (long long)b * kT1Rows * W1;
-  const double *T2 = d.t2 + (long long)b * 12 * W2;
-  MapPt m;
-  m.r = T1[(2 * q1) * W1 + i];
-  m.J1 = T1[(2 * q1 + 1) * W1 + i];
-  m.sth = T2[(3 * q2) * W2 + j];
-  m.cth = T2[(3 * q2 + 1) * W2 + j];
-  m.J2 = T2[(3 * q2 + 2) * W2 + j];
-  return m;
-}
-
-// Covariant code metric at a point given by table selectors (MKS/BL) or
-// coordinates (CKS).
-template <int MT>
-__device__ __forceinline__ void gcov_at(const Dims &d, const pangu_params &p, int b, int i, int q1,
-                                        int j, int q2, const double x[4], double g[4][4]) {
-  if (MT == MKS) {
-    ks_code_gcov(map_pt(d, b, i, q1, j, q2), p.a, g);
-  } else if (MT == BL) {
-    bl_code_gcov(map_pt(d, b, i, q1, j, q2), p.a, g);
-  } else if (MT == CKS) {
-    cks_code_gcov(x[1], x[2], x[3], p.a, g);
-  } else {
-    minkowski_gcov(g);
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Static metric tables. The MKS and BL metrics depend on (x1, x2) only and not
-// on time, so ComputeMetricAtLocation (christoffel.h:53-62) and
-// ComputeChristoffelConnection (christoffel.h:74-148) are evaluated once per
-// (j, i) point by the dense reference arithmetic (k_build_tables) and stored:
-// the structurally non-zero entries of gcov and gcon (upper triangle), gdet,
-// sqrt|gdet|, the lapse 1/sqrt(-gcon00), a validity flag (0 where the
-// inversion is singular) and, at cell centres, the structurally non-zero
-// Christoffel symbols (symmetric in their lower indices). Loads reproduce
-// the dense values bit for bit.
-// ---------------------------------------------------------------------------
-struct TabLayout {
-  int nsym, nmet, nconn, ncen;
-  int sym[4][4];      // slot of g_rc (r, c symmetric), -1 if structurally zero
-  int conn[4][4][4];  // slot of Gamma^a_bc (b, c symmetric), -1 if zero
-};
-
-__host__ __device__ constexpr TabLayout tab_layout(int mt) {
-  TabLayout L{};
-  const Pattern pt = metric_pattern(mt);
-  int n = 0;
-  for (int r = 0; r < 4; ++r)
-    for (int c = 0; c < 4; ++c) L.sym[r][c] = -1;
-  for (int r = 0; r < 4; ++r)
-    for (int c = r; c < 4; ++c)
-      if (pt.nz[r][c]) {
-        L.sym[r][c] = n;
-        L.sym[c][r] = n;
-        ++n;
-      }
-  L.nsym = n;
-  L.nmet = 2 * n + 4;
-  // derivative directions with non-zero metric derivatives
-  bool ddir[4] = {false, true, true, mt == CKS};
-  if (mt == MINKOWSKI) ddir[1] = ddir[2] = ddir[3] = false;
-  bool dg[4][4][4] = {};
-  for (int dd = 0; dd < 4; ++dd)
-    for (int r = 0; r < 4; ++r)
-      for (int c = 0; c < 4; ++c) dg[dd][r][c] = ddir[dd] && pt.nz[r][c];
-  int m = 0;
-  for (int a = 0; a < 4; ++a)
-    for (int j = 0; j < 4; ++j)
-      for (int k = 0; k < 4; ++k) L.conn[a][j][k] = -1;
-  for (int a = 0; a < 4; ++a)
-    for (int j = 0; j < 4; ++j)
-      for (int k = j; k < 4; ++k) {
-        bool nz = false;
-        for (int l = 0; l < 4; ++l)
-          nz = nz || (pt.nz[a][l] && (dg[j][l][k] || dg[k][l][j] || dg[l][j][k]));
-        if (nz) {
-          L.conn[a][j][k] = m;
-          L.conn[a][k][j] = m;
-          ++m;
-        }
-      }
-  L.nconn = m;
-  L.ncen = L.nmet + m;
-  return L;
-}
-
-template <int MT>
-__device__ __forceinline__ int load_geo(const double *__restrict__ tab, long long plane,
-                                        long long off, Geo &g) {
-  constexpr TabLayout L = tab_layout(MT);
-  double cov[L.nsym], con[L.nsym];
-#pragma unroll
-  for (int q = 0; q < L.nsym; ++q) {
-    cov[q] = __ldg(tab + off + q * plane);
-    con[q] = __ldg(tab + off + (L.nsym + q) * plane);
-  }
-#pragma unroll
-  for (int r = 0; r < 4; ++r)
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      g.gcov[r][c] = L.sym[r][c] >= 0 ? cov[L.sym[r][c]] : 0.0;
-      g.gcon[r][c] = L.sym[r][c] >= 0 ? con[L.sym[r][c]] : 0.0;
-    }
-  g.gdet = __ldg(tab + off + (2 * L.nsym) * plane);
-  g.sg = __ldg(tab + off + (2 * L.nsym + 1) * plane);
-  g.alpha = __ldg(tab + off + (2 * L.nsym + 2) * plane);
-  return __ldg(tab + off + (2 * L.nsym + 3) * plane) != 0.0;
-}
-
-__device__ __forceinline__ void minkowski_geo(Geo &g) {
-  minkowski_gcov(g.gcov);
-  minkowski_gcov(g.gcon);
-  g.gdet = -1.0;
-  g.sg = 1.0;
-  g.alpha = 1.0;
-}
-
-// Dense reference arithmetic at an analytic point (CKS; table building).
-template <int MT>
-__device__ __forceinline__ int analytic_geo(const Dims &d, const pangu_params &p, int b, int i,
-                                            int q1, int j, int q2, const double x[4], Geo &g) {
-  gcov_at<MT>(d, p, b, i, q1, j, q2, x, g.gcov);
-  const int ok = gj_invert(g.gcov, g.gcon);
-  g.gdet = determinant(g.gcov);
-  g.sg = sqrt(fabs(g.gdet));
-  g.alpha = 1.0 / sqrt(-g.gcon[0][0]);
-  return ok;
-}
-
-// ComputeMetricAtLocation (christoffel.h:53-62) at cell centre (b, k, j, i).
-// Returns 0 if the metric is singular.
-template <int MT>
-__device__ __forceinline__ int cell_metric(const Dims &d, const pangu_params &p, int b, int k,
-                                           int j, int i, Geo &g) {
-  if (MT == MKS || MT == BL) {
-    constexpr TabLayout L = tab_layout(MT);
-    const long long plane = (long long)d.N2 * d.N1;
-    return load_geo<MT>(d.ctab, plane, (long long)b * L.ncen * plane + (long long)j * d.N1 + i, g);
-  } else if (MT == CKS) {
-    const double x[4] = {0.0, xc(d, b, 0, i), xc(d, b, 1, j), xc(d, b, 2, k)};
-    return analytic_geo<MT>(d, p, b, i, 0, j, 0, x, g);
-  } else {
-    minkowski_geo(g);
-    return 1;
-  }
-}
-
-// Metric at the lower face of (b, k, j, i) along dir (1..3).
-template <int MT>
-__device__ __forceinline__ int face_metric(const Dims &d, const pangu_params &p, int dir, int b,
-                                           int k, int j, int i, Geo &g) {
-  if (MT == MKS || MT == BL) {
-    constexpr TabLayout L = tab_layout(MT);
-    if (dir == 1) {
-      const long long plane = (long long)d.N2 * (d.N1 + 1);
-      return load_geo<MT>(d.f1tab, plane,
-                          (long long)b * L.nmet * plane + (long long)j * (d.N1 + 1) + i, g);
-    } else if (dir == 2) {
-      const long long plane = (long long)(d.N2 + 1) * d.N1;
-      return load_geo<MT>(d.f2tab, plane, (long long)b * L.nmet * plane + (long long)j * d.N1 + i,
-                          g);
-    }
-    return cell_metric<MT>(d, p, b, k, j, i, g);  // independent of x3
-  } else if (MT == CKS) {
-    const double x[4] = {0.0, dir == 1 ? xf(d, b, 0, i) : xc(d, b, 0, i),
-                         dir == 2 ? xf(d, b, 1, j) : xc(d, b, 1, j),
-                         dir == 3 ? xf(d, b, 2, k) : xc(d, b, 2, k)};
-    return analytic_geo<MT>(d, p, b, i, 0, j, 0, x, g);
-  } else {
-    minkowski_geo(g);
-    return 1;
-  }
-}
-
-// Warp-aggregated increment of a hit counter of `job` (counters are
-// [job][PANGU_NCOUNTERS]); a warp may straddle blocks of several jobs.
-__device__ __forceinline__ void count(unsigned long long *cnt, int job, int which, bool pred) {
-  const unsigned mask = __activemask();
-  const unsigned hits = __ballot_sync(mask, pred);
-  if (!hits) return;
-  const unsigned peers = __match_any_sync(mask, job);
-  const unsigned mine = hits & peers;
-  if (mine && (threadIdx.x & 31) == (__ffs(peers) - 1))
-    atomicAdd(&cnt[job * PANGU_NCOUNTERS + which], (unsigned long long)__popc(mine));
-}
-
-// Decomposes a flat index over the box [k0,k1] x [j0,j1] x [i0,i1] of every
-// block. Returns false past the end.
-__device__ __forceinline__ bool box_index(long long t, int NB, int k0, int k1, int j0, int j1,
-                                          int i0, int i1, int &b, int &k, int &j, int &i) {
-  const long long ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
-  if (ni <= 0 || nj <= 0 || nk <= 0) return false;
-  const long long per = ni * nj * nk;
-  if (t >= per * NB) return false;
-  b = (int)(t / per);
-  long long r = t - (long long)b * per;
-  k = k0 + (int)(r / (ni * nj));
-  r -= (long long)(k - k0) * ni * nj;
-  j = j0 + (int)(r / ni);
-  i = i0 + (int)(r - (long long)(j - j0) * ni);
-  return true;
-}
-
-inline unsigned grid_for(long long n) {
-  const long long g = (n + kThreads - 1) / kThreads;
-  return (unsigned)std::max<long long>(1, std::min<long long>(g, 0x7fffffffLL));
-}
-
-// ---------------------------------------------------------------------------
-// FixPrimitive (primitive_fixer.cc:15-169), entire domain.
-// ---------------------------------------------------------------------------
-template <int MT>
-__global__ void __launch_bounds__(kThreads) k_fix_primitive(Dims d, pangu_params p, double *P,
-                                                            unsigned long long *cnt) {
-  int b, k, j, i;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (!box_index(t, d.NB, 0, d.N3 - 1, 0, d.N2 - 1, 0, d.N1 - 1, b, k, j, i)) return;
-  b = slot_of(d, b);
-  const double gam = p.adiabatic_index;
-  constexpr double small = 1.0e-20;
-  const double sigma_max_safe = kmax(p.sigma_max, small);
-  const long long q = vidx(d, b, 0, k, j, i);
-  const long long vs = d.ncell;
-  const double rho_before = kmax(P[q], small);
-  double r = 1.0;
-  double rho_floor, eng_floor;
-  if (MT == MKS) {
-    // r = exp(Xc1) and the radial floor profiles, from the host tables
-    const double *T1 = d.t1 + (long long)b * kT1Rows * (d.N1 + 1);
-    r = T1[i];
-    rho_floor = T1[8 * (d.N1 + 1) + i];
-    eng_floor = T1[9 * (d.N1 + 1) + i];
-  } else if (MT == CKS) {
-    const double x = xc(d, b, 0, i), y = xc(d, b, 1, j), z = xc(d, b, 2, k);
-    const double a2 = p.a * p.a;
-    const double rad2 = x * x + y * y + z * z;
-    const double sa = (rad2 - a2) * (rad2 - a2) + 4.0 * a2 * z * z;
-    r = sqrt(0.5 * (rad2 - a2 + sqrt(sa)));
-    rho_floor = p.density_floor * pgm::pow(fmax(r, 1.0), p.density_floor_pow);
-    eng_floor = p.energy_floor * pgm::pow(fmax(r, 1.0), p.energy_floor_pow);
-  } else {
-    rho_floor = p.density_floor;  // pgm::pow(max(1, 1), q) == 1
-    eng_floor = p.energy_floor;
-  }
-  Geo g;
-  cell_metric<MT>(d, p, b, k, j, i, g);
-  double pc[NPRIM];
-  load_prim(d, P, b, k, j, i, pc);
-  const double rho = pc[RHO], ug = pc[ENY];
-  State st;
-  calc_state<MT>(pc, g, st);
-  if (rho_floor < ug / sigma_max_safe) rho_floor = ug / sigma_max_safe;
-  const double sigma = st.bsq / rho;
-  if (sigma > p.sigma_max) rho_floor = st.bsq / sigma_max_safe;
-  double pr = pc[RHO], pu = pc[ENY];
-  const bool hit_r = pr < rho_floor;
-  if (hit_r) pr = rho_floor;
-  const bool hit_u = pu < eng_floor;
-  if (hit_u) pu = eng_floor;
-  double u1 = pc[UX1], u2 = pc[UX2], u3 = pc[UX3];
-  const double umax2 = p.lorentz_max * p.lorentz_max - 1.0;
-  // primitive_fixer.cc:131-134; structurally zero cross terms skipped
-  constexpr Pattern PT = metric_pattern(MT);
-  double uvsq = g.gcov[1][1] * u1 * u1 + g.gcov[2][2] * u2 * u2 + g.gcov[3][3] * u3 * u3;
-  if (PT.nz[1][2] || PT.nz[1][3] || PT.nz[2][3]) {
-    double cross = 0.0;
-    if (PT.nz[1][2]) cross = cross + g.gcov[1][2] * u1 * u2;
-    if (PT.nz[1][3]) cross = cross + g.gcov[1][3] * u1 * u3;
-    if (PT.nz[2][3]) cross = cross + g.gcov[2][3] * u2 * u3;
-    uvsq = uvsq + 2.0 * cross;
-  }
-  const bool cap = umax2 > 0.0 && uvsq > umax2;
-  if (cap) {
-    const double f = sqrt(umax2 / kmax(uvsq, small));
-    u1 *= f;
-    u2 *= f;
-    u3 *= f;
-  }
-  const double rho_after = kmax(pr, small);
-  double kel = pc[KEL];
-  if (p.enable_heating && rho_after != rho_before) kel *= pgm::pow(rho_after / rho_before, -gam);
-  double ent = (gam - 1.0) * pu * pgm::pow(pr, -gam);
-  if (p.enable_heating) kel = clamp_by_ratio(p.ratio_min, p.ratio_max, ent, kel);
-  if (MT == CKS && r < p.r_excise) {
-    const double e_excise = p.pexcise / (gam - 1.0);
-    pr = p.dexcise;
-    pu = e_excise;
-    u1 = u2 = u3 = 0.0;
-    ent = (gam - 1.0) * e_excise * pgm::pow(p.dexcise, -gam);
-    if (p.enable_heating) kel = e_excise;
-  }
-  P[q] = pr;
-  P[q + vs] = pu;
-  P[q + 2 * vs] = u1;
-  P[q + 3 * vs] = u2;
-  P[q + 4 * vs] = u3;
-  P[q + d.pidx[ENT] * vs] = ent;
-  if (p.enable_heating) P[q + d.pidx[KEL] * vs] = kel;
-  count(cnt, job_of(d, b), PANGU_CNT_RHO_FLOOR, hit_r);
-  count(cnt, job_of(d, b), PANGU_CNT_ENG_FLOOR, hit_u);
-  count(cnt, job_of(d, b), PANGU_CNT_LORENTZ_CAP, cap);
-}
-
-// ---------------------------------------------------------------------------
-// CalculateConservative (conservative.cc:15-110), interior.
-// ---------------------------------------------------------------------------
-template <int MT>
-__global__ void __launch_bounds__(kThreads) k_calc_cons(Dims d, pangu_params p, const double *P,
-                                                        double *U) {
-  int b, k, j, i;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
-  b = slot_of(d, b);
-  Geo g;
-  cell_metric<MT>(d, p, b, k, j, i, g);
-  double pc[NPRIM];
-  load_prim(d, P, b, k, j, i, pc);
-  State s;
-  calc_state<MT>(pc, g, s);
-  double f[NPRIM];
-  flux_from_state(p.adiabatic_index, pc, s, g.sg, 0, f);
-#pragma unroll
-  for (int v = 0; v < NPRIM; ++v)
-    if (d.pidx[v] >= 0) U[vidx(d, b, d.pidx[v], k, j, i)] = f[v];
-}
-
-// ---------------------------------------------------------------------------
-// CalculateLAXF / CalculateHLL (laxf.cc:78-393, hll.cc:78-399).
-//
-// Each cell's reconstruction is computed once and shared by its two faces
-// (the reference calls MC/PPM4 twice per variable and face,
-// laxf.cc:86-105): x1 faces by warp shuffles, x2/x3 faces by marching along
-// the column. The Riemann flux is then assembled component by component
-// from the two states, in the reference's operation order.
-// ---------------------------------------------------------------------------
-
-// Reconstruction of one variable in cell q (stride s along the direction):
-// ql_ip1 = value at the upper face, qr_i = value at the lower face
-// (interpolater_mc.h:38-48, interpolater_ppm4.h:29-67).
-__device__ __forceinline__ void recon_cell(bool use_mc, const double *q, long long s,
-                                           double &ql_ip1, double &qr_i) {
-  if (use_mc) {
-    mc(q[-s], q[0], q[s], ql_ip1, qr_i);
-  } else {
-    ppm4(q[-2 * s], q[-s], q[0], q[s], q[2 * s], ql_ip1, qr_i);
-  }
-}
-
-// One flux component from a state (contravariant_flux.h:12-39).
-template <int c>
-__device__ __forceinline__ double flux_component(double gam, const double P[NPRIM],
-                                                 const State &s, double sg, int dir) {
-  const double f_rho = P[RHO] * s.ucon[dir];
-  if (c == RHO) return f_rho * sg;
-  if (c == ENT) return (P[ENT] * f_rho) * sg;
-  if (c == KEL) return (P[KEL] * f_rho) * sg;
-  if (c >= BX1 && c <= BX3) {
-    const int m = c - BX1 + 1;
-    return SUB(MUL(s.bcon[m], s.ucon[dir]), MUL(s.bcon[dir], s.ucon[m])) * sg;
-  }
-  const double hh = P[RHO] + gam * P[ENY];
-  const double e_tot = hh + s.bsq;
-  const double p_tot = (gam - 1.) * P[ENY] + 0.5 * s.bsq;
-  const int m = (c == ENY) ? 0 : c - UX1 + 1;
-  const double t = e_tot * s.ucon[dir] * s.ucov[m] + p_tot * (dir == m) - s.bcon[dir] * s.bcov[m];
-  if (c == ENY) return (t + f_rho) * sg;
-  return t * sg;
-}
-
-// Riemann flux and fast speed at the lower face of (b, k, j, i) along DIR
-// from the left and right states.
-template <int MT, int DIR>
-__device__ __forceinline__ void face_flux(const Dims &d, const pangu_params &p, int b, int k, int j,
-                                          int i, const double PL[NPRIM], const double PR[NPRIM],
-                                          double *F, double *alfven) {
-  Geo g;
-  const long long fo = vidx(d, b, 0, k, j, i);
-  if (!face_metric<MT>(d, p, DIR, b, k, j, i, g)) {
-    // Singular code metric (theta = 0 exactly on a polar face): zero flux,
-    // zero speed (the reference reads an unwritten inverse here).
-    alfven[aidx(d, b, DIR - 1, k, j, i)] = 0.0;
-#pragma unroll
-    for (int s = 0; s < NPRIM; ++s)
-      if (d.pidx[s] >= 0) F[fo + d.pidx[s] * d.ncell] = 0.0;
-    return;
-  }
-  const double gam = p.adiabatic_index;
-  const double sg = g.sg;
-  State sL, sR;
-  calc_state<MT>(PL, g, sL);
-  calc_state<MT>(PR, g, sR);
-  double vmaxL, vminL, vmaxR, vminR;
-  fast_speed_from_state(gam, PL, g, sL, DIR, vmaxL, vminL);
-  fast_speed_from_state(gam, PR, g, sR, DIR, vmaxR, vminR);
-  const double cmax = fabs(kmax(kmax(0., vmaxL), vmaxR));
-  const double cmin = fabs(kmax(kmax(0., -vminL), -vminR));
-  const double cms = kmax(cmax, cmin);
-  alfven[aidx(d, b, DIR - 1, k, j, i)] = cms;
-  const bool hll = p.riemann_solver == PANGU_RIEMANN_HLL;
-#define PGD_FACE_COMPONENT(C)                                                         \
-  if (d.pidx[C] >= 0) {                                                               \
-    const double fl = flux_component<C>(gam, PL, sL, sg, DIR);                        \
-    const double fr = flux_component<C>(gam, PR, sR, sg, DIR);                        \
-    const double ul = flux_component<C>(gam, PL, sL, sg, 0);                          \
-    const double ur = flux_component<C>(gam, PR, sR, sg, 0);                          \
-    F[fo + d.pidx[C] * d.ncell] =                                                     \
-        hll ? (cmax * fl + cmin * fr - cmax * cmin * (ur - ul)) / (cmax + cmin + 1e-20) \
-            : 0.5 * (fl + fr - cms * (ur - ul));                                      \
-  }
-  PGD_FACE_COMPONENT(RHO)
-  PGD_FACE_COMPONENT(ENY)
-  PGD_FACE_COMPONENT(UX1)
-  PGD_FACE_COMPONENT(UX2)
-  PGD_FACE_COMPONENT(UX3)
-  PGD_FACE_COMPONENT(BX1)
-  PGD_FACE_COMPONENT(BX2)
-  PGD_FACE_COMPONENT(BX3)
-  PGD_FACE_COMPONENT(ENT)
-  PGD_FACE_COMPONENT(KEL)
-#undef PGD_FACE_COMPONENT
-}
-
-// x1 faces: a warp covers 31 consecutive faces of one row. Lane l
-// reconstructs cell c = f0 - 1 + l; face c takes its left state from lane
-// l - 1 (upper-face value of cell c - 1) and its right state from lane l.
-constexpr int kFacesPerWarp = 31;
-constexpr int kFluxThreads = 128;  // flux kernels use ~160 registers: 3 CTAs of 4 warps per SM
-
-template <int MT>
-__global__ void __launch_bounds__(kFluxThreads, 4) k_flux_x1(Dims d, pangu_params p, int k0, int k1,
-                                                      int j0, int j1, int i0, int i1,
-                                                      const double *P, double *F,
-                                                      double *alfven) {
-  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  const int nf = i1 - i0 + 1;
-  const int nseg = (nf + kFacesPerWarp - 1) / kFacesPerWarp;
-  const long long nrow = (long long)(k1 - k0 + 1) * (j1 - j0 + 1);
-  if (warp >= nrow * d.NB * nseg) return;  // whole warps exit together
-  const int seg = (int)(warp % nseg);
-  const long long row = warp / nseg;
-  const int bb = (int)(row / nrow);
-  const long long rr = row - (long long)bb * nrow;
-  const int b = slot_of(d, bb);
-  const int k = k0 + (int)(rr / (j1 - j0 + 1));
-  const int j = j0 + (int)(rr % (j1 - j0 + 1));
-  const int c = i0 - 1 + seg * kFacesPerWarp + lane;
-  const bool active = c <= i1;  // cell c is needed by face c (and c + 1)
-  const bool use_mc = p.limiter == PANGU_LIMITER_MC;
-  double PL[NPRIM], PR[NPRIM];
-#pragma unroll
-  for (int s = 0; s < NPRIM; ++s) {
-    double up = 0.0, lo = 0.0;
-    if (d.pidx[s] >= 0 && active)
-      recon_cell(use_mc, P + vidx(d, b, d.pidx[s], k, j, c), 1, up, lo);
-    PL[s] = __shfl_up_sync(0xffffffffu, up, 1);
-    PR[s] = lo;
-  }
-  if (lane == 0 || !active) return;
-  face_flux<MT, 1>(d, p, b, k, j, c, PL, PR, F, alfven);
-}
-
-// x2 / x3 faces: a thread marches over kMarch consecutive faces of one
-// column, carrying the upper-face value of the previous cell.
-constexpr int kMarch = 4;
-
-template <int MT, int DIR>
-__device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_params &p, int k0,
-                                                int k1, int j0, int j1, int i0, int i1,
-                                                const double *P, double *F, double *alfven) {
-  // the marching index is j (DIR 2) or k (DIR 3); the other two form the column
-  const int m0 = DIR == 2 ? j0 : k0, m1 = DIR == 2 ? j1 : k1;
-  const int a0 = DIR == 2 ? k0 : j0, a1 = DIR == 2 ? k1 : j1;  // outer transverse index
-  const int ni = i1 - i0 + 1, na = a1 - a0 + 1;
-  const int nruns = (m1 - m0 + 1 + kMarch - 1) / kMarch;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)d.NB * na * nruns * ni) return;
-  const int i = i0 + (int)(t % ni);
-  long long r = t / ni;
-  const int run = (int)(r % nruns);
-  r /= nruns;
-  const int a = a0 + (int)(r % na);
-  const int b = slot_of(d, (int)(r / na));
-  const long long stride = DIR == 2 ? (long long)d.N1 : (long long)d.N1 * d.N2;
-  const bool use_mc = p.limiter == PANGU_LIMITER_MC;
-  const int f0 = m0 + run * kMarch;
-  const int f1 = min(f0 + kMarch - 1, m1);
-  double carry[NPRIM];
-  {
-    const int c = f0 - 1;
-    const int kk = DIR == 2 ? a : c, jj = DIR == 2 ? c : a;
-#pragma unroll
-    for (int s = 0; s < NPRIM; ++s) {
-      double up = 0.0, lo;
-      if (d.pidx[s] >= 0) recon_cell(use_mc, P + vidx(d, b, d.pidx[s], kk, jj, i), stride, up, lo);
-      carry[s] = up;
-    }
-  }
-  for (int f = f0; f <= f1; ++f) {
-    const int kk = DIR == 2 ? a : f, jj = DIR == 2 ? f : a;
-    double PR[NPRIM], up[NPRIM];
-#pragma unroll
-    for (int s = 0; s < NPRIM; ++s) {
-      up[s] = 0.0;
-      PR[s] = 0.0;
-      if (d.pidx[s] >= 0)
-        recon_cell(use_mc, P + vidx(d, b, d.pidx[s], kk, jj, i), stride, up[s], PR[s]);
-    }
-    face_flux<MT, DIR>(d, p, b, kk, jj, i, carry, PR, F, alfven);
-#pragma unroll
-    for (int s = 0; s < NPRIM; ++s) carry[s] = up[s];
-  }
-}
-
-template <int MT>
-__global__ void __launch_bounds__(kFluxThreads, 4) k_flux_march2(Dims d, pangu_params p, int k0, int k1,
-                                                          int j0, int j1, int i0, int i1,
-                                                          const double *P, double *F,
-                                                          double *alfven) {
-  flux_march_body<MT, 2>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
-}
-template <int MT>
-__global__ void __launch_bounds__(kFluxThreads, 4) k_flux_march3(Dims d, pangu_params p, int k0, int k1,
-                                                          int j0, int j1, int i0, int i1,
-                                                          const double *P, double *F,
-                                                          double *alfven) {
-  flux_march_body<MT, 3>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
-}
-
-// ---------------------------------------------------------------------------
-// ConstraintedTransport (constrained_transport.cc:13-130).
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_ct_emf(Dims d, const double *F1, const double *F2,
-                                                     const double *F3, double *E) {
-  int b, k, j, i;
-  const int o1 = d.N1 > 1, o2 = d.N2 > 1, o3 = d.N3 > 1;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (!box_index(t, d.NB, d.ks, d.ke + o3, d.js, d.je + o2, d.is, d.ie + o1, b, k, j, i)) return;
-  b = slot_of(d, b);
-  const long long sj = d.N1, sk = (long long)d.N1 * d.N2;
-  double e1 = 0.0, e2 = 0.0, e3 = 0.0;
-  if (o2 && o3) {
-    const long long a = vidx(d, b, BX3, k, j, i), c = vidx(d, b, BX2, k, j, i);
-    e1 = 0.25 * ((F2[a] + F2[a - sk]) - (F3[c] + F3[c - sj]));
-  }
-  if (o3 && o1) {
-    const long long a = vidx(d, b, BX1, k, j, i), c = vidx(d, b, BX3, k, j, i);
-    e2 = 0.25 * ((F3[a] + F3[a - 1]) - (F1[c] + F1[c - sk]));
-  }
-  if (o1 && o2) {
-    const long long a = vidx(d, b, BX2, k, j, i), c = vidx(d, b, BX1, k, j, i);
-    e3 = 0.25 * ((F1[a] + F1[a - sj]) - (F2[c] + F2[c - 1]));
-  }
-  E[aidx(d, b, 0, k, j, i)] = e1;
-  E[aidx(d, b, 1, k, j, i)] = e2;
-  E[aidx(d, b, 2, k, j, i)] = e3;
-}
-
-// Face-B overwrite of direction dir (constrained_transport.cc:78-127).
-__global__ void __launch_bounds__(kThreads) k_ct_faces(Dims d, int dir, double *F,
-                                                       const double *E) {
-  int b, k, j, i;
-  const int o1 = d.N1 > 1, o2 = d.N2 > 1, o3 = d.N3 > 1;
-  const int E1 = o2 && o3, E2 = o3 && o1, E3 = o1 && o2;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int ei = dir == 1 ? o1 : 0, ej = dir == 2 ? o2 : 0, ek = dir == 3 ? o3 : 0;
-  if (!box_index(t, d.NB, d.ks, d.ke + ek, d.js, d.je + ej, d.is, d.ie + ei, b, k, j, i)) return;
-  b = slot_of(d, b);
-  const long long sj = d.N1, sk = (long long)d.N1 * d.N2;
-  const long long e0 = aidx(d, b, 0, k, j, i), e1 = aidx(d, b, 1, k, j, i),
-                  e2 = aidx(d, b, 2, k, j, i);
-  if (dir == 1) {
-    if (o1) F[vidx(d, b, BX1, k, j, i)] = 0;
-    if (E2) F[vidx(d, b, BX3, k, j, i)] = -0.5 * (E[e1] + E[e1 + sk]);
-    if (E3) F[vidx(d, b, BX2, k, j, i)] = 0.5 * (E[e2] + E[e2 + sj]);
-  } else if (dir == 2) {
-    if (E1) F[vidx(d, b, BX3, k, j, i)] = 0.5 * (E[e0] + E[e0 + sk]);
-    if (o2) F[vidx(d, b, BX2, k, j, i)] = 0.;
-    if (E3) F[vidx(d, b, BX1, k, j, i)] = -0.5 * (E[e2] + E[e2 + 1]);
-  } else {
-    if (E1) F[vidx(d, b, BX2, k, j, i)] = -0.5 * (E[e0] + E[e0 + sj]);
-    if (E2) F[vidx(d, b, BX1, k, j, i)] = 0.5 * (E[e1] + E[e1 + 1]);
-    if (o3) F[vidx(d, b, BX3, k, j, i)] = 0;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// FluxDivergence + UpdateIndependentData, interior (ideal_grmhd.cc:73-76).
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_flux_div_update(Dims d, const double *F1,
-                                                              const double *F2, const double *F3,
-                                                              const double *Uinit, double *Uout,
-                                                              double beta, const double *dt) {
-  int b, k, j, i;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (!box_index(t, d.NB * d.NF, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
-  // b here runs over (active block, variable) pairs
-  const int v = b % d.NF;
-  b = slot_of(d, b / d.NF);
-  const long long q = vidx(d, b, v, k, j, i);
-  const double dx0 = dx_of(d, b, 0), dx1 = dx_of(d, b, 1), dx2 = dx_of(d, b, 2);
-  const double A1 = MUL(dx1, dx2), A2 = MUL(dx0, dx2), A3 = MUL(dx0, dx1);
-  const double V = MUL(MUL(dx0, dx1), dx2);
-  double du = SUB(MUL(A1, F1[q + 1]), MUL(A1, F1[q]));
-  if (d.ndim >= 2) du = ADD(du, SUB(MUL(A2, F2[q + d.N1]), MUL(A2, F2[q])));
-  if (d.ndim == 3) {
-    const long long sk = (long long)d.N1 * d.N2;
-    du = ADD(du, SUB(MUL(A3, F3[q + sk]), MUL(A3, F3[q])));
-  }
-  const double dudt = DIV(-du, V);
-  const double bdt = MUL(beta, dt[job_of(d, b)]);
-  Uout[q] = ADD(Uinit[q], MUL(bdt, dudt));
-}
-
-// ---------------------------------------------------------------------------
-// Ghost exchange: ghost <- neighbour interior, prim and flag.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_exchange(Dims d, long long n, const long long *dst,
-                                                       const long long *src, double *P,
-                                                       double *flag) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  const long long dc = dst[t], sc = src[t];
-  const long long db = dc / d.ncell, sb = sc / d.ncell;
-  const long long dp = db * d.NF * d.ncell + (dc - db * d.ncell);
-  const long long sp = sb * d.NF * d.ncell + (sc - sb * d.ncell);
-  for (int v = 0; v < d.NF; ++v) P[dp + v * d.ncell] = P[sp + v * d.ncell];
-  if (flag) flag[dc] = flag[sc];
-}
-
-// ---------------------------------------------------------------------------
-// AddGeometricSource (source_term.cc:15-121): Christoffel symbols by central
-// differences of the code metric (christoffel.h:74-148), rounded step by
-// step like the metric itself.
-// ---------------------------------------------------------------------------
-template <int MT>
-__device__ __forceinline__ void christoffel(const Dims &d, const pangu_params &p, int b, int k,
-                                            int j, int i, const Geo &g, double conn[4][4][4]) {
-  constexpr double twod = 2.0 * 1.0e-5;
-  double dg[4][4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) dg[a][r][c] = 0.0;
-  double x[4] = {0.0, 0.0, 0.0, 0.0};
-  if (MT == CKS) {
-    x[1] = xc(d, b, 0, i);
-    x[2] = xc(d, b, 1, j);
-    x[3] = xc(d, b, 2, k);
-  }
-#pragma unroll
-  for (int dir = 1; dir < 4; ++dir) {
-    if ((MT == MKS || MT == BL) && dir == 3) continue;  // metric independent of x3: exactly 0
-    double gp[4][4], gm[4][4];
-    double xp[4] = {x[0], x[1], x[2], x[3]}, xm[4] = {x[0], x[1], x[2], x[3]};
-    xp[dir] = ADD(xp[dir], 1.0e-5);
-    xm[dir] = SUB(xm[dir], 1.0e-5);
-    gcov_at<MT>(d, p, b, i, dir == 1 ? 1 : 0, j, dir == 2 ? 1 : 0, xp, gp);
-    gcov_at<MT>(d, p, b, i, dir == 1 ? 2 : 0, j, dir == 2 ? 2 : 0, xm, gm);
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) dg[dir][r][c] = DIV(SUB(gp[r][c], gm[r][c]), twod);
-  }
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int jj = 0; jj < 4; ++jj)
-#pragma unroll
-      for (int kk = 0; kk < 4; ++kk) {
-        double v = 0.0;
-#pragma unroll
-        for (int l = 0; l < 4; ++l) {
-          const double cc = MUL(0.5, SUB(ADD(dg[jj][l][kk], dg[kk][l][jj]), dg[l][jj][kk]));
-          v = ADD(v, MUL(g.gcon[a][l], cc));
-        }
-        conn[a][jj][kk] = v;
-      }
-}
-
-template <int MT>
-__global__ void __launch_bounds__(kThreads) k_source(Dims d, pangu_params p, const double *P,
-                                                     double *U, double beta, const double *dt) {
-  int b, k, j, i;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
-  b = slot_of(d, b);
-  if (MT == MINKOWSKI) return;  // connection identically zero (christoffel.h:90)
-  Geo g;
-  cell_metric<MT>(d, p, b, k, j, i, g);
-  const double sg = g.sg;
-  double pc[NPRIM];
-  load_prim(d, P, b, k, j, i, pc);
-  State s;
-  calc_state<MT>(pc, g, s);
-  double T[4][4];
-#pragma unroll
-  for (int r = 0; r < 4; ++r) emt_from_state(p.adiabatic_index, pc, s, r, T[r]);
-  const double bdt = beta * dt[job_of(d, b)];
-  if (MT == MKS || MT == BL) {
-    // Christoffel symbols from the centre table; structural zeros skipped
-    constexpr TabLayout L = tab_layout(MT);
-    const long long plane = (long long)d.N2 * d.N1;
-    const double *cn = d.ctab + (long long)b * L.ncen * plane + (long long)j * d.N1 + i +
-                       (long long)L.nmet * plane;
-#pragma unroll
-    for (int dir = 0; dir < 4; ++dir) {
-      double con = 0.0;
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-          if (L.conn[c][dir][r] >= 0) con += T[r][c] * __ldg(cn + L.conn[c][dir][r] * plane);
-      const int v = dir == 0 ? d.pidx[ENY] : d.pidx[UX1] + dir - 1;
-      const long long q = vidx(d, b, v, k, j, i);
-      U[q] += con * sg * bdt;
-    }
-  } else {
-    double conn[4][4][4];
-    christoffel<MT>(d, p, b, k, j, i, g, conn);
-#pragma unroll
-    for (int dir = 0; dir < 4; ++dir) {
-      double con = 0.0;
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) con += T[r][c] * conn[c][dir][r];
-      const int v = dir == 0 ? d.pidx[ENY] : d.pidx[UX1] + dir - 1;
-      const long long q = vidx(d, b, v, k, j, i);
-      U[q] += con * sg * bdt;
-    }
-  }
-}
-
-// Builds the static metric tables of an MKS or BL engine with the dense
-// reference arithmetic (one thread per table point).
-template <int MT>
-__global__ void __launch_bounds__(kThreads) k_build_tables(Dims d, pangu_params p, double *ctab,
-                                                           double *f1tab, double *f2tab) {
-  constexpr TabLayout L = tab_layout(MT);
-  const long long pc = (long long)d.N2 * d.N1, p1 = (long long)d.N2 * (d.N1 + 1),
-                  p2 = (long long)(d.N2 + 1) * d.N1;
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long per = pc + p1 + p2;
-  if (t >= per * d.NB) return;
-  const int bb = (int)(t / per);
-  t -= (long long)bb * per;
-  const int b = slot_of(d, bb);
-  int which, W;
-  long long plane;
-  double *tab;
-  int nc;
-  if (t < pc) {
-    which = 0, W = d.N1, plane = pc, tab = ctab, nc = L.ncen;
-  } else if (t < pc + p1) {
-    t -= pc;
-    which = 1, W = d.N1 + 1, plane = p1, tab = f1tab, nc = L.nmet;
-  } else {
-    t -= pc + p1;
-    which = 2, W = d.N1, plane = p2, tab = f2tab, nc = L.nmet;
-  }
-  const int j = (int)(t / W), i = (int)(t % W);
-  const double x[4] = {0.0, 0.0, 0.0, 0.0};
-  Geo g;
-  const int ok = analytic_geo<MT>(d, p, b, i, which == 1 ? 3 : 0, j, which == 2 ? 3 : 0, x, g);
-  double *o = tab + (long long)b * nc * plane + t;
-#pragma unroll
-  for (int r = 0; r < 4; ++r)
-#pragma unroll
-    for (int c = r; c < 4; ++c)
-      if (L.sym[r][c] >= 0) {
-        o[L.sym[r][c] * plane] = g.gcov[r][c];
-        o[(L.nsym + L.sym[r][c]) * plane] = g.gcon[r][c];
-      }
-  o[(2 * L.nsym) * plane] = g.gdet;
-  o[(2 * L.nsym + 1) * plane] = g.sg;
-  o[(2 * L.nsym + 2) * plane] = g.alpha;
-  o[(2 * L.nsym + 3) * plane] = ok ? 1.0 : 0.0;
-  if (which == 0) {
-    double conn[4][4][4];
-    christoffel<MT>(d, p, b, 0, j, i, g, conn);
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int jj = 0; jj < 4; ++jj)
-#pragma unroll
-        for (int kk = jj; kk < 4; ++kk)
-          if (L.conn[a][jj][kk] >= 0) o[(L.nmet + L.conn[a][jj][kk]) * plane] = conn[a][jj][kk];
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Recovery (invertor.cc:18-210).
-// ---------------------------------------------------------------------------
-// Warp-aggregated append of `value` to list[*count] for the lanes with pred.
-__device__ __forceinline__ void append(int *count, long long *list, bool pred, long long value) {
-  const unsigned mask = __activemask();
-  const unsigned hits = __ballot_sync(mask, pred);
-  if (!hits) return;
-  const int lane = threadIdx.x & 31;
-  const int leader = __ffs(mask) - 1;
-  int base = 0;
-  if (lane == leader) base = atomicAdd(count, __popc(hits));
-  base = __shfl_sync(mask, base, leader);
-  if (pred) list[base + __popc(hits & ((1u << lane) - 1u))] = value;
-}
-
-// The HARM-normalised conserved state and the stale primitive guess of one
-// cell (invertor.cc:100-174); writes the magnetic primitives
-// (invertor.cc:137-147).
-template <int MT>
-__device__ __forceinline__ void c2p_inputs(const Dims &d, const pangu_params &p, double *P,
-                                           const double *U, int b, int k, int j, int i,
-                                           const Geo &g, double UH[9], double PH[9],
-                                           bool write_b) {
-  const long long q = vidx(d, b, 0, k, j, i);
-  const long long vs = d.ncell;
-  double C[9];
-#pragma unroll
-  for (int s = 0; s < 9; ++s) {
-    C[s] = d.pidx[s] >= 0 ? U[q + d.pidx[s] * vs] : 0.0;
-    PH[s] = d.pidx[s] >= 0 ? P[q + d.pidx[s] * vs] : 0.0;
-  }
-  const double isg = 1.0 / g.sg;
-  const double aisg = g.alpha * isg;
-  if (p.enable_B && write_b) {
-    P[q + d.pidx[BX1] * vs] = C[BX1] * isg;
-    P[q + d.pidx[BX2] * vs] = C[BX2] * isg;
-    P[q + d.pidx[BX3] * vs] = C[BX3] * isg;
-  }
-  UH[RHO] = aisg * C[RHO];
-  UH[ENY] = aisg * (C[ENY] - C[RHO]);
-  UH[UX1] = aisg * C[UX1];
-  UH[UX2] = aisg * C[UX2];
-  UH[UX3] = aisg * C[UX3];
-  UH[BX1] = aisg * C[BX1];
-  UH[BX2] = aisg * C[BX2];
-  UH[BX3] = aisg * C[BX3];
-  UH[ENT] = aisg * C[ENT];
-}
-
-__device__ __forceinline__ void c2p_write(const Dims &d, double *P, int b, int k, int j, int i,
-                                          const double PH[9]) {
-  const long long q = vidx(d, b, 0, k, j, i);
-  const long long vs = d.ncell;
-  P[q] = PH[RHO];
-  P[q + vs] = PH[ENY];
-  P[q + 2 * vs] = PH[UX1];
-  P[q + 3 * vs] = PH[UX2];
-  P[q + 4 * vs] = PH[UX3];
-}
-
-// Recovery, first pass: Kastaun (robuster), or Scheme2D of the chain. Cells
-// where Scheme2D fails are appended to `retry` (their primitives are left
-// untouched) and finished by k_recovery_retry, so the long 1Dvsq/1D Newton
-// loops of a few cells do not hold whole warps of converged cells.
-template <int MT>
-__global__ void __launch_bounds__(kThreads, 3) k_recovery(Dims d, pangu_params p, double *P,
-                                                       const double *U, double *flag,
-                                                       unsigned long long *cnt, int *nretry,
-                                                       long long *retry) {
-  int b, k, j, i;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
-  b = slot_of(d, b);
-  const bool robuster = p.recovery == PANGU_RECOVERY_ROBUSTER;
-  const long long fc = cidx(d, b, k, j, i);
-  if (MT == CKS) {
-    const double x = xc(d, b, 0, i), y = xc(d, b, 1, j), z = xc(d, b, 2, k);
-    const double a2 = p.a * p.a;
-    const double rad2 = x * x + y * y + z * z;
-    const double sa = (rad2 - a2) * (rad2 - a2) + 4.0 * a2 * z * z;
-    const bool exc = sqrt(0.5 * (rad2 - a2 + sqrt(sa))) < p.r_excise;
-    count(cnt, job_of(d, b), PANGU_CNT_EXCISED, exc);
-    if (exc) {
-      if (!robuster) flag[fc] = 0;
-      return;
-    }
-  }
-  Geo g;
-  cell_metric<MT>(d, p, b, k, j, i, g);
-  double UH[9], PH[9];
-  c2p_inputs<MT>(d, p, P, U, b, k, j, i, g, UH, PH, true);
-  const double gam = p.adiabatic_index;
-  if (robuster) {
-    const int st = invert_kastaun(UH, PH, gam, g);
-    count(cnt, job_of(d, b), PANGU_CNT_KASTAUN_FAIL, st != 0);
-    if (st != 0) return;
-  } else {
-    Harm hs;
-    harm_setup<MT>(UH, g, hs);
-    const bool ok = invert_2d<MT>(UH, PH, gam, g, hs) == 0;
-    count(cnt, job_of(d, b), PANGU_CNT_C2P_2D, ok);
-    append(nretry, retry, !ok, fc);
-    flag[fc] = ok ? 1.0 : 0.0;
-    if (!ok) return;
-  }
-  c2p_write(d, P, b, k, j, i, PH);
-}
-
-// Recovery, second pass over the cells Scheme2D failed: Scheme1Dvsq, then
-// Scheme1D (invertor.cc:185-197).
-template <int MT>
-__global__ void __launch_bounds__(kThreads) k_recovery_retry(Dims d, pangu_params p, double *P,
-                                                             const double *U, double *flag,
-                                                             unsigned long long *cnt,
-                                                             const int *nretry,
-                                                             const long long *retry) {
-  const int n = *nretry;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
-       t += (long long)gridDim.x * blockDim.x) {
-    const long long fc = retry[t];
-    const int b = (int)(fc / d.ncell);
-    long long c = fc - (long long)b * d.ncell;
-    const int k = (int)(c / ((long long)d.N2 * d.N1));
-    c -= (long long)k * d.N2 * d.N1;
-    const int j = (int)(c / d.N1), i = (int)(c % d.N1);
-    Geo g;
-    cell_metric<MT>(d, p, b, k, j, i, g);
-    double UH[9], PH[9];
-    c2p_inputs<MT>(d, p, P, U, b, k, j, i, g, UH, PH, false);
-    const double gam = p.adiabatic_index;
-    Harm hs;
-    harm_setup<MT>(UH, g, hs);
-    bool ok = invert_1dvsq<MT>(UH, PH, gam, g, hs) == 0;
-    count(cnt, job_of(d, b), PANGU_CNT_C2P_1DVSQ, ok);
-    if (!ok) {
-      ok = invert_1d<MT>(UH, PH, gam, g, hs) == 0;
-      count(cnt, job_of(d, b), PANGU_CNT_C2P_1D, ok);
-      count(cnt, job_of(d, b), PANGU_CNT_C2P_FAIL, !ok);
-    }
-    flag[fc] = ok ? 1.0 : 0.0;
-    c2p_write(d, P, b, k, j, i, PH);
-  }
-}
-
-// ---------------------------------------------------------------------------
-// ApplyElectronHeating (electron_heating.cc:14-112).
-// ---------------------------------------------------------------------------
-template <int MT>
-__global__ void __launch_bounds__(kThreads) k_heating(Dims d, pangu_params p, double *P,
-                                                      const double *U) {
-  int b, k, j, i;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
-  b = slot_of(d, b);
-  Geo g;
-  cell_metric<MT>(d, p, b, k, j, i, g);
-  double pc[NPRIM];
-  load_prim(d, P, b, k, j, i, pc);
-  State s;
-  calc_state<MT>(pc, g, s);
-  const long long q = vidx(d, b, 0, k, j, i);
-  const long long vs = d.ncell;
-  const double cr = U[q];
-  const HeatParams hp = {p.model, p.adiabatic_index, p.gamma_p, p.gamma_e, p.fel_constant,
-                         p.ratio_min, p.ratio_max, p.limit_kel, p.suppress_highb_heat,
-                         p.enforce_positive_dissipation};
-  P[q + d.pidx[KEL] * vs] = heating_apply(hp, pc[RHO], pc[ENY], s.bsq, U[q + d.pidx[ENT] * vs] / cr,
-                                          pc[ENT], U[q + d.pidx[KEL] * vs] / cr);
-}
-
-// ---------------------------------------------------------------------------
-// FixRecovery (recovery_fixer.cc:12-119), two phases over the failure list.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_fixrec_scan(Dims d, pangu_params p,
-                                                          const double *flag, int *count_out,
-                                                          long long *list) {
-  int b, k, j, i;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
-  b = slot_of(d, b);
-  const long long fc = cidx(d, b, k, j, i);
-  if (flag[fc] != 0) return;
-  if (p.metric_type == PANGU_METRIC_CKS) {
-    const double x = xc(d, b, 0, i), y = xc(d, b, 1, j), z = xc(d, b, 2, k);
-    const double a2 = p.a * p.a;
-    const double rad2 = x * x + y * y + z * z;
-    const double sa = (rad2 - a2) * (rad2 - a2) + 4.0 * a2 * z * z;
-    if (sqrt(0.5 * (rad2 - a2 + sqrt(sa))) < p.r_excise) return;
-  }
-  const int n = atomicAdd(count_out, 1);
-  list[n] = fc;
-}
-
-__global__ void __launch_bounds__(kThreads) k_fixrec_compute(Dims d, const int *count_in,
-                                                             const long long *list,
-                                                             const double *P, const double *flag,
-                                                             double *vals) {
-  const int n = *count_in;
-  const int off2 = d.js != d.je ? 1 : 0;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
-       t += (long long)gridDim.x * blockDim.x) {
-    const long long fc = list[t];
-    const long long b = fc / d.ncell;
-    const long long c = fc - b * d.ncell;
-    const long long sj = (long long)off2 * d.N1;
-    auto fl = [&](long long o) { return (int)flag[fc + o]; };
-    const int pf1 = fl(sj - 1), pf2 = fl(sj), pf3 = fl(sj + 1), pf4 = fl(1);
-    const int pf5 = fl(-sj + 1), pf6 = fl(-sj), pf7 = fl(-sj - 1), pf8 = fl(-1);
-    for (int v = 0; v < d.NF; ++v) {
-      const double *q = P + (b * d.NF + v) * d.ncell + c;
-      double val;
-      if (pf2 && pf4 && pf6 && pf8)
-        val = 0.25 * (q[sj] + q[-sj] + q[-1] + q[1]);
-      else if (pf1 && pf3 && pf5 && pf7)
-        val = 0.25 * (q[sj + 1] + q[sj - 1] + q[-sj + 1] + q[-sj - 1]);
-      else
-        val = 0.125 * (q[sj - 1] + q[sj] + q[sj + 1] + q[1] + q[-sj + 1] + q[-sj] + q[-sj - 1] +
-                       q[-1]);
-      vals[t * d.NF + v] = val;
-    }
-  }
-}
-
-__global__ void __launch_bounds__(kThreads) k_fixrec_write(Dims d, const int *count_in,
-                                                           const long long *list,
-                                                           const double *vals, double *P,
-                                                           double *flag,
-                                                           unsigned long long *cnt) {
-  const int n = *count_in;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
-       t += (long long)gridDim.x * blockDim.x) {
-    const long long fc = list[t];
-    const long long b = fc / d.ncell;
-    const long long c = fc - b * d.ncell;
-    for (int v = 0; v < d.NF; ++v) P[(b * d.NF + v) * d.ncell + c] = vals[t * d.NF + v];
-    for (int v = 2; v < 5; ++v) P[(b * d.NF + v) * d.ncell + c] = 0.;
-    flag[fc] = 1;
-    count(cnt, job_of(d, (int)b), PANGU_CNT_FIXRECOVERY, true);
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Physical boundary conditions (outflow / reflecting) of all faces in one
-// pass. Applying the faces in the order ix1, ox1, ix2, ox2, ix3, ox3, each over
-// its full transverse range, leaves every ghost cell equal to one interior
-// (or exchanged) cell, reached by applying each direction's rule in turn to
-// the index, with the reflections' sign flips composed. The kernel computes
-// that composition directly; its sources are never written by it.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_bcs(Dims d, int enable_B, double *P,
-                                                  double *flag) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)d.NB * d.ncell) return;
-  const int bb = (int)(t / d.ncell);
-  long long c = t - (long long)bb * d.ncell;
-  const int b = slot_of(d, bb);
-  int idx[3];
-  idx[2] = (int)(c / ((long long)d.N2 * d.N1));
-  c -= (long long)idx[2] * d.N2 * d.N1;
-  idx[1] = (int)(c / d.N1);
-  idx[0] = (int)(c % d.N1);
-  const signed char *bcf = d.bcf + 6 * b;  // -1 unless the face is a physical boundary
-  const int st[3] = {d.is, d.js, d.ks}, en[3] = {d.ie, d.je, d.ke};
-  int src[3] = {idx[0], idx[1], idx[2]};
-  int flip[3] = {0, 0, 0};
-  bool ghost = false;
-#pragma unroll
-  for (int dir = 0; dir < 3; ++dir) {
-    const int x = src[dir];
-    int kind = -1, outer = 0;
-    if (x < st[dir]) {
-      kind = bcf[2 * dir];
-    } else if (x > en[dir]) {
-      kind = bcf[2 * dir + 1];
-      outer = 1;
-    }
-    if (kind < 0) continue;
-    ghost = true;
-    if (kind == PANGU_BC_OUTFLOW) {
-      src[dir] = outer ? en[dir] : st[dir];
-    } else {
-      src[dir] = outer ? (2 * en[dir] + 1 - x) : (2 * st[dir] - 1 - x);
-      flip[dir] ^= 1;
-    }
-  }
-  if (!ghost) return;
-  const long long dc = cidx(d, b, idx[2], idx[1], idx[0]);
-  const long long sc = cidx(d, b, src[2], src[1], src[0]);
-  const long long base = (long long)b * (d.NF - 1) * d.ncell;
-  for (int v = 0; v < d.NF; ++v) {
-    double val = P[base + sc + v * d.ncell];
-#pragma unroll
-    for (int dir = 0; dir < 3; ++dir) {
-      const bool vel = v == d.pidx[UX1] + dir;
-      const bool mag = enable_B && v == d.pidx[BX1] + dir;
-      if (flip[dir] && (vel || mag)) val = -val;
-    }
-    P[base + dc + v * d.ncell] = val;
-  }
-  if (flag) flag[dc] = flag[sc];
-}
-
-// ---------------------------------------------------------------------------
-// EstimateTimestepMesh (timestep_estimation.cc:13-102).
-// ---------------------------------------------------------------------------
-__global__ void k_dt_init(int n, unsigned long long *mins) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) mins[t] = (unsigned long long)__double_as_longlong(DBL_MAX);
-}
-
-// One CTA row per mesh block (blockIdx.y); warp and CTA minima, then one
-// atomic per CTA and direction. Positive doubles order like their bit
-// patterns; a NaN speed never lowers the minimum (the reference's
-// "if (dt_min > dt)" skips it as well).
-__global__ void __launch_bounds__(kThreads) k_dt_reduce(Dims d, double cfl,
-                                                        const double *alfven,
-                                                        unsigned long long *mins) {
-  __shared__ unsigned long long red[3][kThreads / 32];
-  const int b = slot_of(d, blockIdx.y);
-  const int ni = d.ie - d.is + 1, nj = d.je - d.js + 1, nk = d.ke - d.ks + 1;
-  const long long per = (long long)ni * nj * nk;
-  const unsigned long long big = (unsigned long long)__double_as_longlong(DBL_MAX);
-  unsigned long long m[3] = {big, big, big};
-  const double cdx[3] = {MUL(cfl, dx_of(d, b, 0)), MUL(cfl, dx_of(d, b, 1)),
-                         MUL(cfl, dx_of(d, b, 2))};
-  const int act[3] = {d.N1 > 1, d.N2 > 1, d.N3 > 1};
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < per;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int k = d.ks + (int)(t / ((long long)ni * nj));
-    const long long r = t - (long long)(k - d.ks) * ni * nj;
-    const int j = d.js + (int)(r / ni);
-    const int i = d.is + (int)(r - (long long)(j - d.js) * ni);
-#pragma unroll
-    for (int dir = 0; dir < 3; ++dir) {
-      if (!act[dir]) continue;
-      const double dt = cdx[dir] / alfven[aidx(d, b, dir, k, j, i)];
-      if (dt >= 0.0) {
-        const unsigned long long bits = (unsigned long long)__double_as_longlong(dt);
-        m[dir] = bits < m[dir] ? bits : m[dir];
-      }
-    }
-  }
-#pragma unroll
-  for (int dir = 0; dir < 3; ++dir) {
-    unsigned long long v = m[dir];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
-      v = w < v ? w : v;
-    }
-    if ((threadIdx.x & 31) == 0) red[dir][threadIdx.x >> 5] = v;
-  }
-  __syncthreads();
-  if (threadIdx.x < 3) {
-    const int dir = threadIdx.x;
-    unsigned long long v = red[dir][0];
-    for (int w = 1; w < kThreads / 32; ++w) v = red[dir][w] < v ? red[dir][w] : v;
-    if (act[dir]) atomicMin(&mins[b * 3 + dir], v);
-  }
-}
-
-// One thread per job: the minimum over the job's blocks, active entries
-// jr[3q+1] .. jr[3q+2]-1 of job jr[3q] (the whole domain as job 0 when jr is
-// null), written to dt_out[job].
-__global__ void k_dt_finalize(Dims d, int njobs, const int *jr, const unsigned long long *mins,
-                              double *dt_out) {
-  if (blockIdx.x != 0) return;
-  for (int q = threadIdx.x; q < njobs; q += blockDim.x) {
-    const int job = jr ? jr[3 * q] : 0;
-    const int s0 = jr ? jr[3 * q + 1] : 0, s1 = jr ? jr[3 * q + 2] : d.NB;
-    double gmin = DBL_MAX;
-    for (int bb = s0; bb < s1; ++bb) {
-      const int b = slot_of(d, bb);
-      const double m0 = __longlong_as_double((long long)mins[3 * b + 0]);
-      const double m1 = __longlong_as_double((long long)mins[3 * b + 1]);
-      const double m2 = __longlong_as_double((long long)mins[3 * b + 2]);
-      const double bdt = 1.0 / (1.0 / m0 + 1.0 / m1 + 1.0 / m2);
-      if (bdt < gmin) gmin = bdt;
-    }
-    dt_out[job] = gmin;
-  }
-}
-
-__global__ void k_update_dt(int njobs, const int *jr, double *dt, const double *dt_est,
-                            double factor) {
-  if (blockIdx.x != 0) return;
-  for (int q = threadIdx.x; q < njobs; q += blockDim.x) {
-    const int job = jr ? jr[3 * q] : 0;
-    const double grown = factor * dt[job];
-    dt[job] = (dt_est[job] < grown) ? dt_est[job] : grown;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// launch helpers
-// ---------------------------------------------------------------------------
-inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
-
-inline int check_launch() {
-  const cudaError_t e = cudaGetLastError();
-  return e == cudaSuccess ? PANGU_OK : PANGU_ECUDA;
-}
-
-inline long long box_count(int NB, int k0, int k1, int j0, int j1, int i0, int i1) {
-  if (k1 < k0 || j1 < j0 || i1 < i0) return 0;
-  return (long long)NB * (k1 - k0 + 1) * (j1 - j0 + 1) * (i1 - i0 + 1);
-}
-
-#define DISPATCH_MT(mt, KERNEL, grid, stream, ...)                          \
-  do {                                                                      \
-    switch (mt) {                                                           \
-      case PANGU_METRIC_MKS: KERNEL<MKS><<<grid, kThreads, 0, stream>>>(__VA_ARGS__); break; \
-      case PANGU_METRIC_BL: KERNEL<BL><<<grid, kThreads, 0, stream>>>(__VA_ARGS__); break;   \
-      case PANGU_METRIC_CKS: KERNEL<CKS><<<grid, kThreads, 0, stream>>>(__VA_ARGS__); break; \
-      default: KERNEL<MINKOWSKI><<<grid, kThreads, 0, stream>>>(__VA_ARGS__); break;         \
-    }                                                                       \
-  } while (0)
-
-#define DISPATCH_MT_T(mt, KERNEL, grid, threads, stream, ...)                                 \
-  do {                                                                                       \
-    switch (mt) {                                                                            \
-      case PANGU_METRIC_MKS: KERNEL<MKS><<<grid, threads, 0, stream>>>(__VA_ARGS__); break;   \
-      case PANGU_METRIC_BL: KERNEL<BL><<<grid, threads, 0, stream>>>(__VA_ARGS__); break;     \
-      case PANGU_METRIC_CKS: KERNEL<CKS><<<grid, threads, 0, stream>>>(__VA_ARGS__); break;   \
-      default: KERNEL<MINKOWSKI><<<grid, threads, 0, stream>>>(__VA_ARGS__); break;           \
-    }                                                                                        \
-  } while (0)
-
-inline unsigned grid_flux(long long n) {
-  return (unsigned)std::max<long long>(1, (n + kFluxThreads - 1) / kFluxThreads);
-}
-
-bool pack_ok(const pangu_engine *e, const pangu_pack *md) {
-  if (!e || !md || !md->prim || !md->cons || !md->flux1 || !md->alfven || !md->efield) return false;
-  if (e->d.ndim >= 2 && !md->flux2) return false;
-  if (e->d.ndim == 3 && !md->flux3) return false;
-  if (e->p.recovery == PANGU_RECOVERY_CHAINER && !md->flag) return false;
-  return true;
-}
-
-int run_fix_primitive(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
-  const Dims &d = e->d;
-  const long long n = (long long)d.NB * d.ncell;
-  DISPATCH_MT(e->p.metric_type, k_fix_primitive, grid_for(n), s, d, e->p, md->prim, e->d_cnt);
-  ++e->launches;
-  return check_launch();
-}
-
-int run_calc_cons(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
-  const Dims &d = e->d;
-  const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
-  DISPATCH_MT(e->p.metric_type, k_calc_cons, grid_for(n), s, d, e->p, md->prim, md->cons);
-  ++e->launches;
-  return check_launch();
-}
-
-int run_fluxes(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
-  const Dims &d = e->d;
-  const bool hll = e->p.riemann_solver == PANGU_RIEMANN_HLL;
-  for (int dir = 1; dir <= d.ndim; ++dir) {
-    int k0 = d.ks - d.o3, k1 = d.ke + d.o3, j0 = d.js - d.o2, j1 = d.je + d.o2;
-    int i0 = d.is - d.o1, i1 = d.ie + d.o1;
-    if (dir == 1) { i0 = d.is; i1 = d.ie + 1; }
-    if (dir == 2) { j0 = d.js; j1 = d.je + 1; }
-    if (dir == 3) {  // hll.cc:293-296 narrows the transverse range
-      k0 = d.ks; k1 = d.ke + 1;
-      if (hll) { j0 = d.js; j1 = d.je; i0 = d.is; i1 = d.ie; }
-    }
-    double *F = dir == 1 ? md->flux1 : (dir == 2 ? md->flux2 : md->flux3);
-#define FLUX_ARGS d, e->p, k0, k1, j0, j1, i0, i1, md->prim, F, md->alfven
-    if (dir == 1) {
-      const int nseg = (i1 - i0 + 1 + kFacesPerWarp - 1) / kFacesPerWarp;
-      const long long warps = (long long)d.NB * (k1 - k0 + 1) * (j1 - j0 + 1) * nseg;
-      DISPATCH_MT_T(e->p.metric_type, k_flux_x1, grid_flux(32 * warps), kFluxThreads, s, FLUX_ARGS);
-    } else {
-      const int m = dir == 2 ? (j1 - j0 + 1) : (k1 - k0 + 1);
-      const int na = dir == 2 ? (k1 - k0 + 1) : (j1 - j0 + 1);
-      const long long n = (long long)d.NB * na * ((m + kMarch - 1) / kMarch) * (i1 - i0 + 1);
-      if (dir == 2)
-        DISPATCH_MT_T(e->p.metric_type, k_flux_march2, grid_flux(n), kFluxThreads, s, FLUX_ARGS);
-      else
-        DISPATCH_MT_T(e->p.metric_type, k_flux_march3, grid_flux(n), kFluxThreads, s, FLUX_ARGS);
-    }
-#undef FLUX_ARGS
-    ++e->launches;
-    const int rc = check_launch();
-    if (rc) return rc;
-  }
-  return PANGU_OK;
-}
-
-int run_ct(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
-  const Dims &d = e->d;
-  const int o1 = d.N1 > 1, o2 = d.N2 > 1, o3 = d.N3 > 1;
-  k_ct_emf<<<grid_for(box_count(d.NB, d.ks, d.ke + o3, d.js, d.je + o2, d.is, d.ie + o1)),
-             kThreads, 0, s>>>(d, md->flux1, md->flux2, md->flux3, md->efield);
-  ++e->launches;
-  double *F[3] = {md->flux1, md->flux2, md->flux3};
-  for (int dir = 1; dir <= d.ndim; ++dir) {
-    const int ei = dir == 1 ? o1 : 0, ej = dir == 2 ? o2 : 0, ek = dir == 3 ? o3 : 0;
-    const long long n = box_count(d.NB, d.ks, d.ke + ek, d.js, d.je + ej, d.is, d.ie + ei);
-    k_ct_faces<<<grid_for(n), kThreads, 0, s>>>(d, dir, F[dir - 1], md->efield);
-    ++e->launches;
-  }
-  return check_launch();
-}
-
+using namespace pgk64;
+
+// The mixed-precision instantiation of the launch helpers (engine_mixed.cu).
+namespace pgkmx {
+int run_fix_primitive(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
+int run_calc_cons(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
+int run_fluxes(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
+int run_ct(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
 int run_update(pangu_engine *e, const pangu_pack *mi, const pangu_pack *m0, const pangu_pack *m1,
-               double beta, const double *dt, cudaStream_t s) {
-  const Dims &d = e->d;
-  const long long n = box_count(d.NB * d.NF, d.ks, d.ke, d.js, d.je, d.is, d.ie);
-  k_flux_div_update<<<grid_for(n), kThreads, 0, s>>>(d, m0->flux1, m0->flux2, m0->flux3,
-                                                     mi->cons, m1->cons, beta, dt);
-  ++e->launches;
-  return check_launch();
-}
-
-int run_exchange_range(pangu_engine *e, const pangu_pack *md, long long off, long long n,
-                       cudaStream_t s) {
-  if (n == 0) return PANGU_OK;
-  k_exchange<<<grid_for(n), kThreads, 0, s>>>(e->d, n, e->d_xdst + off, e->d_xsrc + off, md->prim,
-                                              md->flag);
-  ++e->launches;
-  return check_launch();
-}
-
-int run_exchange(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
-  return run_exchange_range(e, md, 0, e->nxch, s);
-}
-
+               double beta, const double *dt, cudaStream_t s);
+int run_exchange(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
 int run_source(pangu_engine *e, const pangu_pack *md, double beta, const double *dt,
-               cudaStream_t s) {
-  const Dims &d = e->d;
-  if (e->p.metric_type == PANGU_METRIC_MINKOWSKI) return PANGU_OK;  // zero connection
-  const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
-  DISPATCH_MT(e->p.metric_type, k_source, grid_for(n), s, d, e->p, md->prim, md->cons, beta, dt);
-  ++e->launches;
-  return check_launch();
-}
+               cudaStream_t s);
+int run_recovery(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
+int run_heating(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
+int run_fix_recovery(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
+int run_bcs(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
+int run_estimate_dt(pangu_engine *e, const pangu_pack *md, double *dt_out, cudaStream_t s);
+int run_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
+              double beta, const double *dt, double *dt_est, cudaStream_t s);
+int run_job_start(pangu_engine *e, int job, const pangu_pack *base, const pangu_pack *one,
+                  cudaStream_t s);
+}  // namespace pgkmx
 
-int run_recovery(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
-  const Dims &d = e->d;
-  const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
-  if (cudaMemsetAsync(e->d_fail_count, 0, sizeof(int), s) != cudaSuccess) return PANGU_ECUDA;
-  DISPATCH_MT(e->p.metric_type, k_recovery, grid_for(n), s, d, e->p, md->prim, md->cons, md->flag,
-              e->d_cnt, e->d_fail_count, e->d_fail_list);
-  ++e->launches;
-  if (e->p.recovery == PANGU_RECOVERY_CHAINER) {
-    DISPATCH_MT(e->p.metric_type, k_recovery_retry, 2 * 148, s, d, e->p, md->prim, md->cons,
-                md->flag, e->d_cnt, e->d_fail_count, e->d_fail_list);
-    ++e->launches;
-  }
-  return check_launch();
-}
+// Launch helper of the engine's precision.
+#define RUN(fn, ...)                                                               \
+  (e->p.precision == PANGU_PRECISION_MIXED ? pgkmx::fn(__VA_ARGS__) : pgk64::fn(__VA_ARGS__))
 
-int run_heating(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
-  const Dims &d = e->d;
-  if (!e->p.enable_heating) return PANGU_OK;
-  const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
-  DISPATCH_MT(e->p.metric_type, k_heating, grid_for(n), s, d, e->p, md->prim, md->cons);
-  ++e->launches;
-  return check_launch();
-}
-
-int run_fix_recovery(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
-  const Dims &d = e->d;
-  if (cudaMemsetAsync(e->d_fail_count, 0, sizeof(int), s) != cudaSuccess) return PANGU_ECUDA;
-  const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
-  k_fixrec_scan<<<grid_for(n), kThreads, 0, s>>>(d, e->p, md->flag, e->d_fail_count,
-                                                 e->d_fail_list);
-  const unsigned g = 2 * 148;
-  k_fixrec_compute<<<g, kThreads, 0, s>>>(d, e->d_fail_count, e->d_fail_list, md->prim, md->flag,
-                                          e->d_fail_vals);
-  k_fixrec_write<<<g, kThreads, 0, s>>>(d, e->d_fail_count, e->d_fail_list, e->d_fail_vals,
-                                        md->prim, md->flag, e->d_cnt);
-  e->launches += 3;
-  return check_launch();
-}
-
-// Physical BCs of the blocks of d (all active blocks, or one job's).
-int run_bcs(pangu_engine *e, const Dims &d, bool any_bc, const pangu_pack *md, cudaStream_t s) {
-  if (!any_bc || d.NB == 0) return PANGU_OK;
-  k_bcs<<<grid_for((long long)d.NB * d.ncell), kThreads, 0, s>>>(d, e->p.enable_B, md->prim,
-                                                                md->flag);
-  ++e->launches;
-  return check_launch();
-}
-
-int run_bcs(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
-  return run_bcs(e, e->d, e->any_bc, md, s);
-}
-
-int run_estimate_dt(pangu_engine *e, const pangu_pack *md, double *dt_out, cudaStream_t s) {
-  const Dims &d = e->d;
-  k_dt_init<<<grid_for(3 * e->capacity), kThreads, 0, s>>>(3 * e->capacity, e->d_dtmin);
-  const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
-  const unsigned gx = (unsigned)std::min<long long>((n / std::max(1, d.NB) + kThreads - 1) / kThreads, 592);
-  k_dt_reduce<<<dim3(std::max(1u, gx), d.NB), kThreads, 0, s>>>(d, e->p.cfl_number, md->alfven,
-                                                                 e->d_dtmin);
-  k_dt_finalize<<<1, 128, 0, s>>>(d, e->njobs_active, e->d_jr, e->d_dtmin, dt_out);
-  e->launches += 3;
-  return check_launch();
-}
-
-template <class T>
-int dalloc(T **p, size_t n) {
-  return cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(T)) == cudaSuccess ? PANGU_OK
-                                                                                   : PANGU_ENOMEM;
-}
-
-}  // namespace
 
 // ===========================================================================
 // C ABI
@@ -1576,6 +71,9 @@ int pangu_engine_destroy(pangu_engine *e) {
   cudaFree(e->d_cnt);
   cudaFree(e->d_fail_count);
   cudaFree(e->d_fail_list);
+  cudaFree(e->d_fix_count);
+  cudaFree(e->d_fix_list);
+  cudaFree(e->d_tmp_slots);
   cudaFree(e->d_fail_vals);
   cudaFree(e->d_dtmin);
   delete e;
@@ -1589,7 +87,7 @@ namespace {
 int validate_params(const pangu_params &p) {
   if (p.riemann_solver < 0 || p.riemann_solver > 1 || p.limiter < 0 || p.limiter > 1 ||
       p.recovery < 0 || p.recovery > 1 || p.metric_type < 0 || p.metric_type > 3 || p.model < 0 ||
-      p.model > 5)
+      p.model > 5 || p.precision < 0 || p.precision > 1)
     return PANGU_EINVAL;
   return PANGU_OK;
 }
@@ -1662,8 +160,15 @@ int pool_init(pangu_engine *e, int capacity, int max_jobs) {
   rc |= dalloc(&e->d_cnt, (size_t)max_jobs * PANGU_NCOUNTERS);
   rc |= dalloc(&e->d_fail_count, 1);
   rc |= dalloc(&e->d_fail_list, (size_t)e->fail_cap);
+  rc |= dalloc(&e->d_fix_count, 1);
+  rc |= dalloc(&e->d_fix_list, (size_t)e->fail_cap);
   rc |= dalloc(&e->d_fail_vals, (size_t)e->fail_cap * d.NF);
   rc |= dalloc(&e->d_dtmin, 3 * (size_t)capacity);
+  rc |= dalloc(&e->d_tmp_slots, capacity);
+  // every ghost cell of a slot has at most one exchange source
+  e->xch_cap = (long long)capacity * (d.ncell - (long long)e->m.nx1 * e->m.nx2 * e->m.nx3);
+  rc |= dalloc(&e->d_xdst, (size_t)e->xch_cap);
+  rc |= dalloc(&e->d_xsrc, (size_t)e->xch_cap);
   if (p.metric_type == PANGU_METRIC_MKS || p.metric_type == PANGU_METRIC_BL) {
     const TabLayout T = p.metric_type == PANGU_METRIC_MKS ? tab_layout(MKS) : tab_layout(BL);
     const size_t pc = (size_t)d.N2 * d.N1, p1 = (size_t)d.N2 * (d.N1 + 1),
@@ -1708,14 +213,7 @@ int pool_rebuild(pangu_engine *e) {
     xs.insert(xs.end(), J.xsrc.begin(), J.xsrc.end());
     e->any_bc = e->any_bc || J.any_bc;
   }
-  if ((long long)xd.size() > e->xch_cap) {
-    cudaFree(e->d_xdst);
-    cudaFree(e->d_xsrc);
-    e->d_xdst = e->d_xsrc = nullptr;
-    e->xch_cap = 0;
-    if (dalloc(&e->d_xdst, xd.size()) || dalloc(&e->d_xsrc, xs.size())) return PANGU_ENOMEM;
-    e->xch_cap = (long long)xd.size();
-  }
+  if ((long long)xd.size() > e->xch_cap) return PANGU_ETOOBIG;  // cannot happen
   bool ok = true;
   if (!active.empty())
     ok &= cudaMemcpy(e->d_active, active.data(), active.size() * sizeof(int),
@@ -1727,6 +225,8 @@ int pool_rebuild(pangu_engine *e) {
     ok &= cudaMemcpy(e->d_xdst, xd.data(), xd.size() * 8, cudaMemcpyHostToDevice) == cudaSuccess;
     ok &= cudaMemcpy(e->d_xsrc, xs.data(), xs.size() * 8, cudaMemcpyHostToDevice) == cudaSuccess;
   }
+  // a pageable upload may still be in flight when cudaMemcpy returns
+  ok &= cudaStreamSynchronize(0) == cudaSuccess;
   if (!ok) return PANGU_ECUDA;
   e->d.NB = (int)active.size();
   e->nxch = (long long)xd.size();
@@ -1751,7 +251,6 @@ int pool_attach(pangu_engine *e, const pangu_mesh &m, double a, double h, int *j
   for (int sl = 0; sl < e->capacity && (long long)slots.size() < nbl; ++sl)
     if (!e->slot_used[sl]) slots.push_back(sl);
   if ((long long)slots.size() < nbl) return PANGU_EFULL;
-  if (cudaDeviceSynchronize() != cudaSuccess) return PANGU_ECUDA;
 
   PoolJob J;
   J.m = m;
@@ -1800,12 +299,10 @@ int pool_attach(pangu_engine *e, const pangu_mesh &m, double a, double h, int *j
   if (!ok) return PANGU_ECUDA;
   if (e->p.metric_type == PANGU_METRIC_MKS || e->p.metric_type == PANGU_METRIC_BL) {
     // static metric tables of the job's slots, with the job's a and h
-    int *d_slots = nullptr;
-    if (dalloc(&d_slots, slots.size())) return PANGU_ENOMEM;
-    ok = cudaMemcpy(d_slots, slots.data(), slots.size() * sizeof(int), cudaMemcpyHostToDevice) ==
-         cudaSuccess;
+    ok = cudaMemcpy(e->d_tmp_slots, slots.data(), slots.size() * sizeof(int),
+                    cudaMemcpyHostToDevice) == cudaSuccess;
     Dims dj = d;
-    dj.slot = d_slots;
+    dj.slot = e->d_tmp_slots;
     dj.NB = (int)nbl;
     const long long n = (long long)dj.NB * ((long long)d.N2 * d.N1 + (long long)d.N2 * (d.N1 + 1) +
                                             (long long)(d.N2 + 1) * d.N1);
@@ -1814,9 +311,8 @@ int pool_attach(pangu_engine *e, const pangu_mesh &m, double a, double h, int *j
         k_build_tables<MKS><<<grid_for(n), kThreads>>>(dj, J.p, e->d_ctab, e->d_f1tab, e->d_f2tab);
       else
         k_build_tables<BL><<<grid_for(n), kThreads>>>(dj, J.p, e->d_ctab, e->d_f1tab, e->d_f2tab);
-      ok = cudaGetLastError() == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess;
+      ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(0) == cudaSuccess;
     }
-    cudaFree(d_slots);
     if (!ok) return PANGU_ECUDA;
   }
   J.live = true;
@@ -1892,31 +388,11 @@ int pangu_job_start(pangu_engine *e, int32_t job, const pangu_pack *base, const 
   if (!pack_ok(e, base) || !pack_ok(e, one) || job < 0 || job >= e->max_jobs ||
       !e->jobs[job].live)
     return PANGU_EINVAL;
-  cudaStream_t s = S(stream);
-  const PoolJob &J = e->jobs[job];
-  int first = 0;
-  for (int q = 0; q < job; ++q)
-    if (e->jobs[q].live) first += (int)e->jobs[q].slots.size();
-  Dims dj = e->d;
-  dj.slot = e->d_active + first;
-  dj.NB = (int)J.slots.size();
-  int rc = run_exchange_range(e, base, e->xoff[job], (long long)J.xdst.size(), s);
-  if (!rc) rc = run_bcs(e, dj, J.any_bc, base, s);
-  if (rc) return rc;
-  const size_t blk = (size_t)e->d.NF * e->d.ncell;
-  for (int sl : J.slots) {
-    if (cudaMemcpyAsync(one->prim + sl * blk, base->prim + sl * blk, blk * 8,
-                        cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
-        cudaMemcpyAsync(one->cons + sl * blk, base->cons + sl * blk, blk * 8,
-                        cudaMemcpyDeviceToDevice, s) != cudaSuccess)
-      return PANGU_ECUDA;
-  }
-  return PANGU_OK;
+  return RUN(run_job_start, e, job, base, one, S(stream));
 }
 
 int pangu_job_detach(pangu_engine *e, int32_t job) {
   if (!e || job < 0 || job >= e->max_jobs || !e->jobs[job].live) return PANGU_EINVAL;
-  if (cudaDeviceSynchronize() != cudaSuccess) return PANGU_ECUDA;
   for (int sl : e->jobs[job].slots) e->slot_used[sl] = 0;
   e->jobs[job] = PoolJob{};
   return pool_rebuild(e);
@@ -1940,59 +416,59 @@ int pangu_active_blocks(const pangu_engine *e) { return e ? e->d.NB : PANGU_EINV
 
 int pangu_fix_primitive(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
-  return run_fix_primitive(e, md, S(stream));
+  return RUN(run_fix_primitive, e, md, S(stream));
 }
 int pangu_calculate_conservative(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
-  return run_calc_cons(e, md, S(stream));
+  return RUN(run_calc_cons, e, md, S(stream));
 }
 int pangu_calculate_fluxes(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
-  return run_fluxes(e, md, S(stream));
+  return RUN(run_fluxes, e, md, S(stream));
 }
 int pangu_constrained_transport(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
   if (!e->p.enable_B) return PANGU_EINVAL;
-  return run_ct(e, md, S(stream));
+  return RUN(run_ct, e, md, S(stream));
 }
 int pangu_flux_divergence_update(pangu_engine *e, const pangu_pack *mc_init, const pangu_pack *mc0,
                                  const pangu_pack *mc1, double beta, const double *dt,
                                  void *stream) {
   if (!pack_ok(e, mc_init) || !pack_ok(e, mc0) || !pack_ok(e, mc1) || !dt) return PANGU_EINVAL;
   if (e->d.NB == 0) return PANGU_OK;
-  return run_update(e, mc_init, mc0, mc1, beta, dt, S(stream));
+  return RUN(run_update, e, mc_init, mc0, mc1, beta, dt, S(stream));
 }
 int pangu_exchange_ghosts(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
-  return run_exchange(e, md, S(stream));
+  return RUN(run_exchange, e, md, S(stream));
 }
 int pangu_add_geometric_source(pangu_engine *e, const pangu_pack *md, double beta, const double *dt,
                                void *stream) {
   GUARD(e, md);
   if (!dt) return PANGU_EINVAL;
-  return run_source(e, md, beta, dt, S(stream));
+  return RUN(run_source, e, md, beta, dt, S(stream));
 }
 int pangu_recovery(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
-  return run_recovery(e, md, S(stream));
+  return RUN(run_recovery, e, md, S(stream));
 }
 int pangu_apply_electron_heating(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
-  return run_heating(e, md, S(stream));
+  return RUN(run_heating, e, md, S(stream));
 }
 int pangu_fix_recovery(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
   if (e->p.recovery != PANGU_RECOVERY_CHAINER) return PANGU_EINVAL;
-  return run_fix_recovery(e, md, S(stream));
+  return RUN(run_fix_recovery, e, md, S(stream));
 }
 int pangu_apply_boundary_conditions(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
-  return run_bcs(e, md, S(stream));
+  return RUN(run_bcs, e, md, S(stream));
 }
 int pangu_estimate_dt(pangu_engine *e, const pangu_pack *md, double *dt_out, void *stream) {
   GUARD(e, md);
   if (!dt_out) return PANGU_EINVAL;
-  return run_estimate_dt(e, md, dt_out, S(stream));
+  return RUN(run_estimate_dt, e, md, dt_out, S(stream));
 }
 
 int pangu_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
@@ -2000,23 +476,7 @@ int pangu_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_
   if (!pack_ok(e, base) || !pack_ok(e, one) || !dt || (stage != 1 && stage != 2))
     return PANGU_EINVAL;
   if (e->d.NB == 0) return PANGU_OK;
-  cudaStream_t s = S(stream);
-  const pangu_pack *mc0 = stage == 1 ? base : one;
-  const pangu_pack *mc1 = stage == 1 ? one : base;
-  int rc;
-  if ((rc = run_fix_primitive(e, mc0, s))) return rc;
-  if ((rc = run_calc_cons(e, mc0, s))) return rc;
-  if ((rc = run_fluxes(e, mc0, s))) return rc;
-  if (e->p.enable_B && (rc = run_ct(e, mc0, s))) return rc;
-  if ((rc = run_update(e, base, mc0, mc1, beta, dt, s))) return rc;
-  if ((rc = run_exchange(e, mc1, s))) return rc;
-  if ((rc = run_source(e, mc1, beta, dt, s))) return rc;
-  if ((rc = run_recovery(e, mc1, s))) return rc;
-  if ((rc = run_heating(e, mc1, s))) return rc;
-  if (e->p.recovery == PANGU_RECOVERY_CHAINER && (rc = run_fix_recovery(e, mc1, s))) return rc;
-  if ((rc = run_bcs(e, mc1, s))) return rc;
-  if (stage == 2 && dt_est && (rc = run_estimate_dt(e, mc1, dt_est, s))) return rc;
-  return PANGU_OK;
+  return RUN(run_stage, e, stage, base, one, beta, dt, dt_est, S(stream));
 }
 
 // ---------------------------------------------------------------------------

@@ -1,0 +1,17 @@
+// engine_mixed.cu -- the mixed-precision instantiation of the engine's
+// kernels (namespace pgkmx): primitives stored in FP32; reconstruction,
+// Riemann fluxes and electron heating in FP32; conserved variables, the flux
+// divergence update, the geometric source, C2P, the metric and CT in FP64.
+// Built with FMA contraction on and the CUDA math library's pow/exp/log
+// (the exact build, engine.cu, keeps --fmad=false and correctly rounded
+// functions for bit-exact parity). The device helpers are compiled under
+// their own namespace name so the two builds never share a definition.
+#define pgd pgd_mixed
+#define PGD_POW ::pow
+#define PGD_EXP ::exp
+#define PGD_LOG ::log
+#include "engine_impl.cuh"
+
+#define PGK_NS pgkmx
+#define PGK_MIXED 1
+#include "kernels.cuh"

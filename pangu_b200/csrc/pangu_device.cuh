@@ -14,6 +14,14 @@
 
 #include "pgmath.h"
 
+// Powers, exponentials and logarithms: correctly rounded (pgmath.h) in the
+// exact build; an includer may substitute the CUDA math library.
+#ifndef PGD_POW
+#define PGD_POW pgm::pow
+#define PGD_EXP pgm::exp
+#define PGD_LOG pgm::log
+#endif
+
 namespace pgd {
 
 // variable_mnemonics.h:7-14
@@ -681,7 +689,7 @@ PGD int invert_2d(const double U[9], double prim[9], double g, const Geo &geo,
   if ((rho0 <= 0.) || (uu <= 0.)) return 5;
   prim[RHO] = rho0;
   prim[ENY] = uu;
-  prim[ENT] = (g - 1.) * uu * pgm::pow(rho0, -g);
+  prim[ENT] = (g - 1.) * uu * PGD_POW(rho0, -g);
   harm_velocity<MT>(s, Gamma, W, prim);
   return 0;
 }
@@ -691,7 +699,7 @@ PGD double w_of_vsq(double D, double K, double vsq, double g, double &p, double 
                     double &uu) {
   const double gtmp = (1. - vsq);
   rho = D * sqrt(gtmp);
-  p = (K * pgm::pow(rho, g));
+  p = (K * PGD_POW(rho, g));
   uu = (p / (g - 1.));
   return ((rho + uu + p) / gtmp);
 }
@@ -755,7 +763,7 @@ PGD int invert_1dvsq(const double U[9], double prim[9], double g, const Geo &geo
   if ((rho0 <= 0.) || (uu <= 0.)) return 5;
   prim[RHO] = rho0;
   prim[ENY] = uu;
-  prim[ENT] = (g - 1.) * uu * pgm::pow(rho0, -g);
+  prim[ENT] = (g - 1.) * uu * PGD_POW(rho0, -g);
   harm_velocity<MT>(s, Gamma, Wf, prim);
   return 0;
 }
@@ -771,7 +779,7 @@ PGD int invert_1d(const double U[9], double prim[9], double g, const Geo &geo, c
   double Gamma = sqrt(uvsq);
   const double Bsq = s.Bsq, QdotBsq = s.QdotBsq, Qtsq = s.Qtsq, D = s.D;
   double rho0 = D / Gamma;
-  double p = (K * pgm::pow(rho0, g));
+  double p = (K * PGD_POW(rho0, g));
   double uu = (p / (g - 1.));
   double w = rho0 + uu + p;
   double W_last = w * uvsq;
@@ -822,12 +830,12 @@ PGD int invert_1d(const double U[9], double prim[9], double g, const Geo &geo, c
   const double gtmp = sqrt(1. - vsq);
   Gamma = 1. / gtmp;
   rho0 = D * gtmp;
-  p = (K * pgm::pow(rho0, g));
+  p = (K * PGD_POW(rho0, g));
   uu = (p / (g - 1.));
   if ((rho0 <= 0.) || (uu <= 0.)) return 5;
   prim[RHO] = rho0;
   prim[ENY] = uu;
-  prim[ENT] = (g - 1.) * uu * pgm::pow(rho0, -g);
+  prim[ENT] = (g - 1.) * uu * PGD_POW(rho0, -g);
   harm_velocity<MT>(s, Gamma, W, prim);
   return 0;
 }
@@ -947,7 +955,7 @@ PGD int invert_kastaun(const double U[9], double prim[9], double g, const Geo &g
   const double Wmu_x = lorentz * mu * x;
   prim[RHO] = rho;
   prim[ENY] = eps;
-  prim[ENT] = (g - 1.) * eps * pgm::pow(rho, -g);
+  prim[ENT] = (g - 1.) * eps * PGD_POW(rho, -g);
 #pragma unroll
   for (int d = 0; d < 3; ++d) prim[UX1 + d] = Wmu_x * (Su[d] * inv_D + rbv * mu * (Bu[d] / sqrt_D));
   return 0;
@@ -965,7 +973,7 @@ struct HeatParams {
 PGD double heating_fraction(const HeatParams &p, double rho, double energy, double bsq,
                             double adv_electron) {
   const double tpr = (p.gamma_p - 1.0) * energy / rho;
-  const double tel = adv_electron * pgm::pow(rho, p.gamma_e - 1.0);
+  const double tel = adv_electron * PGD_POW(rho, p.gamma_e - 1.0);
   switch (p.model) {
     case 0:
       return p.fel_constant;
@@ -973,12 +981,12 @@ PGD double heating_fraction(const HeatParams &p, double rho, double energy, doub
       const double trat = tpr / tel;
       const double pres = rho * tpr;
       const double beta = kmin(2.0 * pres / bsq, 1.0e20);
-      const double log_trat = pgm::log(trat) / pgm::log(10.0);
+      const double log_trat = PGD_LOG(trat) / PGD_LOG(10.0);
       const double mbeta = 2.0 - 0.2 * log_trat;
       const double c2 = (trat <= 1.0) ? 1.6 / trat : 1.2 / trat;
       const double c3 = (trat <= 1.0) ? 18.0 + 5.0 * log_trat : 18.0;
-      const double bp = pgm::pow(beta, mbeta);
-      const double qrat = 0.92 * (c2 * c2 + bp) / (c3 * c3 + bp) * pgm::exp(-1.0 / beta) *
+      const double bp = PGD_POW(beta, mbeta);
+      const double qrat = 0.92 * (c2 * c2 + bp) / (c3 * c3 + bp) * PGD_EXP(-1.0 / beta) *
                           sqrt(1.67262171e-24 / 9.1093826e-28 * trat);
       return 1.0 / (1.0 + qrat);
     }
@@ -986,7 +994,7 @@ PGD double heating_fraction(const HeatParams &p, double rho, double energy, doub
       const double trat = tpr / tel;
       const double pres = rho * tpr;
       const double beta = kmin(2.0 * pres / bsq, 1.0e20);
-      const double qi_qe = 35.0 / (1.0 + pgm::pow(beta / 15.0, -1.4) * pgm::exp(-0.1 / trat));
+      const double qi_qe = 35.0 / (1.0 + PGD_POW(beta / 15.0, -1.4) * PGD_EXP(-0.1 / trat));
       return 1.0 / (1.0 + qi_qe);
     }
     case 3: {
@@ -999,7 +1007,7 @@ PGD double heating_fraction(const HeatParams &p, double rho, double energy, doub
       const double beta = 2.0 * pres / bsq;
       const double sigma = bsq / (rho + energy + pg);
       const double betamax = 0.25 / sigma;
-      return 0.5 * pgm::exp(-pgm::pow(1.0 - beta / betamax, 3.3) / (1.0 + 1.2 * pgm::pow(sigma, 0.7)));
+      return 0.5 * PGD_EXP(-PGD_POW(1.0 - beta / betamax, 3.3) / (1.0 + 1.2 * PGD_POW(sigma, 0.7)));
     }
     case 5: {
       const double trat_inv = tel / tpr;
@@ -1013,7 +1021,7 @@ PGD double heating_fraction(const HeatParams &p, double rho, double energy, doub
 PGD double heating_apply(const HeatParams &p, double rho, double energy, double bsq,
                          double adv_total, double rec_total, double adv_electron) {
   const double fel = heating_fraction(p, rho, energy, bsq, adv_electron);
-  const double rpow = pgm::pow(rho, p.gamma - p.gamma_e);
+  const double rpow = PGD_POW(rho, p.gamma - p.gamma_e);
   double diss = (p.gamma_e - 1.0) / (p.gamma - 1.0) * rpow * (rec_total - adv_total);
   if (p.suppress_highb_heat && (bsq / rho > 1.0)) diss = 0.0;
   if (p.enforce_positive_dissipation) diss = kmax(diss, 0.0);
@@ -1033,6 +1041,224 @@ PGD double clamp_by_ratio(double rmin, double rmax, double total, double electro
   const double hi = total / (1.0 + rmin);
   const double b = kmax(0.0, kmin(electron, total));
   return kmax(lo, kmin(b, hi));
+}
+
+// ---------------------------------------------------------------------------
+// Generic-precision forms of the face and heating physics, in the operation
+// order of the FP64 forms above. The mixed-precision engine instantiates them
+// with float for reconstruction, Riemann fluxes and electron heating.
+// ---------------------------------------------------------------------------
+PGD float tmin(float a, float b) { return fminf(a, b); }
+PGD float tmax(float a, float b) { return fmaxf(a, b); }
+PGD double tmin(double a, double b) { return fmin(a, b); }
+PGD double tmax(double a, double b) { return fmax(a, b); }
+PGD float tpow(float a, float b) { return powf(a, b); }
+PGD double tpow(double a, double b) { return pow(a, b); }
+PGD float texp(float a) { return expf(a); }
+PGD double texp(double a) { return exp(a); }
+PGD float tlog(float a) { return logf(a); }
+PGD double tlog(double a) { return log(a); }
+
+template <typename T>
+struct GeoT {
+  T gcov[4][4];
+  T gcon[4][4];
+  T gdet, sg, alpha;
+};
+
+template <typename T>
+struct StateT {
+  T ucon[4], ucov[4], bcon[4], bcov[4], bsq;
+};
+
+// Rounds an FP64 metric to T, keeping its structural zeros exact.
+template <int MT, typename T>
+PGD void geo_cast(const Geo &g, GeoT<T> &o) {
+  constexpr Pattern PT = metric_pattern(MT);
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      o.gcov[r][c] = PT.nz[r][c] ? (T)g.gcov[r][c] : T(0);
+      o.gcon[r][c] = PT.nz[r][c] ? (T)g.gcon[r][c] : T(0);
+    }
+  o.gdet = (T)g.gdet;
+  o.sg = (T)g.sg;
+  o.alpha = (T)g.alpha;
+}
+
+// state_calculation.h:19-69
+template <int MT, typename T>
+PGD void calc_state_t(const T P[NPRIM], const GeoT<T> &g, StateT<T> &s) {
+  constexpr Pattern PT = metric_pattern(MT);
+  const T alpha = g.alpha;
+  const T u[3] = {P[UX1], P[UX2], P[UX3]};
+  T sq = T(0);
+#pragma unroll
+  for (int i = 1; i < 4; ++i)
+#pragma unroll
+    for (int j = 1; j < 4; ++j)
+      if (PT.nz[i][j]) sq = sq + u[i - 1] * g.gcov[i][j] * u[j - 1];
+  const T lor = sqrt(T(1) + sq);
+  s.ucon[0] = lor / alpha;
+#pragma unroll
+  for (int i = 1; i < 4; ++i)
+    s.ucon[i] = PT.nz[0][i] ? u[i - 1] - s.ucon[0] * g.gcon[0][i] * alpha * alpha : u[i - 1];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    T v = T(0);
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+      if (PT.nz[r][c]) v += g.gcov[r][c] * s.ucon[c];
+    s.ucov[r] = v;
+  }
+  s.bcon[0] = P[BX1] * s.ucov[1] + P[BX2] * s.ucov[2] + P[BX3] * s.ucov[3];
+  const T iu0 = T(1) / s.ucon[0];
+  s.bcon[1] = (P[BX1] + s.bcon[0] * s.ucon[1]) * iu0;
+  s.bcon[2] = (P[BX2] + s.bcon[0] * s.ucon[2]) * iu0;
+  s.bcon[3] = (P[BX3] + s.bcon[0] * s.ucon[3]) * iu0;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    T v = T(0);
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+      if (PT.nz[r][c]) v += g.gcov[r][c] * s.bcon[c];
+    s.bcov[r] = v;
+  }
+  s.bsq = s.bcon[0] * s.bcov[0] + s.bcon[1] * s.bcov[1] + s.bcon[2] * s.bcov[2] +
+          s.bcon[3] * s.bcov[3];
+}
+
+// fast_magnetosonic_speed.h:11-81
+template <typename T>
+PGD void fast_speed_t(T gam, const T P[NPRIM], const GeoT<T> &g, const StateT<T> &s, int dir,
+                      T &vmax, T &vmin) {
+  const T hh = P[RHO] + gam * P[ENY];
+  const T h_tot = s.bsq + hh;
+  const T va_sq = s.bsq / h_tot;
+  const T cs_sq = gam * (gam - T(1)) * P[ENY] / hh;
+  T cf_sq = cs_sq + va_sq - cs_sq * va_sq;
+  if (cf_sq < T(0)) cf_sq = T(1e-10);
+  if (cf_sq > T(1)) cf_sq = T(1);
+  const T n_sq = g.gcon[dir][dir];
+  const T t_sq = g.gcon[0][0];
+  const T n_dot_u = s.ucon[dir];
+  const T t_dot_u = s.ucon[0];
+  const T n_dot_t = g.gcon[0][dir];
+  const T nu2 = n_dot_u * n_dot_u;
+  const T tu2 = t_dot_u * t_dot_u;
+  const T nutu = n_dot_u * t_dot_u;
+  const T A = tu2 - (t_sq + tu2) * cf_sq;
+  const T B = T(2) * (nutu - (n_dot_t + nutu) * cf_sq);
+  const T C = nu2 - (n_sq + nu2) * cf_sq;
+  T disc = B * B - T(4) * A * C;
+  if (disc < T(0)) disc = T(0);
+  disc = sqrt(disc);
+  const T i2a = T(1) / (T(2) * A);
+  const T vp = -(-B + disc) * i2a;
+  const T vm = -(-B - disc) * i2a;
+  vmax = vp > vm ? vp : vm;
+  vmin = vp > vm ? vm : vp;
+}
+
+// interpolater_mc.h:16-48
+template <typename T>
+PGD void mc_t(T qm1, T q, T qp1, T &ql_ip1, T &qr_i) {
+  const T a = T(2) * (q - qm1), b = T(0.5) * (qp1 - qm1), c = T(2) * (qp1 - q);
+  T slope = T(0);
+  if (a > T(0) && b > T(0) && c > T(0)) slope = tmin(tmin(a, b), c);
+  if (a < T(0) && b < T(0) && c < T(0)) slope = tmax(tmax(a, b), c);
+  ql_ip1 = q + T(0.5) * slope;
+  qr_i = q - T(0.5) * slope;
+}
+
+// interpolater_ppm4.h:29-67
+template <typename T>
+PGD void ppm4_t(T qm2, T qm1, T q, T qp1, T qp2, T &ql_ip1, T &qr_i) {
+  const T c12 = T(1) / T(12);
+  T qlv = (T(7) * (q + qm1) - (qm2 + qp1)) * c12;
+  T qrv = (T(7) * (q + qp1) - (qm1 + qp2)) * c12;
+  qlv = tmax(qlv, tmin(q, qm1));
+  qlv = tmin(qlv, tmax(q, qm1));
+  qrv = tmax(qrv, tmin(q, qp1));
+  qrv = tmin(qrv, tmax(q, qp1));
+  const T qc = qrv - q;
+  const T qd = qlv - q;
+  if ((qc * qd) >= T(0)) {
+    qlv = q;
+    qrv = q;
+  } else {
+    if (fabs(qc) >= T(2) * fabs(qd)) qrv = q - T(2) * qd;
+    if (fabs(qd) >= T(2) * fabs(qc)) qlv = q - T(2) * qc;
+  }
+  ql_ip1 = qrv;
+  qr_i = qlv;
+}
+
+// heating_model.h:53-179
+template <typename T>
+PGD T heating_fraction_t(const HeatParams &p, T rho, T energy, T bsq, T adv_electron) {
+  const T tpr = (T(p.gamma_p) - T(1)) * energy / rho;
+  const T tel = adv_electron * tpow(rho, T(p.gamma_e) - T(1));
+  switch (p.model) {
+    case 0:
+      return T(p.fel_constant);
+    case 1: {
+      const T trat = tpr / tel;
+      const T beta = tmin(T(2) * rho * tpr / bsq, T(1.0e20));
+      const T log_trat = tlog(trat) / tlog(T(10));
+      const T mbeta = T(2) - T(0.2) * log_trat;
+      const T c2 = (trat <= T(1)) ? T(1.6) / trat : T(1.2) / trat;
+      const T c3 = (trat <= T(1)) ? T(18) + T(5) * log_trat : T(18);
+      const T bp = tpow(beta, mbeta);
+      const T qrat = T(0.92) * (c2 * c2 + bp) / (c3 * c3 + bp) * texp(T(-1) / beta) *
+                     sqrt(T(1.67262171e-24 / 9.1093826e-28) * trat);
+      return T(1) / (T(1) + qrat);
+    }
+    case 2: {
+      const T trat = tpr / tel;
+      const T beta = tmin(T(2) * rho * tpr / bsq, T(1.0e20));
+      const T qi_qe = T(35) / (T(1) + tpow(beta / T(15), T(-1.4)) * texp(T(-0.1) / trat));
+      return T(1) / (T(1) + qi_qe);
+    }
+    case 3: {
+      const T sigma = bsq / rho;
+      return T(0.25) * (T(1) + sqrt((sigma / T(5)) / (T(2) + sigma / T(5))));
+    }
+    case 4: {
+      const T pres = (T(p.gamma_p) - T(1)) * energy;
+      const T pg = (T(p.gamma) - T(1)) * energy;
+      const T beta = T(2) * pres / bsq;
+      const T sigma = bsq / (rho + energy + pg);
+      const T betamax = T(0.25) / sigma;
+      return T(0.5) * texp(-tpow(T(1) - beta / betamax, T(3.3)) /
+                           (T(1) + T(1.2) * tpow(sigma, T(0.7))));
+    }
+    case 5: {
+      const T qe_qi = T(0.33) * sqrt(tel / tpr);
+      return T(1) / (T(1) + T(1) / qe_qi);
+    }
+  }
+  return T(p.fel_constant);
+}
+
+template <typename T>
+PGD T heating_apply_t(const HeatParams &p, T rho, T energy, T bsq, T adv_total, T rec_total,
+                      T adv_electron) {
+  const T fel = heating_fraction_t<T>(p, rho, energy, bsq, adv_electron);
+  const T gam = T(p.gamma), ge = T(p.gamma_e), gp = T(p.gamma_p);
+  const T rpow = tpow(rho, gam - ge);
+  T diss = (ge - T(1)) / (gam - T(1)) * rpow * (rec_total - adv_total);
+  if (p.suppress_highb_heat && (bsq / rho > T(1))) diss = T(0);
+  if (p.enforce_positive_dissipation) diss = diss < T(0) ? T(0) : diss;
+  const T kel = adv_electron + fel * diss;
+  if (!p.limit_kel && p.model == 0) return kel;
+  const T kel_max = adv_total * rpow /
+                    (T(p.ratio_min) * (gam - T(1)) / (gp - T(1)) + (gam - T(1)) / (ge - T(1)));
+  const T kel_min = adv_total * rpow /
+                    (T(p.ratio_max) * (gam - T(1)) / (gp - T(1)) + (gam - T(1)) / (ge - T(1)));
+  const T lo = kel < kel_max ? kel : kel_max;
+  return kel_min < lo ? lo : kel_min;
 }
 
 }  // namespace pgd

@@ -1,0 +1,410 @@
+// serve.cu -- continuous-batching request loop over block pools (host code).
+//
+// A server holds one block pool (pangu_pool_create) per job class -- one
+// parameter set and block shape -- with its containers, dt arrays, CUDA
+// stream and captured RK2-cycle graph, all allocated at class creation
+// against the server's HBM budget. Submitted jobs wait until their arrival
+// time; a job is admitted as soon as its class pool has a free job id and
+// enough free block slots (first fit in arrival order) and then runs one RK2
+// cycle per tick of its class together with every other admitted job of the
+// class (one graph launch per tick). Classes tick independently, each on its
+// own stream, so their kernels overlap and a class of small jobs is not held
+// to the pace of a class of large ones. A job is copied out and detached
+// after its last cycle. Latency = completion - arrival, on the host clock.
+//
+// No counterpart in the reference, which runs one mesh per process.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <new>
+#include <thread>
+#include <vector>
+
+#include "pangu_b200.h"
+
+namespace {
+
+struct Arena {
+  pangu_pack base{}, one{};
+  double *dt = nullptr, *dt_est = nullptr;
+  std::vector<void *> allocs;
+};
+
+struct SClass {
+  pangu_params p{};
+  pangu_mesh block{};
+  int capacity = 0, max_jobs = 0, nf = 0;
+  long long ncell = 0, interior = 0;  // cells per block (entire, interior)
+  size_t prim_bytes = 8;
+  double dt_factor = 2.0;
+  pangu_engine *e = nullptr;
+  Arena a;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t tick_done = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  bool dirty = true, inflight = false;
+  int running = 0;
+};
+
+struct SJob {
+  int cls = 0;
+  pangu_mesh mesh{};
+  double a = 0, h = 0, dt_init = 0, arrival = 0;
+  long long cycles = 0, done_cycles = 0;
+  std::vector<double> prim;  // initial state, then the result
+  int state = 0;             // 0 waiting, 1 running, 2 done
+  int job = -1;
+  std::vector<int32_t> slots;
+  double t_admit = 0, t_done = 0;
+  uint64_t counters[PANGU_NCOUNTERS] = {};
+};
+
+double now_s(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+}  // namespace
+
+struct pangu_server {
+  uint64_t budget = 0, used = 0;
+  std::vector<SClass> classes;
+  std::vector<SJob> jobs;
+  pangu_server_stats stats{};
+};
+
+namespace {
+
+template <class T>
+int salloc(pangu_server *s, Arena &a, T **p, size_t n) {
+  const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+  if (s->used + bytes > s->budget) return PANGU_ENOMEM;
+  if (cudaMalloc((void **)p, bytes) != cudaSuccess) return PANGU_ENOMEM;
+  a.allocs.push_back(*p);
+  s->used += bytes;
+  if (cudaMemset(*p, 0, bytes) != cudaSuccess) return PANGU_ECUDA;
+  return PANGU_OK;
+}
+
+void free_class(SClass &c) {
+  if (c.graph) cudaGraphExecDestroy(c.graph);
+  if (c.e) pangu_engine_destroy(c.e);
+  for (void *p : c.a.allocs) cudaFree(p);
+  if (c.tick_done) cudaEventDestroy(c.tick_done);
+  if (c.stream) cudaStreamDestroy(c.stream);
+  c = SClass{};
+}
+
+// Captures one RK2 cycle of the class pool (both stages and the dt policy).
+int capture(SClass &c) {
+  if (c.graph) {
+    cudaGraphExecDestroy(c.graph);
+    c.graph = nullptr;
+  }
+  if (cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    return PANGU_ECUDA;
+  int rc = pangu_stage(c.e, 1, &c.a.base, &c.a.one, 0.5, c.a.dt, nullptr, c.stream);
+  if (!rc) rc = pangu_stage(c.e, 2, &c.a.base, &c.a.one, 1.0, c.a.dt, c.a.dt_est, c.stream);
+  if (!rc) rc = pangu_update_dt(c.e, c.a.dt, c.a.dt_est, c.dt_factor, c.stream);
+  cudaGraph_t g = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(c.stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (ec != cudaSuccess) return PANGU_ECUDA;
+  const cudaError_t ei = cudaGraphInstantiate(&c.graph, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) return PANGU_ECUDA;
+  c.dirty = false;
+  return PANGU_OK;
+}
+
+// Places a job in its class pool and uploads its initial state. Needs the
+// class idle (no cycle in flight).
+int admit(SClass &c, SJob &j) {
+  const long long nb = (long long)j.mesh.nbx1 * j.mesh.nbx2 * j.mesh.nbx3;
+  j.slots.assign(nb, -1);
+  int32_t job = -1;
+  int rc = pangu_job_attach(c.e, &j.mesh, j.a, j.h, &job, j.slots.data());
+  if (rc) return rc;
+  j.job = job;
+  // uploads are ordered on the class stream before the job's first kernels;
+  // a pageable source is consumed before cudaMemcpyAsync returns
+  const size_t blk = (size_t)c.nf * c.ncell;
+  std::vector<float> tmp;
+  for (long long b = 0; b < nb; ++b) {
+    const int sl = j.slots[b];
+    const double *src = j.prim.data() + b * blk;
+    char *dst = (char *)c.a.base.prim + (size_t)sl * blk * c.prim_bytes;
+    cudaError_t ec;
+    if (c.prim_bytes == 4) {
+      tmp.assign(src, src + blk);
+      ec = cudaMemcpyAsync(dst, tmp.data(), blk * 4, cudaMemcpyHostToDevice, c.stream);
+    } else {
+      ec = cudaMemcpyAsync(dst, src, blk * 8, cudaMemcpyHostToDevice, c.stream);
+    }
+    if (ec != cudaSuccess ||
+        cudaMemsetAsync(c.a.base.cons + (size_t)sl * blk, 0, blk * 8, c.stream) != cudaSuccess ||
+        cudaMemsetAsync(c.a.base.flag + (size_t)sl * c.ncell, 0, c.ncell * 8, c.stream) !=
+            cudaSuccess)
+      return PANGU_ECUDA;
+  }
+  if (cudaMemcpyAsync(c.a.dt + job, &j.dt_init, 8, cudaMemcpyHostToDevice, c.stream) !=
+      cudaSuccess)
+    return PANGU_ECUDA;
+  rc = pangu_job_start(c.e, job, &c.a.base, &c.a.one, c.stream);
+  if (rc) return rc;
+  c.dirty = true;
+  ++c.running;
+  return PANGU_OK;
+}
+
+// Copies a finished job's primitives and counters back and detaches it.
+// Needs the class idle.
+int retire(SClass &c, SJob &j) {
+  const size_t blk = (size_t)c.nf * c.ncell;
+  std::vector<float> tmp(c.prim_bytes == 4 ? blk : 0);
+  for (size_t b = 0; b < j.slots.size(); ++b) {
+    const char *src = (const char *)c.a.base.prim + (size_t)j.slots[b] * blk * c.prim_bytes;
+    double *dst = j.prim.data() + b * blk;
+    if (c.prim_bytes == 4) {
+      if (cudaMemcpy(tmp.data(), src, blk * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return PANGU_ECUDA;
+      for (size_t q = 0; q < blk; ++q) dst[q] = tmp[q];
+    } else if (cudaMemcpy(dst, src, blk * 8, cudaMemcpyDeviceToHost) != cudaSuccess) {
+      return PANGU_ECUDA;
+    }
+  }
+  int rc = pangu_job_counters(c.e, j.job, j.counters);
+  if (!rc) rc = pangu_job_detach(c.e, j.job);
+  if (rc) return rc;
+  c.dirty = true;
+  --c.running;
+  return PANGU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pangu_server_create(uint64_t hbm_budget_bytes, pangu_server **out) {
+  if (!out || hbm_budget_bytes == 0) return PANGU_EINVAL;
+  *out = new (std::nothrow) pangu_server;
+  if (!*out) return PANGU_ENOMEM;
+  (*out)->budget = hbm_budget_bytes;
+  return PANGU_OK;
+}
+
+int pangu_server_destroy(pangu_server *s) {
+  if (!s) return PANGU_EINVAL;
+  for (SClass &c : s->classes)
+    if (c.stream) cudaStreamSynchronize(c.stream);
+  for (SClass &c : s->classes) free_class(c);
+  delete s;
+  return PANGU_OK;
+}
+
+int pangu_server_add_class(pangu_server *s, const pangu_params *params, const pangu_mesh *block,
+                           int32_t capacity_blocks, int32_t max_jobs, double dt_factor,
+                           int32_t *class_out) {
+  if (!s || !params || !block || !class_out || capacity_blocks < 1 || max_jobs < 1)
+    return PANGU_EINVAL;
+  SClass c;
+  c.p = *params;
+  c.block = *block;
+  c.capacity = capacity_blocks;
+  c.max_jobs = max_jobs;
+  c.dt_factor = dt_factor;
+  c.nf = pangu_num_fields(params);
+  c.prim_bytes = params->precision == PANGU_PRECISION_MIXED ? 4 : 8;
+  const int act[3] = {block->nx1 > 1, block->nx2 > 1, block->nx3 > 1};
+  const int nx[3] = {block->nx1, block->nx2, block->nx3};
+  c.ncell = 1;
+  c.interior = 1;
+  for (int d = 0; d < 3; ++d) {
+    c.ncell *= nx[d] + 2 * block->ng * act[d];
+    c.interior *= nx[d];
+  }
+  const uint64_t used0 = s->used;
+  int rc = pangu_pool_create(params, block, capacity_blocks, max_jobs, &c.e);
+  const size_t nv = (size_t)capacity_blocks * c.nf * c.ncell;
+  const size_t na = (size_t)capacity_blocks * 3 * c.ncell;
+  Arena &a = c.a;
+  double *alfven = nullptr, *efield = nullptr, *flag = nullptr;
+  if (!rc) rc = salloc(s, a, &alfven, na);
+  if (!rc) rc = salloc(s, a, &efield, na);
+  if (!rc) rc = salloc(s, a, &flag, (size_t)capacity_blocks * c.ncell);
+  pangu_pack *packs[2] = {&a.base, &a.one};
+  for (pangu_pack *pk : packs) {
+    if (rc) break;
+    if (c.prim_bytes == 4) {
+      float *pf = nullptr;
+      rc = salloc(s, a, &pf, nv);
+      pk->prim = reinterpret_cast<double *>(pf);
+    } else {
+      rc = salloc(s, a, &pk->prim, nv);
+    }
+    if (!rc) rc = salloc(s, a, &pk->cons, nv);
+    if (!rc) rc = salloc(s, a, &pk->flux1, nv);
+    if (!rc && act[1]) rc = salloc(s, a, &pk->flux2, nv);
+    if (!rc && act[2]) rc = salloc(s, a, &pk->flux3, nv);
+    pk->alfven = alfven;
+    pk->efield = efield;
+    pk->flag = flag;
+  }
+  if (!rc) rc = salloc(s, a, &a.dt, max_jobs);
+  if (!rc) rc = salloc(s, a, &a.dt_est, max_jobs);
+  if (!rc && cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess)
+    rc = PANGU_ECUDA;
+  if (!rc && cudaEventCreateWithFlags(&c.tick_done, cudaEventDisableTiming) != cudaSuccess)
+    rc = PANGU_ECUDA;
+  if (rc) {
+    free_class(c);
+    s->used = used0;
+    return rc;
+  }
+  *class_out = (int32_t)s->classes.size();
+  s->classes.push_back(c);
+  return PANGU_OK;
+}
+
+int pangu_server_submit(pangu_server *s, int32_t cls, const pangu_mesh *mesh, double a, double h,
+                        double dt_init, int64_t cycles, double arrival_s, const double *prim_host,
+                        int32_t *ticket_out) {
+  if (!s || !mesh || !prim_host || !ticket_out || cls < 0 || cls >= (int)s->classes.size() ||
+      cycles < 1)
+    return PANGU_EINVAL;
+  const SClass &c = s->classes[cls];
+  if (mesh->nx1 != c.block.nx1 || mesh->nx2 != c.block.nx2 || mesh->nx3 != c.block.nx3 ||
+      mesh->ng != c.block.ng)
+    return PANGU_EINVAL;
+  const long long nb = (long long)mesh->nbx1 * mesh->nbx2 * mesh->nbx3;
+  if (nb < 1 || nb > c.capacity) return PANGU_ETOOBIG;
+  SJob j;
+  j.cls = cls;
+  j.mesh = *mesh;
+  j.a = a;
+  j.h = h;
+  j.dt_init = dt_init;
+  j.cycles = cycles;
+  j.arrival = arrival_s;
+  j.prim.assign(prim_host, prim_host + (size_t)nb * c.nf * c.ncell);
+  *ticket_out = (int32_t)s->jobs.size();
+  s->jobs.push_back(std::move(j));
+  return PANGU_OK;
+}
+
+int pangu_server_run(pangu_server *s) {
+  if (!s) return PANGU_EINVAL;
+  std::vector<int> order(s->jobs.size());
+  for (size_t q = 0; q < order.size(); ++q) order[q] = (int)q;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return s->jobs[x].arrival < s->jobs[y].arrival; });
+  size_t done = 0;
+  for (const SJob &j : s->jobs) done += j.state == 2;
+  pangu_server_stats &st = s->stats;
+  st = pangu_server_stats{};
+  const auto t0 = std::chrono::steady_clock::now();
+  int rc = PANGU_OK;
+  // Every class advances on its own: when its previous cycle has finished,
+  // the cycle is credited to its running jobs, finished jobs are copied out
+  // and detached, arrived jobs admitted, and the next cycle launched.
+  while (done < s->jobs.size()) {
+    bool busy = false;
+    for (int ci = 0; ci < (int)s->classes.size(); ++ci) {
+      SClass &c = s->classes[ci];
+      if (c.inflight) {
+        const cudaError_t q = cudaEventQuery(c.tick_done);
+        if (q == cudaErrorNotReady) {
+          busy = true;
+          continue;
+        }
+        if (q != cudaSuccess) return PANGU_ECUDA;
+        c.inflight = false;
+        ++st.ticks;
+        for (SJob &j : s->jobs) {
+          if (j.state != 1 || j.cls != ci) continue;
+          ++j.done_cycles;
+          st.zone_cycles += (double)c.interior * j.slots.size();
+          if (j.done_cycles < j.cycles) continue;
+          if ((rc = retire(c, j))) return rc;
+          j.state = 2;
+          j.t_done = now_s(t0);
+          ++done;
+        }
+      }
+      const double t = now_s(t0);
+      for (int q : order) {  // first fit in arrival order
+        SJob &j = s->jobs[q];
+        if (j.cls != ci || j.state != 0 || j.arrival > t) continue;
+        rc = admit(c, j);
+        if (rc == PANGU_EFULL) continue;
+        if (rc) return rc;
+        j.state = 1;
+        j.t_admit = now_s(t0);
+      }
+      if (!c.running) continue;
+      if (c.dirty && (rc = capture(c))) return rc;
+      if (cudaGraphLaunch(c.graph, c.stream) != cudaSuccess ||
+          cudaEventRecord(c.tick_done, c.stream) != cudaSuccess)
+        return PANGU_ECUDA;
+      c.inflight = true;
+      busy = true;
+    }
+    if (!busy && done < s->jobs.size()) {
+      // nothing on the device: sleep until the next arrival
+      const double t = now_s(t0);
+      double next = -1;
+      for (int q : order)
+        if (s->jobs[q].state == 0) {
+          next = s->jobs[q].arrival;
+          break;
+        }
+      if (next > t) std::this_thread::sleep_for(std::chrono::duration<double>(next - t));
+    }
+  }
+  st.wall_s = now_s(t0);
+  std::vector<double> lat;
+  for (const SJob &j : s->jobs) lat.push_back(j.t_done - j.arrival);
+  std::sort(lat.begin(), lat.end());
+  if (!lat.empty()) {
+    auto pct = [&](double f) {
+      const double pos = f * (lat.size() - 1);
+      const size_t lo = (size_t)pos;
+      const size_t hi = std::min(lo + 1, lat.size() - 1);
+      return lat[lo] + (pos - lo) * (lat[hi] - lat[lo]);
+    };
+    st.p50_s = pct(0.50);
+    st.p99_s = pct(0.99);
+  }
+  st.jobs = (int64_t)s->jobs.size();
+  st.zone_cycles_per_s = st.wall_s > 0 ? st.zone_cycles / st.wall_s : 0;
+  st.hbm_bytes = s->used;
+  return PANGU_OK;
+}
+
+int pangu_server_result(pangu_server *s, int32_t ticket, double *prim_out, double *times_out,
+                        uint64_t counters_out[PANGU_NCOUNTERS]) {
+  if (!s || ticket < 0 || ticket >= (int)s->jobs.size()) return PANGU_EINVAL;
+  const SJob &j = s->jobs[ticket];
+  if (j.state != 2) return PANGU_EINVAL;
+  if (prim_out) std::memcpy(prim_out, j.prim.data(), j.prim.size() * 8);
+  if (times_out) {
+    times_out[0] = j.arrival;
+    times_out[1] = j.t_admit;
+    times_out[2] = j.t_done;
+  }
+  if (counters_out)
+    for (int q = 0; q < PANGU_NCOUNTERS; ++q) counters_out[q] = j.counters[q];
+  return PANGU_OK;
+}
+
+int pangu_server_get_stats(const pangu_server *s, pangu_server_stats *out) {
+  if (!s || !out) return PANGU_EINVAL;
+  *out = s->stats;
+  return PANGU_OK;
+}
+
+}  // extern "C"

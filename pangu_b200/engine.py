@@ -13,7 +13,8 @@ import os
 import numpy as np
 
 from . import abi
-from .params import ParameterInput, mesh_struct, params_struct, process_packages
+from .params import (ParameterInput, engine_precision, mesh_struct, params_struct,
+                     process_packages)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _lib = None
@@ -78,6 +79,17 @@ def lib():
     L.pangu_job_detach.argtypes = [_P, C.c_int32]
     L.pangu_job_counters.argtypes = [_P, C.c_int32, C.POINTER(C.c_uint64)]
     L.pangu_active_blocks.argtypes = [_P]
+    L.pangu_server_create.argtypes = [C.c_uint64, C.POINTER(_P)]
+    L.pangu_server_destroy.argtypes = [_P]
+    L.pangu_server_add_class.argtypes = [_P, C.POINTER(abi.Params), C.POINTER(abi.Mesh), C.c_int32,
+                                         C.c_int32, C.c_double, C.POINTER(C.c_int32)]
+    L.pangu_server_submit.argtypes = [_P, C.c_int32, C.POINTER(abi.Mesh), C.c_double, C.c_double,
+                                      C.c_double, C.c_int64, C.c_double, C.c_void_p,
+                                      C.POINTER(C.c_int32)]
+    L.pangu_server_run.argtypes = [_P]
+    L.pangu_server_result.argtypes = [_P, C.c_int32, C.c_void_p, C.c_void_p,
+                                      C.POINTER(C.c_uint64)]
+    L.pangu_server_get_stats.argtypes = [_P, C.POINTER(abi.ServerStats)]
     _lib = L
     return L
 
@@ -97,11 +109,13 @@ class DeviceContainer:
 
     FIELDS = ("prim", "cons", "flux1", "flux2", "flux3", "alfven", "efield", "flag")
 
-    def __init__(self, nb, nf, shape, device, shared=None):
+    def __init__(self, nb, nf, shape, device, shared=None, mixed=False):
         torch = _torch()
         n3, n2, n1 = shape
         z = lambda *s: torch.zeros(s, dtype=torch.float64, device=device)  # noqa: E731
-        self.prim = z(nb, nf, n3, n2, n1)
+        # the mixed-precision form stores the primitives in FP32
+        self.prim = torch.zeros((nb, nf, n3, n2, n1), device=device,
+                                dtype=torch.float32 if mixed else torch.float64)
         self.cons = z(nb, nf, n3, n2, n1)
         self.flux1 = z(nb, nf, n3, n2, n1)
         self.flux2 = z(nb, nf, n3, n2, n1)
@@ -161,9 +175,14 @@ class Engine:
         import torch
         return _P(torch.cuda.current_stream(self.device).cuda_stream)
 
+    @property
+    def mixed(self) -> bool:
+        return self.params.precision == abi.PRECISION["mixed"]
+
     def new_containers(self):
-        base = DeviceContainer(self.nb, self.nf, self.shape, self.device)
-        one = DeviceContainer(self.nb, self.nf, self.shape, self.device, shared=base)
+        base = DeviceContainer(self.nb, self.nf, self.shape, self.device, mixed=self.mixed)
+        one = DeviceContainer(self.nb, self.nf, self.shape, self.device, shared=base,
+                              mixed=self.mixed)
         return base, one
 
     # ---- per-task entry points ------------------------------------------
@@ -255,6 +274,7 @@ class Simulation:
         self.pin = pin
         self.packages = process_packages(pin)
         self.params = params_struct(self.packages)
+        self.params.precision = engine_precision(pin)
         self.mesh = mesh_struct(pin)
         self.engine = Engine(self.params, self.mesh, device)
         self.base, self.one = self.engine.new_containers()
@@ -271,11 +291,9 @@ class Simulation:
         exchange then physical BCs, as Parthenon does after the problem
         generator). Container "1" starts as a copy of "base"."""
         torch = _torch()
-        self.base.prim.copy_(torch.as_tensor(prim, device=self.engine.device))
-        self.engine.exchange_ghosts(self.base)
-        self.engine.apply_boundary_conditions(self.base)
-        self.one.prim.copy_(self.base.prim)
-        self.one.cons.copy_(self.base.cons)
+        src = torch.as_tensor(prim, device=self.engine.device)
+        self.base.prim.copy_(src.to(self.base.prim.dtype))
+        self.engine.job_start(0, self.base, self.one)
 
     def stage(self, st: int, dt_est=None):
         self.engine.stage(st, self.base, self.one, RK2_BETA[st % 2], self.dt, dt_est)
@@ -309,7 +327,7 @@ class Simulation:
         self.cycle += 1
 
     def primitives(self) -> np.ndarray:
-        return self.base.prim.cpu().numpy()
+        return self.base.prim.double().cpu().numpy()
 
 
 class Pool:
@@ -328,6 +346,7 @@ class Pool:
     def __init__(self, template: ParameterInput, capacity_blocks: int, max_jobs: int, device=0):
         torch = _torch()
         self.params = params_struct(process_packages(template))
+        self.params.precision = engine_precision(template)
         block = mesh_struct(template)
         block.nbx1 = block.nbx2 = block.nbx3 = 1
         self.engine = Engine(self.params, block, device, pool=(capacity_blocks, max_jobs))
@@ -355,11 +374,13 @@ class Pool:
         numpy or a device tensor), fills its ghosts and sets dt[job] = dt_init."""
         torch = _torch()
         p = params_struct(process_packages(pin))
+        p.precision = engine_precision(pin)
         self._check_compatible(p)
         mesh = mesh_struct(pin)
+        torch.cuda.synchronize(self.engine.device)  # no pool work in flight
         job, slots = self.engine.attach(mesh, p.a, p.h)
         idx = torch.tensor(slots, dtype=torch.long, device=self.engine.device)
-        src = torch.as_tensor(prim, device=self.engine.device, dtype=torch.float64)
+        src = torch.as_tensor(prim, device=self.engine.device).to(self.base.prim.dtype)
         self.base.prim.index_copy_(0, idx, src)
         self.base.cons.index_fill_(0, idx, 0.0)
         self.base.flag.index_fill_(0, idx, 0.0)
@@ -372,11 +393,12 @@ class Pool:
     def primitives(self, job) -> np.ndarray:
         torch = _torch()
         idx = torch.tensor(self.jobs[job], dtype=torch.long, device=self.engine.device)
-        return self.base.prim.index_select(0, idx).cpu().numpy()
+        return self.base.prim.index_select(0, idx).double().cpu().numpy()
 
     def detach(self, job) -> np.ndarray:
         """Detaches a job and returns its primitives."""
         out = self.primitives(job)
+        _torch().cuda.synchronize(self.engine.device)  # no pool work in flight
         self.engine.detach(job)
         del self.jobs[job]
         self._graph = None
@@ -405,3 +427,92 @@ class Pool:
             torch.cuda.current_stream(self.engine.device).wait_stream(s)
             self._graph = g
         self._graph.replay()
+
+
+class Server:
+    """Continuous-batching request loop (pangu_server_*): one block pool per job
+    class, jobs admitted at their arrival time as slots free up, every class
+    stepped on its own stream, results copied back at completion."""
+
+    def __init__(self, hbm_budget_bytes: int, device=0):
+        torch = _torch()
+        self.device = torch.device("cuda", device)
+        self.L = lib()
+        h = _P()
+        with torch.cuda.device(self.device):
+            _check(self.L.pangu_server_create(int(hbm_budget_bytes), C.byref(h)),
+                   "pangu_server_create")
+        self.h = h
+        self.classes = []   # (params, block mesh, nf, block shape)
+        self.tickets = {}   # ticket -> (class, nblocks)
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.L.pangu_server_destroy(self.h)
+            self.h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_class(self, template: ParameterInput, capacity_blocks: int, max_jobs: int) -> int:
+        params = params_struct(process_packages(template))
+        params.precision = engine_precision(template)
+        block = mesh_struct(template)
+        block.nbx1 = block.nbx2 = block.nbx3 = 1
+        factor = template.get_or_add_real("parthenon/time", "dt_factor", 2.0)
+        out = C.c_int32()
+        _check(self.L.pangu_server_add_class(self.h, C.byref(params), C.byref(block),
+                                             int(capacity_blocks), int(max_jobs), factor,
+                                             C.byref(out)), "pangu_server_add_class")
+        nf = self.L.pangu_num_fields(C.byref(params))
+        act = [block.nx1 > 1, block.nx2 > 1, block.nx3 > 1]
+        n = [block.nx1, block.nx2, block.nx3]
+        shape = tuple(n[d] + 2 * block.ng * act[d] for d in (2, 1, 0))
+        self.classes.append((params, block, nf, shape))
+        return out.value
+
+    def submit(self, cls: int, pin: ParameterInput, prim: np.ndarray, cycles: int,
+               arrival_s: float) -> int:
+        params, _, nf, shape = self.classes[cls]
+        p = params_struct(process_packages(pin))
+        p.precision = engine_precision(pin)
+        for name, _ in abi.Params._fields_:
+            if name not in Pool.PER_JOB and getattr(p, name) != getattr(params, name):
+                raise EngineError(f"job parameter {name} differs from the class's")
+        mesh = mesh_struct(pin)
+        arr = np.ascontiguousarray(prim, dtype=np.float64)
+        dt_init = pin.get_or_add_real("parthenon/time", "dt_init", 1e-5)
+        t = C.c_int32()
+        _check(self.L.pangu_server_submit(self.h, cls, C.byref(mesh), p.a, p.h, dt_init,
+                                          int(cycles), float(arrival_s),
+                                          arr.ctypes.data_as(C.c_void_p), C.byref(t)),
+               "pangu_server_submit")
+        self.tickets[t.value] = (cls, arr.shape[0])
+        return t.value
+
+    def run(self):
+        torch = _torch()
+        torch.cuda.synchronize(self.device)
+        with torch.cuda.device(self.device):
+            _check(self.L.pangu_server_run(self.h), "pangu_server_run")
+
+    def result(self, ticket: int):
+        """(primitives [block][var][k][j][i] FP64, (arrival, admission,
+        completion) seconds, counters) of a finished job."""
+        cls, nb = self.tickets[ticket]
+        _, _, nf, shape = self.classes[cls]
+        out = np.empty((nb, nf) + shape, dtype=np.float64)
+        times = np.empty(3, dtype=np.float64)
+        cnt = (C.c_uint64 * abi.NCOUNTERS)()
+        _check(self.L.pangu_server_result(self.h, ticket, out.ctypes.data_as(C.c_void_p),
+                                          times.ctypes.data_as(C.c_void_p), cnt),
+               "pangu_server_result")
+        return out, times, np.array(list(cnt), dtype=np.uint64)
+
+    def stats(self) -> dict:
+        st = abi.ServerStats()
+        _check(self.L.pangu_server_get_stats(self.h, C.byref(st)), "pangu_server_get_stats")
+        return {name: getattr(st, name) for name, _ in abi.ServerStats._fields_}

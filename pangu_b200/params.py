@@ -221,6 +221,15 @@ def params_struct(packages: dict[str, StateDescriptor]) -> abi.Params:
     return p
 
 
+def engine_precision(pin: ParameterInput) -> int:
+    """<b200>/precision = fp64 (default) | mixed: the engine's arithmetic. Not a
+    reference key; the reference is FP64 throughout."""
+    name = pin.get_or_add_string("b200", "precision", "fp64")
+    if name not in abi.PRECISION:
+        raise ValueError("Unknown precision: " + name)
+    return abi.PRECISION[name]
+
+
 def mesh_struct(pin: ParameterInput) -> abi.Mesh:
     """<parthenon/mesh> + <parthenon/meshblock> into the C-ABI mesh struct.
 

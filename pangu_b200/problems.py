@@ -138,14 +138,14 @@ def orszag_tang(geo: Geometry, packages) -> np.ndarray:
 # ---------------------------------------------------------------------------
 # Brio-Wu
 # ---------------------------------------------------------------------------
-def brio_wu_input(n: int = 1024) -> ParameterInput:
+def brio_wu_input(n: int = 1024, nblock: int | None = None) -> ParameterInput:
     pin = ParameterInput()
     for k, v in dict(nx1=n, x1min=-0.5, x1max=0.5, ix1_bc="outflow", ox1_bc="outflow",
                      nx2=1, x2min=-0.5, x2max=0.5, ix2_bc="periodic", ox2_bc="periodic",
                      nx3=1, x3min=-0.5, x3max=0.5, ix3_bc="periodic", ox3_bc="periodic",
                      nghost=2).items():
         pin.set("parthenon/mesh", k, v)
-    for k, v in dict(nx1=n, nx2=1, nx3=1).items():
+    for k, v in dict(nx1=nblock or n, nx2=1, nx3=1).items():
         pin.set("parthenon/meshblock", k, v)
     for k, v in dict(cfl_number=0.4, adiabatic_index=2.0, riemann_solver="hll",
                      limiter="mc", recovery="chainer", enable_B=True,
