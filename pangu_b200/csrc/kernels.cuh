@@ -1098,29 +1098,19 @@ __device__ __forceinline__ void c2p_write(const Dims &d, PT *P, int b, int k, in
 // where Scheme2D fails are appended to `retry` (their primitives are left
 // untouched) and finished by k_recovery_retry, so the long 1Dvsq/1D Newton
 // loops of a few cells do not hold whole warps of converged cells.
-//
-// With fuse != 0 the kernel runs the stage's AddGeometricSource -> Recovery
-// -> ApplyElectronHeating sequence on its cell (ideal_grmhd.cc:80-90): the
-// source is added to the cell's conserved variables first and heating is
-// applied once the cell's primitives are final (here, or in the retry pass),
-// each step reading what the previous one wrote, so the result is that of
-// the three separate tasks. The cell's metric is loaded once for all three.
+// (Folding the geometric source and electron heating into this kernel was
+// measured slower: their registers cut the occupancy of the Newton loops.)
 template <int MT>
 __global__ void __launch_bounds__(kThreads, 3) k_recovery(Dims d, pangu_params p, PT *P,
-                                                       double *U, double *flag,
+                                                       const double *U, double *flag,
                                                        unsigned long long *cnt, int *nretry,
-                                                       long long *retry, int fuse, double beta,
-                                                       const double *dt) {
+                                                       long long *retry) {
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
   b = slot_of(d, b);
   const bool robuster = p.recovery == PANGU_RECOVERY_ROBUSTER;
-  const bool heat = fuse && p.enable_heating;
   const long long fc = cidx(d, b, k, j, i);
-  Geo g;
-  cell_metric<MT>(d, p, b, k, j, i, g);
-  if (fuse) source_cell<MT>(d, p, P, U, b, k, j, i, g, beta * dt[job_of(d, b)]);
   if (MT == CKS) {
     const double x = xc(d, b, 0, i), y = xc(d, b, 1, j), z = xc(d, b, 2, k);
     const double a2 = p.a * p.a;
@@ -1130,20 +1120,18 @@ __global__ void __launch_bounds__(kThreads, 3) k_recovery(Dims d, pangu_params p
     count(cnt, job_of(d, b), PANGU_CNT_EXCISED, exc);
     if (exc) {
       if (!robuster) flag[fc] = 0;
-      if (heat) heat_cell<MT>(d, p, P, U, b, k, j, i, g);
       return;
     }
   }
+  Geo g;
+  cell_metric<MT>(d, p, b, k, j, i, g);
   double UH[9], PH[9];
   c2p_inputs<MT>(d, p, P, U, b, k, j, i, g, UH, PH, true);
   const double gam = p.adiabatic_index;
   if (robuster) {
     const int st = invert_kastaun(UH, PH, gam, g);
     count(cnt, job_of(d, b), PANGU_CNT_KASTAUN_FAIL, st != 0);
-    if (st != 0) {
-      if (heat) heat_cell<MT>(d, p, P, U, b, k, j, i, g);
-      return;
-    }
+    if (st != 0) return;
   } else {
     Harm hs;
     harm_setup<MT>(UH, g, hs);
@@ -1154,20 +1142,18 @@ __global__ void __launch_bounds__(kThreads, 3) k_recovery(Dims d, pangu_params p
     if (!ok) return;
   }
   c2p_write(d, P, b, k, j, i, PH);
-  if (heat) heat_cell<MT>(d, p, P, U, b, k, j, i, g);
 }
 
 // Recovery, second pass over the cells Scheme2D failed: Scheme1Dvsq, then
 // Scheme1D (invertor.cc:185-197).
 template <int MT>
-// With fuse != 0: also the electron heating of the cell once its primitives
-// are final, and cells the whole chain failed are appended to the
-// FixRecovery list (nfix, fix) -- exactly the cells whose flag ends at 0.
+// With fix non-null the cells the whole chain failed are appended to the
+// FixRecovery list (nfix, fix): exactly the cells whose flag ends at 0.
 __global__ void __launch_bounds__(kThreads) k_recovery_retry(Dims d, pangu_params p, PT *P,
                                                              const double *U, double *flag,
                                                              unsigned long long *cnt,
                                                              const int *nretry,
-                                                             const long long *retry, int fuse,
+                                                             const long long *retry,
                                                              int *nfix, long long *fix) {
   const int n = *nretry;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
@@ -1194,10 +1180,7 @@ __global__ void __launch_bounds__(kThreads) k_recovery_retry(Dims d, pangu_param
     }
     flag[fc] = ok ? 1.0 : 0.0;
     c2p_write(d, P, b, k, j, i, PH);
-    if (fuse) {
-      if (p.enable_heating) heat_cell<MT>(d, p, P, U, b, k, j, i, g);
-      append(nfix, fix, !ok, fc);
-    }
+    if (fix) append(nfix, fix, !ok, fc);
   }
 }
 
@@ -1583,30 +1566,28 @@ int run_source(pangu_engine *e, const pangu_pack *md, double beta, const double 
   return check_launch();
 }
 
-// Recovery; with fuse, preceded by the geometric source and followed by
-// electron heating on each cell, and the FixRecovery list built by the retry
-// pass (the stage path).
-int run_recovery(pangu_engine *e, const pangu_pack *md, bool fuse, double beta, const double *dt,
-                 cudaStream_t s) {
+// Recovery; with list_fix the retry pass also lists the cells FixRecovery
+// repairs (the stage path).
+int run_recovery(pangu_engine *e, const pangu_pack *md, bool list_fix, cudaStream_t s) {
   const Dims &d = e->d;
   const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
   if (cudaMemsetAsync(e->d_fail_count, 0, sizeof(int), s) != cudaSuccess) return PANGU_ECUDA;
-  if (fuse && cudaMemsetAsync(e->d_fix_count, 0, sizeof(int), s) != cudaSuccess)
+  if (list_fix && cudaMemsetAsync(e->d_fix_count, 0, sizeof(int), s) != cudaSuccess)
     return PANGU_ECUDA;
   DISPATCH_MT(e->p.metric_type, k_recovery, grid_for(n), s, d, e->p, prim_of(md), md->cons, md->flag,
-              e->d_cnt, e->d_fail_count, e->d_fail_list, fuse ? 1 : 0, beta, dt);
+              e->d_cnt, e->d_fail_count, e->d_fail_list);
   ++e->launches;
   if (e->p.recovery == PANGU_RECOVERY_CHAINER) {
     DISPATCH_MT(e->p.metric_type, k_recovery_retry, 2 * 148, s, d, e->p, prim_of(md), md->cons,
-                md->flag, e->d_cnt, e->d_fail_count, e->d_fail_list, fuse ? 1 : 0, e->d_fix_count,
-                e->d_fix_list);
+                md->flag, e->d_cnt, e->d_fail_count, e->d_fail_list,
+                list_fix ? e->d_fix_count : nullptr, list_fix ? e->d_fix_list : nullptr);
     ++e->launches;
   }
   return check_launch();
 }
 
 int run_recovery(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
-  return run_recovery(e, md, false, 0.0, nullptr, s);
+  return run_recovery(e, md, false, s);
 }
 
 int run_heating(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
@@ -1618,7 +1599,7 @@ int run_heating(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
   return check_launch();
 }
 
-// FixRecovery. listed: the failed cells were listed by the fused recovery
+// FixRecovery. listed: the failed cells were listed by the recovery retry pass
 // (the stage path); otherwise a scan of the flags finds them. Both lists hold
 // the same cells (in a different order, which the two-phase fix ignores).
 int run_fix_recovery(pangu_engine *e, const pangu_pack *md, bool listed, cudaStream_t s) {
@@ -1686,9 +1667,10 @@ int run_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pa
   if (e->p.enable_B && (rc = run_ct(e, mc0, s))) return rc;
   if ((rc = run_update(e, base, mc0, mc1, beta, dt, s))) return rc;
   if ((rc = run_exchange(e, mc1, s))) return rc;
-  // AddGeometricSource, Recovery and ApplyElectronHeating in one pass; the
-  // retry pass lists the cells FixRecovery repairs
-  if ((rc = run_recovery(e, mc1, true, beta, dt, s))) return rc;
+  if ((rc = run_source(e, mc1, beta, dt, s))) return rc;
+  // the retry pass of Recovery lists the cells FixRecovery repairs
+  if ((rc = run_recovery(e, mc1, true, s))) return rc;
+  if ((rc = run_heating(e, mc1, s))) return rc;
   if (e->p.recovery == PANGU_RECOVERY_CHAINER && (rc = run_fix_recovery(e, mc1, true, s)))
     return rc;
   if ((rc = run_bcs(e, mc1, s))) return rc;

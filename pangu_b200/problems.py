@@ -369,6 +369,10 @@ def fm_torus(geo: Geometry, packages, pin: ParameterInput) -> np.ndarray:
     # MeshPostInitialization (problem_generator.cpp:291-558)
     rhomax = float(P[:, S["rho"]].max())
     umax = float(P[:, S["u"]].max())
+    if not rhomax > 0.0:
+        # the enthalpy never exceeds its inner-edge value: these (a, rin,
+        # rmax) admit no bound torus and the normalisation is undefined
+        raise ValueError(f"no bound torus for a={a}, rin={rin}, rmax={rmax}")
     P[:, S["rho"]] /= rhomax
     P[:, S["u"]] /= rhomax
     if not eB:

@@ -1,0 +1,78 @@
+"""Serving loop: jobs of several classes arriving over time are admitted as
+pool slots free up, stepped together, and each result is bit-identical to
+the job run alone (states and counters)."""
+import numpy as np
+import pytest
+
+from pangu_b200 import params as prm
+from pangu_b200 import problems
+
+pytestmark = pytest.mark.gpu
+
+
+def _job(problem, precision="fp64", **kw):
+    pin, gen = problems.make_problem(problem, **kw)
+    pin.set("b200", "precision", precision)
+    geo = problems.Geometry(prm.mesh_struct(pin))
+    return pin, gen(geo, prm.process_packages(pin), pin)
+
+
+def _alone(pin, prim, cycles):
+    import torch
+    from pangu_b200.engine import Simulation
+    sim = Simulation(pin)
+    sim.set_primitives(prim)
+    for _ in range(cycles):
+        sim.step()
+    torch.cuda.synchronize()
+    return sim.primitives(), sim.engine.counters()
+
+
+def test_server_results_match_alone():
+    from pangu_b200.engine import Server
+    tb = (32, 16, 1)
+    jobs = [  # (class, (pin, prim), cycles, arrival seconds)
+        ("torus", _job("torus", nx1=64, nx2=32, bx=tb, a=0.9375, seed=1), 5, 0.0),
+        ("torus", _job("torus", nx1=32, nx2=16, bx=tb, a=0.5, seed=2), 3, 0.0),
+        ("torus", _job("torus", nx1=64, nx2=32, bx=tb, a=0.98, seed=3), 4, 0.001),
+        ("ot", _job("ot", n=32, nblock=16), 4, 0.0),
+        ("ot", _job("ot", n=48, nblock=16), 3, 0.002),
+        ("bw", _job("bw", n=256, nblock=64), 6, 0.0),
+        ("bw", _job("bw", n=128, nblock=64), 2, 0.003),
+        ("mixed", _job("torus", "mixed", nx1=64, nx2=32, bx=tb, a=0.7, seed=4), 3, 0.0),
+    ]
+    srv = Server(8 << 30)
+    templates = {"torus": jobs[0][1][0], "ot": jobs[3][1][0], "bw": jobs[5][1][0],
+                 "mixed": jobs[7][1][0]}
+    # the torus pool holds 5 blocks: the third torus waits for the second
+    caps = {"torus": (5, 2), "ot": (13, 2), "bw": (4, 2), "mixed": (4, 1)}
+    cls = {k: srv.add_class(t, *caps[k]) for k, t in templates.items()}
+    tickets = [srv.submit(cls[c], pin, prim, n, t) for c, (pin, prim), n, t in jobs]
+    srv.run()
+    st = srv.stats()
+    lat = []
+    for tk, (c, (pin, prim), n, t) in zip(tickets, jobs):
+        got, times, cnt = srv.result(tk)
+        ref, ref_cnt = _alone(pin, prim, n)
+        np.testing.assert_array_equal(got, ref, err_msg=c)
+        np.testing.assert_array_equal(cnt, ref_cnt, err_msg=c)
+        assert times[0] == t and times[1] >= t and times[2] > times[1]
+        lat.append(times[2] - times[0])
+    assert st["jobs"] == len(jobs)
+    assert st["p50_s"] <= st["p99_s"] <= max(lat) + 1e-9
+    cells = sum(np.prod([pin.get_or_add_integer("parthenon/mesh", f"nx{d}", 1)
+                         for d in (1, 2, 3)]) * n for _, (pin, _p), n, _t in jobs)
+    assert st["zone_cycles"] == cells
+    # the third torus (4 blocks) could only start after the second finished
+    _, t_b, _ = srv.result(tickets[1])
+    _, t_c, _ = srv.result(tickets[2])
+    assert t_c[1] >= t_b[2]
+
+
+def test_server_budget_enforced():
+    from pangu_b200.engine import EngineError, Server
+    pin, _ = _job("torus", nx1=64, nx2=32, bx=(32, 16, 1))
+    srv = Server(64 << 20)  # 64 MiB
+    with pytest.raises(EngineError):
+        srv.add_class(pin, 1000, 4)
+    srv.add_class(pin, 4, 2)
