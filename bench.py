@@ -267,6 +267,7 @@ def run_engine(args):
     for _ in range(args.warmup):
         sim.step()
     torch.cuda.synchronize()
+    sim.autotune()  # flux tile shapes for this grid (results do not depend on them)
     if not args.no_graph:
         # one RK2 cycle per CUDA graph replay; the capture runs no kernel
         launches_per_step = sim.engine.launches()
@@ -324,6 +325,7 @@ def run_engine(args):
                 "step_algorithmic_bytes": step_bytes,
                 "step_achieved_gbs": round(step_bytes * value / n_int / world / 1e9, 2),
                 "task_ms": {k: round(v, 5) for k, v in tasks.items()}}
+        tiles = sim.engine.flux_config()
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             pin.set("b200", "precision", "fp64")
@@ -345,7 +347,7 @@ def run_engine(args):
                         "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
                         "steps": e2e["steps"]},
                 "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
-                "gpu_launches": launches}
+                "gpu_launches": launches, "flux_tiles": tiles}
         if err is not None:
             line["error_vs_fp64"] = err
     if world > 1:
@@ -524,6 +526,7 @@ def run_batch(args):
     for _ in range(args.warmup):
         pool.step(graph=False)
     torch.cuda.synchronize()
+    pool.autotune()
     launches0 = pool.engine.launches()
     pool.step()  # captures the cycle graph, then replays it
     torch.cuda.synchronize()
@@ -577,7 +580,8 @@ def run_batch(args):
                 "launch": "one CUDA graph replay per RK2 step of all 48 jobs"}),
             "e2e": {"value": round(e2e, 1), "unit": METRIC, "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes, "steps": k},
-            "clocks": clk.summary(), "gpu_launches": per_step * args.steps}
+            "clocks": clk.summary(), "gpu_launches": per_step * args.steps,
+            "flux_tiles": pool.engine.flux_config()}
     if err is not None:
         line["error_vs_fp64"] = err
     print(json.dumps(line), flush=True)

@@ -248,6 +248,19 @@ int pangu_reset_counters(pangu_engine *e, void *stream);
 /* Number of CUDA kernels this handle has launched so far (host-side count). */
 long long pangu_launches(const pangu_engine *e);
 
+/* Autotuner of the flux kernels' tile shapes (no counterpart in the
+ * reference): times each candidate shape of every direction -- CTA size 64
+ * or 128, and for x2/x3 a march depth of 1, 2 or 4 faces per thread -- on
+ * the pack's own data and keeps the fastest for this engine. Every candidate
+ * computes each face identically, so results never depend on the choice.
+ * Overwrites the pack's fluxes and alfven (which every stage recomputes
+ * before reading them), synchronises the stream, and must not be called
+ * during stream capture. */
+int pangu_autotune(pangu_engine *e, const pangu_pack *md, void *stream);
+/* Current tile shapes: {march1, threads1, march2, threads2, march3,
+ * threads3, tuned}. */
+int pangu_flux_config(const pangu_engine *e, int32_t out[7]);
+
 /* ---- block pool: many jobs stepped by the same launches ---------------- */
 /* No counterpart in the reference, which runs one mesh per process. A pool
  * engine owns a block table over `capacity_blocks` slots of the block shape

@@ -36,6 +36,7 @@ int run_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pa
               double beta, const double *dt, double *dt_est, cudaStream_t s);
 int run_job_start(pangu_engine *e, int job, const pangu_pack *base, const pangu_pack *one,
                   cudaStream_t s);
+int run_autotune(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
 }  // namespace pgkmx
 
 // Launch helper of the engine's precision.
@@ -469,6 +470,21 @@ int pangu_estimate_dt(pangu_engine *e, const pangu_pack *md, double *dt_out, voi
   GUARD(e, md);
   if (!dt_out) return PANGU_EINVAL;
   return RUN(run_estimate_dt, e, md, dt_out, S(stream));
+}
+
+int pangu_autotune(pangu_engine *e, const pangu_pack *md, void *stream) {
+  GUARD(e, md);
+  return RUN(run_autotune, e, md, S(stream));
+}
+
+int pangu_flux_config(const pangu_engine *e, int32_t out[7]) {
+  if (!e || !out) return PANGU_EINVAL;
+  for (int d = 0; d < 3; ++d) {
+    out[2 * d] = e->tune.march[d];
+    out[2 * d + 1] = e->tune.threads[d];
+  }
+  out[6] = e->tune.tuned;
+  return PANGU_OK;
 }
 
 int pangu_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,

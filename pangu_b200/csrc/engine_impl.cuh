@@ -95,6 +95,13 @@ struct pangu_engine {
   long long fail_cap = 0;
   unsigned long long *d_dtmin = nullptr;  // [capacity][3]
   long long launches = 0;  // kernels launched through this handle
+  // Tile shapes of the flux kernels per direction: march depth (x2/x3) and
+  // CTA size; set by pangu_autotune.
+  struct {
+    int march[3] = {1, 2, 2};
+    int threads[3] = {128, 128, 128};
+    int tuned = 0;
+  } tune;
 };
 
 #endif  // PANGU_ENGINE_IMPL_CUH

@@ -643,11 +643,11 @@ __global__ void __launch_bounds__(kFluxThreads, 4) k_flux_x1(Dims d, pangu_param
   face_flux<MT, 1>(d, p, b, k, j, c, PL, PR, F, alfven);
 }
 
-// x2 / x3 faces: a thread marches over kMarch consecutive faces of one
-// column, carrying the upper-face value of the previous cell.
-constexpr int kMarch = 4;
-
-template <int MT, int DIR>
+// x2 / x3 faces: a thread marches over MARCH consecutive faces of one
+// column, carrying the upper-face value of the previous cell. A deeper march
+// reconstructs fewer cells twice but gives fewer threads; the autotuner picks
+// the depth (and the CTA size) for the engine's grid.
+template <int MT, int DIR, int MARCH>
 __device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_params &p, int k0,
                                                 int k1, int j0, int j1, int i0, int i1,
                                                 const PT *P, double *F, double *alfven) {
@@ -655,7 +655,7 @@ __device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_param
   const int m0 = DIR == 2 ? j0 : k0, m1 = DIR == 2 ? j1 : k1;
   const int a0 = DIR == 2 ? k0 : j0, a1 = DIR == 2 ? k1 : j1;  // outer transverse index
   const int ni = i1 - i0 + 1, na = a1 - a0 + 1;
-  const int nruns = (m1 - m0 + 1 + kMarch - 1) / kMarch;
+  const int nruns = (m1 - m0 + 1 + MARCH - 1) / MARCH;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)d.NB * na * nruns * ni) return;
   const int i = i0 + (int)(t % ni);
@@ -666,8 +666,8 @@ __device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_param
   const int b = slot_of(d, (int)(r / na));
   const long long stride = DIR == 2 ? (long long)d.N1 : (long long)d.N1 * d.N2;
   const bool use_mc = p.limiter == PANGU_LIMITER_MC;
-  const int f0 = m0 + run * kMarch;
-  const int f1 = min(f0 + kMarch - 1, m1);
+  const int f0 = m0 + run * MARCH;
+  const int f1 = min(f0 + MARCH - 1, m1);
   FT carry[NPRIM];
   {
     const int c = f0 - 1;
@@ -695,19 +695,19 @@ __device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_param
   }
 }
 
-template <int MT>
+template <int MT, int MARCH>
 __global__ void __launch_bounds__(kFluxThreads, 4) k_flux_march2(Dims d, pangu_params p, int k0, int k1,
                                                           int j0, int j1, int i0, int i1,
                                                           const PT *P, double *F,
                                                           double *alfven) {
-  flux_march_body<MT, 2>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
+  flux_march_body<MT, 2, MARCH>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
 }
-template <int MT>
+template <int MT, int MARCH>
 __global__ void __launch_bounds__(kFluxThreads, 4) k_flux_march3(Dims d, pangu_params p, int k0, int k1,
                                                           int j0, int j1, int i0, int i1,
                                                           const PT *P, double *F,
                                                           double *alfven) {
-  flux_march_body<MT, 3>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
+  flux_march_body<MT, 3, MARCH>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
 }
 
 // ---------------------------------------------------------------------------
@@ -1442,8 +1442,8 @@ inline long long box_count(int NB, int k0, int k1, int j0, int j1, int i0, int i
     }                                                                                        \
   } while (0)
 
-inline unsigned grid_flux(long long n) {
-  return (unsigned)std::max<long long>(1, (n + kFluxThreads - 1) / kFluxThreads);
+inline unsigned grid_flux(long long n, int threads) {
+  return (unsigned)std::max<long long>(1, (n + threads - 1) / threads);
 }
 
 bool pack_ok(const pangu_engine *e, const pangu_pack *md) {
@@ -1482,40 +1482,112 @@ int run_calc_cons(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
   return run_calc_cons(e, e->d, md, !PGK_MIXED, s);
 }
 
-int run_fluxes(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
+// Launches the flux kernel of one direction with a given march depth
+// (x2/x3) and CTA size.
+template <int MT>
+void launch_flux_dir(const pangu_engine *e, const pangu_pack *md, int dir, int march, int threads,
+                     cudaStream_t s) {
   const Dims &d = e->d;
   const bool hll = e->p.riemann_solver == PANGU_RIEMANN_HLL;
-  for (int dir = 1; dir <= d.ndim; ++dir) {
-    int k0 = d.ks - d.o3, k1 = d.ke + d.o3, j0 = d.js - d.o2, j1 = d.je + d.o2;
-    int i0 = d.is - d.o1, i1 = d.ie + d.o1;
-    if (dir == 1) { i0 = d.is; i1 = d.ie + 1; }
-    if (dir == 2) { j0 = d.js; j1 = d.je + 1; }
-    if (dir == 3) {  // hll.cc:293-296 narrows the transverse range
-      k0 = d.ks; k1 = d.ke + 1;
-      if (hll) { j0 = d.js; j1 = d.je; i0 = d.is; i1 = d.ie; }
-    }
-    double *F = dir == 1 ? md->flux1 : (dir == 2 ? md->flux2 : md->flux3);
-#define FLUX_ARGS d, e->p, k0, k1, j0, j1, i0, i1, prim_of(md), F, md->alfven
-    if (dir == 1) {
-      const int nseg = (i1 - i0 + 1 + kFacesPerWarp - 1) / kFacesPerWarp;
-      const long long warps = (long long)d.NB * (k1 - k0 + 1) * (j1 - j0 + 1) * nseg;
-      DISPATCH_MT_T(e->p.metric_type, k_flux_x1, grid_flux(32 * warps), kFluxThreads, s, FLUX_ARGS);
-    } else {
-      const int m = dir == 2 ? (j1 - j0 + 1) : (k1 - k0 + 1);
-      const int na = dir == 2 ? (k1 - k0 + 1) : (j1 - j0 + 1);
-      const long long n = (long long)d.NB * na * ((m + kMarch - 1) / kMarch) * (i1 - i0 + 1);
-      if (dir == 2)
-        DISPATCH_MT_T(e->p.metric_type, k_flux_march2, grid_flux(n), kFluxThreads, s, FLUX_ARGS);
-      else
-        DISPATCH_MT_T(e->p.metric_type, k_flux_march3, grid_flux(n), kFluxThreads, s, FLUX_ARGS);
-    }
-#undef FLUX_ARGS
-    ++e->launches;
-    const int rc = check_launch();
+  int k0 = d.ks - d.o3, k1 = d.ke + d.o3, j0 = d.js - d.o2, j1 = d.je + d.o2;
+  int i0 = d.is - d.o1, i1 = d.ie + d.o1;
+  if (dir == 1) { i0 = d.is; i1 = d.ie + 1; }
+  if (dir == 2) { j0 = d.js; j1 = d.je + 1; }
+  if (dir == 3) {  // hll.cc:293-296 narrows the transverse range
+    k0 = d.ks; k1 = d.ke + 1;
+    if (hll) { j0 = d.js; j1 = d.je; i0 = d.is; i1 = d.ie; }
+  }
+  double *F = dir == 1 ? md->flux1 : (dir == 2 ? md->flux2 : md->flux3);
+  const PT *P = prim_of(md);
+  if (dir == 1) {
+    const int nseg = (i1 - i0 + 1 + kFacesPerWarp - 1) / kFacesPerWarp;
+    const long long warps = (long long)d.NB * (k1 - k0 + 1) * (j1 - j0 + 1) * nseg;
+    k_flux_x1<MT><<<grid_flux(32 * warps, threads), threads, 0, s>>>(d, e->p, k0, k1, j0, j1, i0,
+                                                                     i1, P, F, md->alfven);
+    return;
+  }
+  const int m = dir == 2 ? (j1 - j0 + 1) : (k1 - k0 + 1);
+  const int na = dir == 2 ? (k1 - k0 + 1) : (j1 - j0 + 1);
+  const long long n = (long long)d.NB * na * ((m + march - 1) / march) * (i1 - i0 + 1);
+  const unsigned g = grid_flux(n, threads);
+#define PGK_MARCH(M)                                                                         \
+  if (dir == 2)                                                                              \
+    k_flux_march2<MT, M><<<g, threads, 0, s>>>(d, e->p, k0, k1, j0, j1, i0, i1, P, F, md->alfven); \
+  else                                                                                       \
+    k_flux_march3<MT, M><<<g, threads, 0, s>>>(d, e->p, k0, k1, j0, j1, i0, i1, P, F, md->alfven);
+  switch (march) {
+    case 1: PGK_MARCH(1) break;
+    case 2: PGK_MARCH(2) break;
+    default: PGK_MARCH(4) break;
+  }
+#undef PGK_MARCH
+}
+
+int run_flux_dir(pangu_engine *e, const pangu_pack *md, int dir, int march, int threads,
+                 cudaStream_t s) {
+  switch (e->p.metric_type) {
+    case PANGU_METRIC_MKS: launch_flux_dir<MKS>(e, md, dir, march, threads, s); break;
+    case PANGU_METRIC_BL: launch_flux_dir<BL>(e, md, dir, march, threads, s); break;
+    case PANGU_METRIC_CKS: launch_flux_dir<CKS>(e, md, dir, march, threads, s); break;
+    default: launch_flux_dir<MINKOWSKI>(e, md, dir, march, threads, s); break;
+  }
+  ++e->launches;
+  return check_launch();
+}
+
+int run_fluxes(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
+  for (int dir = 1; dir <= e->d.ndim; ++dir) {
+    const int rc = run_flux_dir(e, md, dir, e->tune.march[dir - 1], e->tune.threads[dir - 1], s);
     if (rc) return rc;
   }
   return PANGU_OK;
 }
+
+// Times every candidate tile shape of each direction's flux kernel on the
+// pack's own data (best of three launches after one untimed launch, CUDA
+// events on stream s) and keeps the fastest in e->tune. The candidates
+// compute every face identically, so the choice never changes results.
+int run_autotune(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
+  if (e->d.NB == 0) return PANGU_OK;
+  cudaEvent_t ev[2];
+  if (cudaEventCreate(&ev[0]) != cudaSuccess) return PANGU_ECUDA;
+  if (cudaEventCreate(&ev[1]) != cudaSuccess) {
+    cudaEventDestroy(ev[0]);
+    return PANGU_ECUDA;
+  }
+  int rc = PANGU_OK;
+  const int thread_opts[2] = {64, 128};
+  const int march_opts[3] = {1, 2, 4};
+  for (int dir = 1; dir <= e->d.ndim && !rc; ++dir) {
+    float best = 1e30f;
+    const int nm = dir == 1 ? 1 : 3;
+    for (int mi = 0; mi < nm && !rc; ++mi)
+      for (int ti = 0; ti < 2 && !rc; ++ti) {
+        const int march = dir == 1 ? 1 : march_opts[mi], threads = thread_opts[ti];
+        float t = 1e30f;
+        for (int rep = 0; rep < 4 && !rc; ++rep) {
+          if (cudaEventRecord(ev[0], s) != cudaSuccess) rc = PANGU_ECUDA;
+          if (!rc) rc = run_flux_dir(e, md, dir, march, threads, s);
+          if (!rc && (cudaEventRecord(ev[1], s) != cudaSuccess ||
+                      cudaEventSynchronize(ev[1]) != cudaSuccess))
+            rc = PANGU_ECUDA;
+          float ms = 0;
+          if (!rc && cudaEventElapsedTime(&ms, ev[0], ev[1]) != cudaSuccess) rc = PANGU_ECUDA;
+          if (!rc && rep > 0) t = std::min(t, ms);
+        }
+        if (!rc && t < best) {
+          best = t;
+          e->tune.march[dir - 1] = march;
+          e->tune.threads[dir - 1] = threads;
+        }
+      }
+  }
+  if (!rc) e->tune.tuned = 1;
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  return rc;
+}
+
 
 int run_ct(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
   const Dims &d = e->d;

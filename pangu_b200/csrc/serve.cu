@@ -44,7 +44,7 @@ struct SClass {
   cudaStream_t stream = nullptr;
   cudaEvent_t tick_done = nullptr;
   cudaGraphExec_t graph = nullptr;
-  bool dirty = true, inflight = false;
+  bool dirty = true, inflight = false, tuned = false;
   int running = 0;
 };
 
@@ -346,6 +346,10 @@ int pangu_server_run(pangu_server *s) {
         j.t_admit = now_s(t0);
       }
       if (!c.running) continue;
+      if (!c.tuned) {  // flux tile shapes, tuned once on the class's first jobs
+        if ((rc = pangu_autotune(c.e, &c.a.base, c.stream))) return rc;
+        c.tuned = true;
+      }
       if (c.dirty && (rc = capture(c))) return rc;
       if (cudaGraphLaunch(c.graph, c.stream) != cudaSuccess ||
           cudaEventRecord(c.tick_done, c.stream) != cudaSuccess)

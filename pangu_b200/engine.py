@@ -79,6 +79,8 @@ def lib():
     L.pangu_job_detach.argtypes = [_P, C.c_int32]
     L.pangu_job_counters.argtypes = [_P, C.c_int32, C.POINTER(C.c_uint64)]
     L.pangu_active_blocks.argtypes = [_P]
+    L.pangu_autotune.argtypes = [_P, _PK, _P]
+    L.pangu_flux_config.argtypes = [_P, C.POINTER(C.c_int32)]
     L.pangu_server_create.argtypes = [C.c_uint64, C.POINTER(_P)]
     L.pangu_server_destroy.argtypes = [_P]
     L.pangu_server_add_class.argtypes = [_P, C.POINTER(abi.Params), C.POINTER(abi.Mesh), C.c_int32,
@@ -232,6 +234,17 @@ class Engine:
     def reset_counters(self):
         _check(self.L.pangu_reset_counters(self.h, self.stream()), "pangu_reset_counters")
 
+    def autotune(self, md):
+        """Picks the flux kernels' tile shapes by timing them on md's data."""
+        _check(self.L.pangu_autotune(self.h, md.pack, self.stream()), "pangu_autotune")
+
+    def flux_config(self) -> dict:
+        out = (C.c_int32 * 7)()
+        _check(self.L.pangu_flux_config(self.h, out), "pangu_flux_config")
+        v = list(out)
+        return {"x1_threads": v[1], "x2_march": v[2], "x2_threads": v[3],
+                "x3_march": v[4], "x3_threads": v[5], "tuned": bool(v[6])}
+
     # ---- block pool --------------------------------------------------------
     def attach(self, mesh: abi.Mesh, a: float, h: float):
         job = C.c_int32()
@@ -303,6 +316,11 @@ class Simulation:
         self.stage(2, self.dt_est)
         if not fixed_dt:
             self.engine.update_dt(self.dt, self.dt_est, self.dt_factor)
+
+    def autotune(self):
+        """Tunes the flux kernels' tile shapes on this job's current state
+        (call between cycles, before capture)."""
+        self.engine.autotune(self.base)
 
     def capture(self):
         """Captures one RK2 cycle (both stages and the device dt policy) as a
@@ -409,6 +427,11 @@ class Pool:
         e.stage(1, self.base, self.one, RK2_BETA[1], self.dt)
         e.stage(2, self.base, self.one, RK2_BETA[0], self.dt, self.dt_est)
         e.update_dt(self.dt, self.dt_est, self.dt_factor)
+
+    def autotune(self):
+        """Tunes the flux kernels' tile shapes on the attached jobs' state."""
+        self.engine.autotune(self.base)
+        self._graph = None
 
     def step(self, graph: bool = True):
         """One RK2 cycle of every attached job."""
