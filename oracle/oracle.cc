@@ -873,6 +873,11 @@ double or_cell_clamp(double rmin, double rmax, double total, double electron) {
 void or_pgm_pow(int n, const double *x, const double *y, double *out) {
   for (int i = 0; i < n; ++i) out[i] = pgm::pow(x[i], y[i]);
 }
+// The slow double-double path of pgm::pow alone (finite x > 0), for tests of
+// the table-driven fast path.
+void or_pgm_pow_slow(int n, const double *x, const double *y, double *out) {
+  for (int i = 0; i < n; ++i) out[i] = pgm::exp_round(pgm::mul_d(pgm::log_dd(x[i]), y[i]));
+}
 void or_pgm_exp(int n, const double *x, double *out) {
   for (int i = 0; i < n; ++i) out[i] = pgm::exp(x[i]);
 }

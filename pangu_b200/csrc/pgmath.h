@@ -11,19 +11,29 @@
 // Method (textbook double-double arithmetic, own implementation):
 //   * error-free transforms two_sum (Knuth) and two_prod via fused
 //     multiply-add (Dekker's product with an exact fma);
-//   * log x = e ln 2 + 2 atanh(s), s = (m - 1)/(m + 1), m in [1/sqrt2, sqrt2),
-//     the atanh series summed to |s|^42 (first nine terms in double-double);
-//   * exp t = 2^k exp(r), r = (t - k ln 2)/64, Taylor series of exp(r) - 1 to
-//     r^12 (first five terms in double-double), then six squarings;
-//   * pow x^y = exp(y log x).
-// The relative error before the final rounding is below 2^-95, so the result
-// is the correctly rounded one except when the exact value lies within
-// 2^-95 of a rounding boundary. tests/test_pgmath.py checks agreement with
-// the C library's pow/exp/log on many inputs.
+//   * slow path: log x = e ln 2 + 2 atanh(s), s = (m - 1)/(m + 1), m in
+//     [1/sqrt2, sqrt2), the atanh series summed to |s|^42 (first nine terms in
+//     double-double); exp t = 2^k exp(r), r = (t - k ln 2)/64, Taylor series
+//     of exp(r) - 1 to r^12 (first five terms in double-double), then six
+//     squarings. Relative error before the final rounding below 2^-95.
+//   * fast path of pow (table-driven, pgmath_tables.h): ln m = L_j +
+//     log1p(m inv_j - 1) with |m inv_j - 1| < 2^-9.5 (363 intervals of width
+//     1/512; the product m inv_j is formed exactly), log1p by its series with
+//     the r^2 and r^3 terms in double-double (relative error < 2^-80);
+//     exp t = 2^(k/128) exp(r), |r| <= ln2/256, Cody-Waite reduction, series
+//     to r^8 (relative error < 2^-76). The result hi + lo is returned only if
+//     every value within the error bound rounds to the same double (Ziv's
+//     rounding test); otherwise the slow path decides, so both paths give
+//     the same correctly rounded result except within 2^-95 of a rounding
+//     boundary.
+// tests/test_pgmath.py checks the results against 60-digit decimal
+// arithmetic and the C library on many inputs.
 #ifndef PANGU_PGMATH_H
 #define PANGU_PGMATH_H
 
 #include <cmath>
+
+#include "pgmath_tables.h"
 
 #if defined(__CUDACC__)
 #define PGM_FN __host__ __device__ __forceinline__
@@ -166,6 +176,91 @@ PGM_FN double exp_round(dd t) {
   return ldexp(E.hi, (int)kd);
 }
 
+// Tables of the fast path, readable from host and device code.
+static const double kLogTabH[] = PGM_LOG_TABLE_INIT;
+static const double kExpTabH[] = PGM_EXP_TABLE_INIT;
+#if defined(__CUDACC__)
+static __device__ const double kLogTabD[] = PGM_LOG_TABLE_INIT;
+static __device__ const double kExpTabD[] = PGM_EXP_TABLE_INIT;
+#endif
+PGM_FN double log_tab(int i) {
+#if defined(__CUDA_ARCH__)
+  return __ldg(kLogTabD + i);
+#else
+  return kLogTabH[i];
+#endif
+}
+PGM_FN double exp_tab(int i) {
+#if defined(__CUDA_ARCH__)
+  return __ldg(kExpTabD + i);
+#else
+  return kExpTabH[i];
+#endif
+}
+
+// ln x as double-double for finite x > 0, relative error below 2^-80.
+PGM_FN dd log_fast(double x) {
+  int e;
+  double m = frexp(x, &e);  // x = m 2^e, m in [0.5, 1)
+  m *= 2.0;
+  e -= 1;
+  if (m > 1.4142135623730951) {
+    m *= 0.5;
+    e += 1;
+  }
+  const int j = (int)((m - PGM_LOG_M0) * 512.0);
+  const double inv = log_tab(3 * j);
+  const dd L = {log_tab(3 * j + 1), log_tab(3 * j + 2)};
+  const dd p = two_prod(m, inv);                   // m inv exactly
+  const dd r = quick_two_sum(p.hi - 1.0, p.lo);    // p.hi - 1 exact (Sterbenz)
+  // log1p(r) = r - r^2/2 + r^3/3 + r^4 Q(r)
+  dd r2 = two_prod(r.hi, r.hi);
+  r2.lo += 2.0 * r.hi * r.lo;
+  const dd r3 = mul(r2, r);
+  const dd t3 = mul(r3, dd{0x1.5555555555555p-2, 0x1.5555555555555p-56});  // r^3/3
+  double q = -0x1.999999999999ap-4;             // -1/10
+  q = 0x1.c71c71c71c71cp-4 + r.hi * q;          // 1/9
+  q = -0x1.0000000000000p-3 + r.hi * q;         // -1/8
+  q = 0x1.2492492492492p-3 + r.hi * q;          // 1/7
+  q = -0x1.5555555555555p-3 + r.hi * q;         // -1/6
+  q = 0x1.999999999999ap-3 + r.hi * q;          // 1/5
+  q = -0x1.0000000000000p-2 + r.hi * q;         // -1/4
+  const double t4 = (r2.hi * r2.hi) * q;
+  dd lg = add(r, dd{-0.5 * r2.hi, -0.5 * r2.lo});
+  lg = add(lg, t3);
+  lg = add(lg, dd{t4, 0.0});
+  lg = add(lg, L);
+  if (e != 0) lg = add(mul_d(PGM_LN2, (double)e), lg);
+  return lg;
+}
+
+// exp t for a double-double t with |t.hi| <= 708 as hi + lo (relative error
+// below 2^-76) and the power of two k >> 7 still to apply.
+PGM_FN dd exp_fast(dd t, int &scale) {
+  const double kd = rint(t.hi * PGM_INV_LN2_128);
+  const int k = (int)kd;
+  // r = t - k ln2/128, Cody-Waite: k C1 is exact and t.hi - k C1 exact
+  const dd kc2 = two_prod(kd, PGM_LN2_128_C2);
+  dd r = two_sum(t.hi - kd * PGM_LN2_128_C1, -kc2.hi);
+  r.lo += (t.lo - kc2.lo) - kd * PGM_LN2_128_C3;
+  r = quick_two_sum(r.hi, r.lo);
+  // exp(r) - 1 = r + r^2/2 + r^3 P(r)
+  dd r2 = two_prod(r.hi, r.hi);
+  r2.lo += 2.0 * r.hi * r.lo;
+  double P = 0x1.a01a01a01a01ap-16;             // 1/8!
+  P = 0x1.a01a01a01a01ap-13 + r.hi * P;         // 1/7!
+  P = 0x1.6c16c16c16c17p-10 + r.hi * P;         // 1/6!
+  P = 0x1.1111111111111p-7 + r.hi * P;          // 1/5!
+  P = 0x1.5555555555555p-5 + r.hi * P;          // 1/4!
+  P = 0x1.5555555555555p-3 + r.hi * P;          // 1/3!
+  dd q = add(r, dd{0.5 * r2.hi, 0.5 * r2.lo});
+  q = add(q, dd{(r2.hi * r.hi) * P, 0.0});
+  const dd E = add(dd{1.0, 0.0}, q);
+  const int jj = k & 127;
+  scale = k >> 7;  // arithmetic shift: floor(k / 128)
+  return mul(dd{exp_tab(2 * jj), exp_tab(2 * jj + 1)}, E);
+}
+
 PGM_FN bool is_inf(double x) { return fabs(x) == HUGE_VAL; }
 PGM_FN bool sign_bit(double x) { return copysign(1.0, x) < 0.0; }
 
@@ -197,7 +292,20 @@ PGM_FN double pow(double x, double y) {
   } else if (is_inf(x)) {
     r = y < 0.0 ? 0.0 : HUGE_VAL;
   } else {
-    r = exp_round(mul_d(log_dd(x), y));
+    const dd t = mul_d(log_fast(x), y);
+    bool done = false;
+    if (fabs(t.hi) < 700.0) {
+      int scale;
+      const dd v = exp_fast(t, scale);
+      // error bound of v: exp part 2^-70, plus |t| times the log's 2^-78
+      const double err = fabs(v.hi) * (0x1p-70 + fabs(t.hi) * 0x1p-78);
+      const double a = v.hi + (v.lo + err), b = v.hi + (v.lo - err);
+      if (a == b) {
+        r = ldexp(a, scale);
+        done = true;
+      }
+    }
+    if (!done) r = exp_round(mul_d(log_dd(x), y));  // slow path
   }
   return negate ? -r : r;
 }

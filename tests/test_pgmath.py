@@ -48,6 +48,35 @@ def test_pow_correctly_rounded():
         assert _is_correctly_rounded(oi, exact), (xi.hex(), yi.hex(), oi.hex())
 
 
+def _pow_slow(x, y):
+    out = np.empty_like(x)
+    L.or_pgm_pow_slow(len(x), x.ctypes.data_as(_D), y.ctypes.data_as(_D),
+                      out.ctypes.data_as(_D))
+    return out
+
+
+def test_fast_path_agrees_with_slow_path():
+    """The table-driven fast path returns a result only when its error bound
+    guarantees the rounding; it must then agree with the 2^-95 slow path
+    everywhere: physics exponents over the floor-to-torus range of values,
+    arbitrary exponents, and arguments near 1 and near table boundaries."""
+    rng = np.random.default_rng(11)
+    n = 400000
+    cases = [
+        (10 ** rng.uniform(-12, 6, n),
+         rng.choice([5 / 3, -5 / 3, 4 / 3, -4 / 3, 1 / 3, 2 / 3, -1.5, -2.5, 0.7, -1.4, 3.3], n)),
+        (10 ** rng.uniform(-300, 300, n), rng.uniform(-1.0, 1.0, n)),
+        (10 ** rng.uniform(-6, 6, n), rng.uniform(-40.0, 40.0, n)),
+        (1.0 + rng.uniform(-1e-3, 1e-3, n), rng.uniform(-1e4, 1e4, n)),
+        (np.ldexp(rng.uniform(0.70, 1.42, n), rng.integers(-60, 60, n)),
+         rng.uniform(-8.0, 8.0, n)),
+    ]
+    for x, y in cases:
+        fast, slow = _pow(x, y), _pow_slow(x, y)
+        bad = fast != slow
+        assert not bad.any(), (x[bad][:3], y[bad][:3], fast[bad][:3], slow[bad][:3])
+
+
 def test_exp_log_correctly_rounded():
     rng = np.random.default_rng(8)
     e = rng.uniform(-700, 700, 2000)
