@@ -1650,7 +1650,8 @@ int run_recovery(pangu_engine *e, const pangu_pack *md, bool list_fix, cudaStrea
               e->d_cnt, e->d_fail_count, e->d_fail_list);
   ++e->launches;
   if (e->p.recovery == PANGU_RECOVERY_CHAINER) {
-    DISPATCH_MT(e->p.metric_type, k_recovery_retry, 2 * 148, s, d, e->p, prim_of(md), md->cons,
+    // one-warp CTAs: the few thousand retried cells spread over every SM
+    DISPATCH_MT_T(e->p.metric_type, k_recovery_retry, 8 * 148, 32, s, d, e->p, prim_of(md), md->cons,
                 md->flag, e->d_cnt, e->d_fail_count, e->d_fail_list,
                 list_fix ? e->d_fix_count : nullptr, list_fix ? e->d_fix_list : nullptr);
     ++e->launches;
