@@ -295,6 +295,28 @@ int pangu_job_counters(pangu_engine *e, int32_t job, uint64_t out[PANGU_NCOUNTER
 /* Blocks in the launch domain (all attached jobs). */
 int pangu_active_blocks(const pangu_engine *e);
 
+/* ---- device-side initial conditions ------------------------------------ */
+/* The benchmark problems' initial primitives, generated on the device into
+ * a job's blocks of base (every cell; then call pangu_job_start). Same
+ * formulas as the host generators of pangu_b200/problems.py: Orszag-Tang,
+ * Brio-Wu, and the Fishbone-Moncrief torus of
+ * fm_torus_mks/problem_generator.cpp:103-558 (MKS only; the job's metric a
+ * and h), with its MeshPostInitialization (density normalisation, SANE A_phi,
+ * field normalised to the target beta) computed by device reductions and a
+ * counter-based random perturbation (SplitMix64 of seed and cell index).
+ * Synchronises the stream for a torus and returns PANGU_EINVAL when its
+ * parameters admit no bound torus. */
+#define PANGU_PROBLEM_ORSZAG_TANG 0
+#define PANGU_PROBLEM_BRIO_WU 1
+#define PANGU_PROBLEM_FM_TORUS 2
+typedef struct pangu_problem {
+  int32_t kind;               /* PANGU_PROBLEM_* */
+  int32_t seed;               /* <fm_torus>/seed */
+  double rin, rmax, kappa, perturbation, beta, aphi_rho_cut;  /* <fm_torus> */
+} pangu_problem;
+int pangu_generate(pangu_engine *e, int32_t job, const pangu_problem *problem,
+                   const pangu_pack *base, void *stream);
+
 /* ---- serving: continuous batching over block pools --------------------- */
 /* No counterpart in the reference. A server owns one block pool per job
  * class (parameter set + block shape), each with its containers, dt arrays,
@@ -326,6 +348,12 @@ int pangu_server_add_class(pangu_server *s, const pangu_params *params,
 int pangu_server_submit(pangu_server *s, int32_t cls, const pangu_mesh *mesh,
                         double a, double h, double dt_init, int64_t cycles,
                         double arrival_s, const double *prim_host, int32_t *ticket_out);
+/* A job whose initial state is generated on the device at admission
+ * (pangu_generate) instead of uploaded. */
+int pangu_server_submit_problem(pangu_server *s, int32_t cls, const pangu_mesh *mesh,
+                                double a, double h, double dt_init, int64_t cycles,
+                                double arrival_s, const pangu_problem *problem,
+                                int32_t *ticket_out);
 /* Runs until every submitted job is done. Blocks the calling thread. */
 int pangu_server_run(pangu_server *s);
 /* A finished job: primitives (FP64, layout of submit), times {arrival,

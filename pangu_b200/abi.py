@@ -99,3 +99,14 @@ class ServerStats(C.Structure):
         ("zone_cycles_per_s", C.c_double), ("p50_s", C.c_double), ("p99_s", C.c_double),
         ("hbm_bytes", C.c_uint64),
     ]
+
+
+PROBLEM = {"ot": 0, "orszag_tang": 0, "bw": 1, "brio_wu": 1, "torus": 2, "fm_torus": 2}
+
+
+class Problem(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32), ("seed", C.c_int32),
+        ("rin", C.c_double), ("rmax", C.c_double), ("kappa", C.c_double),
+        ("perturbation", C.c_double), ("beta", C.c_double), ("aphi_rho_cut", C.c_double),
+    ]

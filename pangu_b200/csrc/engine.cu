@@ -37,6 +37,8 @@ int run_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pa
 int run_job_start(pangu_engine *e, int job, const pangu_pack *base, const pangu_pack *one,
                   cudaStream_t s);
 int run_autotune(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
+int run_generate(pangu_engine *e, int job, const pangu_problem &pb, const pangu_pack *base,
+                 cudaStream_t s);
 }  // namespace pgkmx
 
 // Launch helper of the engine's precision.
@@ -75,6 +77,7 @@ int pangu_engine_destroy(pangu_engine *e) {
   cudaFree(e->d_fix_count);
   cudaFree(e->d_fix_list);
   cudaFree(e->d_tmp_slots);
+  cudaFree(e->d_genred);
   cudaFree(e->d_fail_vals);
   cudaFree(e->d_dtmin);
   delete e;
@@ -166,6 +169,7 @@ int pool_init(pangu_engine *e, int capacity, int max_jobs) {
   rc |= dalloc(&e->d_fail_vals, (size_t)e->fail_cap * d.NF);
   rc |= dalloc(&e->d_dtmin, 3 * (size_t)capacity);
   rc |= dalloc(&e->d_tmp_slots, capacity);
+  rc |= dalloc(&e->d_genred, 3);
   // every ghost cell of a slot has at most one exchange source
   e->xch_cap = (long long)capacity * (d.ncell - (long long)e->m.nx1 * e->m.nx2 * e->m.nx3);
   rc |= dalloc(&e->d_xdst, (size_t)e->xch_cap);
@@ -475,6 +479,17 @@ int pangu_estimate_dt(pangu_engine *e, const pangu_pack *md, double *dt_out, voi
 int pangu_autotune(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
   return RUN(run_autotune, e, md, S(stream));
+}
+
+int pangu_generate(pangu_engine *e, int32_t job, const pangu_problem *problem,
+                   const pangu_pack *base, void *stream) {
+  if (!pack_ok(e, base) || !problem || job < 0 || job >= e->max_jobs || !e->jobs[job].live ||
+      problem->kind < 0 || problem->kind > 2)
+    return PANGU_EINVAL;
+  if (problem->kind == PANGU_PROBLEM_FM_TORUS &&
+      !(problem->kappa > 0 && problem->beta > 0 && problem->rmax > problem->rin))
+    return PANGU_EINVAL;
+  return RUN(run_generate, e, job, *problem, base, S(stream));
 }
 
 int pangu_flux_config(const pangu_engine *e, int32_t out[7]) {

@@ -86,6 +86,7 @@ struct pangu_engine {
   long long *d_xdst = nullptr, *d_xsrc = nullptr;  // [capacity x ghost cells per block]
   long long nxch = 0, xch_cap = 0;
   int *d_tmp_slots = nullptr;  // [capacity] slots of a job being attached
+  unsigned long long *d_genred = nullptr;  // [3] maxima of the device generators
   unsigned long long *d_cnt = nullptr;  // [max_jobs][PANGU_NCOUNTERS]
   int *d_fail_count = nullptr;      // C2P retry list (Scheme2D failures)
   long long *d_fail_list = nullptr;

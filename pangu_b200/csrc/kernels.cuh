@@ -1408,6 +1408,185 @@ __global__ void k_update_dt(int njobs, const int *jr, double *dt, const double *
 }
 
 // ---------------------------------------------------------------------------
+// Device-side initial conditions of the benchmark problems, the same
+// formulas as pangu_b200/problems.py (Orszag-Tang, Brio-Wu, and the
+// Fishbone-Moncrief torus of problem_generator.cpp:103-558 with its
+// MeshPostInitialization), so that jobs can start on the device.
+// ---------------------------------------------------------------------------
+struct GenArgs {
+  int kind;
+  unsigned long long seed;
+  double rin, rmax, kappa, pert, beta, cut;
+  double l, lnh_in;  // torus constants computed on the host
+};
+
+// SplitMix64 (Steele, Lea and Flood 2014) of seed * golden + idx, mapped to
+// [-1, 1) from its top 53 bits; problems.hash_uniform gives the same values.
+__device__ __forceinline__ double hash_uniform(unsigned long long seed, unsigned long long idx) {
+  const unsigned long long gold = 0x9E3779B97F4A7C15ull;
+  unsigned long long z = seed * gold + idx;
+  z += gold;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  return 2.0 * ((double)(z >> 11) * 0x1p-53) - 1.0;
+}
+
+__device__ __forceinline__ void atomic_max_pos(unsigned long long *m, double v) {
+  if (v > 0.0) atomicMax(m, (unsigned long long)__double_as_longlong(v));
+}
+
+// Every cell of the job's blocks (ghosts included, as the host generator
+// fills them). red[0], red[1]: torus maxima of rho and u before normalising.
+template <int MT>
+__global__ void __launch_bounds__(kThreads) k_gen_cells(Dims d, pangu_params p, GenArgs ga, PT *P,
+                                                        unsigned long long *red) {
+  int bb, k, j, i;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (!box_index(t, d.NB, 0, d.N3 - 1, 0, d.N2 - 1, 0, d.N1 - 1, bb, k, j, i)) return;
+  const int b = slot_of(d, bb);
+  const double gam = p.adiabatic_index;
+  double pr[NPRIM] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const double pi = 3.141592653589793;
+  if (ga.kind == PANGU_PROBLEM_ORSZAG_TANG) {
+    const double x = xc(d, b, 0, i), y = xc(d, b, 1, j);
+    const double vx = -0.5 * sin(2 * pi * y), vy = 0.5 * sin(2 * pi * x);
+    const double W = 1.0 / sqrt(1.0 - vx * vx - vy * vy);
+    pr[RHO] = 25.0 / (36.0 * pi);
+    pr[ENY] = 5.0 / (12.0 * pi) / (gam - 1.0);
+    pr[UX1] = W * vx;
+    pr[UX2] = W * vy;
+    pr[BX1] = -sin(2 * pi * y) / sqrt(4 * pi);
+    pr[BX2] = sin(4 * pi * x) / sqrt(4 * pi);
+    pr[ENT] = (gam - 1.0) * pr[ENY] * PGK_POW(pr[RHO], -gam);
+  } else if (ga.kind == PANGU_PROBLEM_BRIO_WU) {
+    const bool left = xc(d, b, 0, i) < 0;
+    pr[RHO] = left ? 1.0 : 0.125;
+    pr[ENY] = (left ? 1.0 : 0.1) / (gam - 1.0);
+    pr[BX1] = 0.5;
+    pr[BX2] = left ? 1.0 : -1.0;
+    pr[ENT] = (gam - 1.0) * pr[ENY] * PGK_POW(pr[RHO], -gam);
+  } else if (MT == MKS) {
+    const int W1 = d.N1 + 1, W2 = d.N2 + 1;
+    const double *T1 = d.t1 + (long long)b * kT1Rows * W1;
+    const double *T2 = d.t2 + (long long)b * 12 * W2;
+    const double r = T1[i], sth = T2[j], cth = T2[W2 + j];
+    const double a = p.a, a2 = a * a, l = ga.l;
+    const double DD = r * r - 2.0 * r + a2;
+    const double AA = (r * r + a2) * (r * r + a2) - DD * a2 * sth * sth;
+    const double SS = r * r + a2 * cth * cth;
+    double lnh = 0.5 * log((1.0 + sqrt(1.0 + 4.0 * (l * l * SS * SS) * DD /
+                                        (AA * sth * AA * sth))) / (SS * DD / AA)) -
+                 0.5 * sqrt(1.0 + 4.0 * (l * l * SS * SS) * DD / (AA * AA * sth * sth)) -
+                 2.0 * a * r * l / AA - ga.lnh_in;
+    if (!(r >= ga.rin)) lnh = 1.0;
+    const double hm1 = exp(lnh) - 1.0;
+    const bool inside = lnh >= 0.0 && r >= ga.rin && hm1 > 0.0;
+    if (inside) {
+      const double rho = PGK_POW(hm1 * (gam - 1.0) / (ga.kappa * gam), 1.0 / (gam - 1.0));
+      const long long cell = ((long long)bb * d.N3 + k) * d.N2 * d.N1 + (long long)j * d.N1 + i;
+      const double rnd = hash_uniform(ga.seed, (unsigned long long)cell);
+      const double eint = ga.kappa * PGK_POW(rho, gam) / (gam - 1.0) * (1.0 + ga.pert * rnd);
+      const double ent = (gam - 1.0) * eint * PGK_POW(rho, -gam);
+      const double expm2chi = SS * SS * DD / (AA * AA * sth * sth);
+      const double up1 = sqrt((-1.0 + sqrt(1.0 + 4.0 * l * l * expm2chi)) / 2.0);
+      const double up_bl = 2.0 * a * r * sqrt(1.0 + up1 * up1) / sqrt(AA * SS * DD) +
+                           sqrt(SS / AA) * up1 / sth;
+      // Boyer-Lindquist metric entries g_00, g_03, g_33 (BL.h; the code
+      // Jacobian leaves them unchanged)
+      const double r2 = r * r, sth2 = sth * sth;
+      const double mu = 1.0 + a2 * cth * cth / r2;
+      const double irm = 1.0 / (r * mu);
+      const double g00 = -1.0 + 2.0 * irm, g03 = -2.0 * a * sth2 * irm;
+      const double g33 = r2 * sth2 * (1.0 + a2 / r2 + 2.0 * a2 * sth2 / (r * r2 * mu));
+      const double AAq = g00, BBq = 2.0 * g03 * up_bl, CCq = 1.0 + g33 * up_bl * up_bl;
+      const double u0 = (-BBq - sqrt(BBq * BBq - 4.0 * AAq * CCq)) / (2.0 * AAq);
+      // BL -> KS -> code: u^r_BL = 0 leaves (u0, 0, 0, up); the weighted
+      // velocity adds the shift beta^i = gcon^{0i} alpha^2 (KS code metric)
+      Geo g;
+      cell_metric<MT>(d, p, b, k, j, i, g);
+      const double al2 = g.alpha * g.alpha;
+      pr[RHO] = rho;
+      pr[ENY] = eint;
+      pr[UX1] = g.gcon[0][1] * al2 * u0;
+      pr[UX2] = g.gcon[0][2] * al2 * u0;
+      pr[UX3] = up_bl + g.gcon[0][3] * al2 * u0;
+      pr[ENT] = ent;
+      atomic_max_pos(&red[0], rho);
+      atomic_max_pos(&red[1], eint);
+    }
+  }
+  pr[KEL] = p.fel_0 * pr[ENT];
+  const long long q = vidx(d, b, 0, k, j, i);
+#pragma unroll
+  for (int v = 0; v < NPRIM; ++v)
+    if (d.pidx[v] >= 0) P[q + d.pidx[v] * d.ncell] = (PT)pr[v];
+}
+
+// Torus: density and energy divided by the maximum density (all cells).
+__global__ void __launch_bounds__(kThreads) k_gen_normalize(Dims d, PT *P,
+                                                            const unsigned long long *red) {
+  int bb, k, j, i;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (!box_index(t, d.NB, 0, d.N3 - 1, 0, d.N2 - 1, 0, d.N1 - 1, bb, k, j, i)) return;
+  const int b = slot_of(d, bb);
+  const double rhomax = __longlong_as_double((long long)red[0]);
+  const long long q = vidx(d, b, 0, k, j, i);
+  P[q] = (PT)((double)P[q] / rhomax);
+  P[q + d.ncell] = (PT)((double)P[q + d.ncell] / rhomax);
+}
+
+// Torus field (interior cells): A_phi = max(<rho> - cut, 0) at cell corners,
+// B = curl A / sqrt|g| by centred differences, and the maximum of b^2.
+template <int MT>
+__global__ void __launch_bounds__(kThreads) k_gen_bfield(Dims d, pangu_params p, GenArgs ga, PT *P,
+                                                         unsigned long long *red) {
+  int bb, k, j, i;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, bb, k, j, i)) return;
+  const int b = slot_of(d, bb);
+  const long long q = vidx(d, b, 0, k, j, i);
+  auto rho = [&](int jj, int ii) -> double { return P[q + (long long)(jj - j) * d.N1 + (ii - i)]; };
+  auto corner = [&](int jj, int ii) -> double {
+    const double avg = 0.25 * (((rho(jj, ii) + rho(jj, ii - 1)) + rho(jj - 1, ii)) + rho(jj - 1, ii - 1));
+    const double v = avg - ga.cut;
+    return v > 0.0 ? v : 0.0;
+  };
+  const double a00 = corner(j - 1, i - 1), a01 = corner(j, i - 1), a10 = corner(j - 1, i),
+               a11 = corner(j, i);
+  Geo g;
+  cell_metric<MT>(d, p, b, k, j, i, g);
+  const double b1 = -(((a00 - a01) + a10) - a11) / ((2.0 * dx_of(d, b, 1)) * g.sg);
+  const double b2 = (((a00 + a01) - a10) - a11) / ((2.0 * dx_of(d, b, 0)) * g.sg);
+  P[q + d.pidx[BX1] * d.ncell] = (PT)b1;
+  P[q + d.pidx[BX2] * d.ncell] = (PT)b2;
+  double pc[NPRIM];
+  load_prim(d, P, b, k, j, i, pc);
+  State st;
+  calc_state<MT>(pc, g, st);
+  atomic_max_pos(&red[2], st.bsq);
+}
+
+// Torus field normalised to the target plasma beta (interior cells).
+__global__ void __launch_bounds__(kThreads) k_gen_scale(Dims d, double gam, double beta,
+                                                        PT *P, const unsigned long long *red) {
+  int bb, k, j, i;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, bb, k, j, i)) return;
+  const int b = slot_of(d, bb);
+  const double rhomax = __longlong_as_double((long long)red[0]);
+  const double umax = __longlong_as_double((long long)red[1]);
+  const double bsq_max = __longlong_as_double((long long)red[2]);
+  const double beta_min = 2.0 * (gam - 1.0) * (umax / rhomax) / (bsq_max + 1.0e-30);
+  const double norm = sqrt(beta_min / beta);
+  const long long q = vidx(d, b, 0, k, j, i);
+  for (int v = BX1; v <= BX3; ++v) {
+    const long long o = q + d.pidx[v] * d.ncell;
+    P[o] = (PT)((double)P[o] * norm);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // launch helpers
 // ---------------------------------------------------------------------------
 inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -1776,6 +1955,82 @@ int run_job_start(pangu_engine *e, int job, const pangu_pack *base, const pangu_
       return PANGU_ECUDA;
   }
   return PANGU_OK;
+}
+
+// problem_generator.cpp:22-35 (angular momentum of the torus at rmax).
+inline double lfish_calc(double r, double a) {
+  const double sr = std::sqrt(r);
+  return (((a * a - 2.0 * a * sr + r * r) *
+           ((-2.0 * a * r * (a * a - 2.0 * a * sr + r * r)) /
+                std::sqrt(2.0 * a * sr + (-3.0 + r) * r) +
+            ((a + (-2.0 + r) * sr) * (r * r * r + a * a * (2.0 + r))) /
+                std::sqrt(1 + (2.0 * a) / std::pow(r, 1.5) - 3.0 / r))) /
+          (r * r * r * std::sqrt(2.0 * a * sr + (-3.0 + r) * r) * (a * a + (-2.0 + r) * r)));
+}
+
+// Initial primitives of a job written into its blocks of base, on stream s;
+// synchronises s to check that a torus has a bound region.
+int run_generate(pangu_engine *e, int job, const pangu_problem &pb, const pangu_pack *base,
+                 cudaStream_t s) {
+  const PoolJob &J = e->jobs[job];
+  const pangu_params &p = J.p;
+  const bool torus = pb.kind == PANGU_PROBLEM_FM_TORUS;
+  if (torus && p.metric_type != PANGU_METRIC_MKS) return PANGU_EINVAL;
+  int first = 0;
+  for (int q = 0; q < job; ++q)
+    if (e->jobs[q].live) first += (int)e->jobs[q].slots.size();
+  Dims dj = e->d;
+  dj.slot = e->d_active + first;
+  dj.NB = (int)J.slots.size();
+  GenArgs ga{};
+  ga.kind = pb.kind;
+  ga.seed = (unsigned long long)pb.seed;
+  ga.rin = pb.rin;
+  ga.rmax = pb.rmax;
+  ga.kappa = pb.kappa;
+  ga.pert = pb.perturbation;
+  ga.beta = pb.beta;
+  ga.cut = pb.aphi_rho_cut;
+  if (torus) {
+    const double a = p.a, a2 = a * a, rin = pb.rin;
+    const double l = lfish_calc(pb.rmax, a);
+    const double sthin = std::sin(M_PI / 2), cthin = std::cos(M_PI / 2);
+    const double DDin = rin * rin - 2.0 * rin + a2;
+    const double AAin = (rin * rin + a2) * (rin * rin + a2) - DDin * a2 * sthin * sthin;
+    const double SSin = rin * rin + a2 * cthin * cthin;
+    ga.l = l;
+    ga.lnh_in = 0.5 * std::log((1.0 + std::sqrt(1.0 + 4.0 * (l * l * SSin * SSin) * DDin /
+                                                   (AAin * AAin * sthin * sthin))) /
+                               (SSin * DDin / AAin)) -
+                0.5 * std::sqrt(1.0 + 4.0 * (l * l * SSin * SSin) * DDin /
+                                    (AAin * AAin * sthin * sthin)) -
+                2.0 * a * rin * l / AAin;
+  }
+  if (cudaMemsetAsync(e->d_genred, 0, 3 * sizeof(unsigned long long), s) != cudaSuccess)
+    return PANGU_ECUDA;
+  const Dims &d = dj;
+  const long long ne = (long long)d.NB * d.ncell;
+  const long long ni = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
+  PT *P = prim_of(base);
+  DISPATCH_MT(p.metric_type, k_gen_cells, grid_for(ne), s, d, p, ga, P, e->d_genred);
+  ++e->launches;
+  if (torus) {
+    k_gen_normalize<<<grid_for(ne), kThreads, 0, s>>>(d, P, e->d_genred);
+    ++e->launches;
+    if (p.enable_B) {
+      k_gen_bfield<MKS><<<grid_for(ni), kThreads, 0, s>>>(d, p, ga, P, e->d_genred);
+      k_gen_scale<<<grid_for(ni), kThreads, 0, s>>>(d, p.adiabatic_index, pb.beta, P,
+                                                    e->d_genred);
+      e->launches += 2;
+    }
+    unsigned long long rhomax = 0;
+    if (check_launch() || cudaMemcpyAsync(&rhomax, e->d_genred, 8, cudaMemcpyDeviceToHost, s) !=
+                              cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+      return PANGU_ECUDA;
+    if (rhomax == 0) return PANGU_EINVAL;  // no bound torus for these parameters
+  }
+  return check_launch();
 }
 
 }  // namespace PGK_NS

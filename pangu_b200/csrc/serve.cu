@@ -53,7 +53,9 @@ struct SJob {
   pangu_mesh mesh{};
   double a = 0, h = 0, dt_init = 0, arrival = 0;
   long long cycles = 0, done_cycles = 0;
-  std::vector<double> prim;  // initial state, then the result
+  std::vector<double> prim;  // initial state (unless generated), then the result
+  bool generated = false;    // initial state generated on the device
+  pangu_problem problem{};
   int state = 0;             // 0 waiting, 1 running, 2 done
   int job = -1;
   std::vector<int32_t> slots;
@@ -136,6 +138,13 @@ int admit(SClass &c, SJob &j) {
   std::vector<float> tmp;
   for (long long b = 0; b < nb; ++b) {
     const int sl = j.slots[b];
+    if (j.generated) {
+      if (cudaMemsetAsync(c.a.base.cons + (size_t)sl * blk, 0, blk * 8, c.stream) != cudaSuccess ||
+          cudaMemsetAsync(c.a.base.flag + (size_t)sl * c.ncell, 0, c.ncell * 8, c.stream) !=
+              cudaSuccess)
+        return PANGU_ECUDA;
+      continue;
+    }
     const double *src = j.prim.data() + b * blk;
     char *dst = (char *)c.a.base.prim + (size_t)sl * blk * c.prim_bytes;
     cudaError_t ec;
@@ -154,6 +163,7 @@ int admit(SClass &c, SJob &j) {
   if (cudaMemcpyAsync(c.a.dt + job, &j.dt_init, 8, cudaMemcpyHostToDevice, c.stream) !=
       cudaSuccess)
     return PANGU_ECUDA;
+  if (j.generated && (rc = pangu_generate(c.e, job, &j.problem, &c.a.base, c.stream))) return rc;
   rc = pangu_job_start(c.e, job, &c.a.base, &c.a.one, c.stream);
   if (rc) return rc;
   c.dirty = true;
@@ -165,6 +175,7 @@ int admit(SClass &c, SJob &j) {
 // Needs the class idle.
 int retire(SClass &c, SJob &j) {
   const size_t blk = (size_t)c.nf * c.ncell;
+  j.prim.resize(j.slots.size() * blk);
   std::vector<float> tmp(c.prim_bytes == 4 ? blk : 0);
   for (size_t b = 0; b < j.slots.size(); ++b) {
     const char *src = (const char *)c.a.base.prim + (size_t)j.slots[b] * blk * c.prim_bytes;
@@ -291,6 +302,33 @@ int pangu_server_submit(pangu_server *s, int32_t cls, const pangu_mesh *mesh, do
   j.cycles = cycles;
   j.arrival = arrival_s;
   j.prim.assign(prim_host, prim_host + (size_t)nb * c.nf * c.ncell);
+  *ticket_out = (int32_t)s->jobs.size();
+  s->jobs.push_back(std::move(j));
+  return PANGU_OK;
+}
+
+int pangu_server_submit_problem(pangu_server *s, int32_t cls, const pangu_mesh *mesh, double a,
+                                double h, double dt_init, int64_t cycles, double arrival_s,
+                                const pangu_problem *problem, int32_t *ticket_out) {
+  if (!s || !mesh || !problem || !ticket_out || cls < 0 || cls >= (int)s->classes.size() ||
+      cycles < 1)
+    return PANGU_EINVAL;
+  const SClass &c = s->classes[cls];
+  if (mesh->nx1 != c.block.nx1 || mesh->nx2 != c.block.nx2 || mesh->nx3 != c.block.nx3 ||
+      mesh->ng != c.block.ng)
+    return PANGU_EINVAL;
+  const long long nb = (long long)mesh->nbx1 * mesh->nbx2 * mesh->nbx3;
+  if (nb < 1 || nb > c.capacity) return PANGU_ETOOBIG;
+  SJob j;
+  j.cls = cls;
+  j.mesh = *mesh;
+  j.a = a;
+  j.h = h;
+  j.dt_init = dt_init;
+  j.cycles = cycles;
+  j.arrival = arrival_s;
+  j.generated = true;
+  j.problem = *problem;
   *ticket_out = (int32_t)s->jobs.size();
   s->jobs.push_back(std::move(j));
   return PANGU_OK;

@@ -80,6 +80,10 @@ def lib():
     L.pangu_job_counters.argtypes = [_P, C.c_int32, C.POINTER(C.c_uint64)]
     L.pangu_active_blocks.argtypes = [_P]
     L.pangu_autotune.argtypes = [_P, _PK, _P]
+    L.pangu_generate.argtypes = [_P, C.c_int32, C.POINTER(abi.Problem), _PK, _P]
+    L.pangu_server_submit_problem.argtypes = [_P, C.c_int32, C.POINTER(abi.Mesh), C.c_double,
+                                              C.c_double, C.c_double, C.c_int64, C.c_double,
+                                              C.POINTER(abi.Problem), C.POINTER(C.c_int32)]
     L.pangu_flux_config.argtypes = [_P, C.POINTER(C.c_int32)]
     L.pangu_server_create.argtypes = [C.c_uint64, C.POINTER(_P)]
     L.pangu_server_destroy.argtypes = [_P]
@@ -238,6 +242,11 @@ class Engine:
         """Picks the flux kernels' tile shapes by timing them on md's data."""
         _check(self.L.pangu_autotune(self.h, md.pack, self.stream()), "pangu_autotune")
 
+    def generate(self, job, problem: abi.Problem, base):
+        """Initial primitives of a job generated on the device into base."""
+        _check(self.L.pangu_generate(self.h, job, C.byref(problem), base.pack, self.stream()),
+               "pangu_generate")
+
     def flux_config(self) -> dict:
         out = (C.c_int32 * 7)()
         _check(self.L.pangu_flux_config(self.h, out), "pangu_flux_config")
@@ -306,6 +315,14 @@ class Simulation:
         torch = _torch()
         src = torch.as_tensor(prim, device=self.engine.device)
         self.base.prim.copy_(src.to(self.base.prim.dtype))
+        self.engine.job_start(0, self.base, self.one)
+
+    def generate(self, name: str):
+        """Initial state of the named problem (ot, bw, torus) generated on the
+        device from this job's inputfile, then the initial ghost fill."""
+        from .problems import problem_struct
+        self.base.prim.zero_()
+        self.engine.generate(0, problem_struct(name, self.pin), self.base)
         self.engine.job_start(0, self.base, self.one)
 
     def stage(self, st: int, dt_est=None):
@@ -403,6 +420,26 @@ class Pool:
         self.base.cons.index_fill_(0, idx, 0.0)
         self.base.flag.index_fill_(0, idx, 0.0)
         self.dt[job] = pin.get_or_add_real("parthenon/time", "dt_init", 1e-5)
+        self.engine.job_start(job, self.base, self.one)
+        self.jobs[job] = slots
+        self._graph = None
+        return job
+
+    def attach_problem(self, pin: ParameterInput, name: str) -> int:
+        """Attaches a job whose initial state is generated on the device."""
+        from .problems import problem_struct
+        torch = _torch()
+        p = params_struct(process_packages(pin))
+        p.precision = engine_precision(pin)
+        self._check_compatible(p)
+        torch.cuda.synchronize(self.engine.device)  # no pool work in flight
+        job, slots = self.engine.attach(mesh_struct(pin), p.a, p.h)
+        idx = torch.tensor(slots, dtype=torch.long, device=self.engine.device)
+        for arr in (self.base.prim, self.base.cons):
+            arr.index_fill_(0, idx, 0.0)
+        self.base.flag.index_fill_(0, idx, 0.0)
+        self.dt[job] = pin.get_or_add_real("parthenon/time", "dt_init", 1e-5)
+        self.engine.generate(job, problem_struct(name, pin), self.base)
         self.engine.job_start(job, self.base, self.one)
         self.jobs[job] = slots
         self._graph = None
@@ -514,6 +551,27 @@ class Server:
                                           arr.ctypes.data_as(C.c_void_p), C.byref(t)),
                "pangu_server_submit")
         self.tickets[t.value] = (cls, arr.shape[0])
+        return t.value
+
+    def submit_problem(self, cls: int, pin: ParameterInput, name: str, cycles: int,
+                       arrival_s: float) -> int:
+        """A job whose initial state the server generates on the device at
+        admission (no host upload)."""
+        from .problems import problem_struct
+        params, _, nf, shape = self.classes[cls]
+        p = params_struct(process_packages(pin))
+        p.precision = engine_precision(pin)
+        for name_, _ in abi.Params._fields_:
+            if name_ not in Pool.PER_JOB and getattr(p, name_) != getattr(params, name_):
+                raise EngineError(f"job parameter {name_} differs from the class's")
+        mesh = mesh_struct(pin)
+        pb = problem_struct(name, pin)
+        dt_init = pin.get_or_add_real("parthenon/time", "dt_init", 1e-5)
+        t = C.c_int32()
+        _check(self.L.pangu_server_submit_problem(self.h, cls, C.byref(mesh), p.a, p.h, dt_init,
+                                                  int(cycles), float(arrival_s), C.byref(pb),
+                                                  C.byref(t)), "pangu_server_submit_problem")
+        self.tickets[t.value] = (cls, mesh.nbx1 * mesh.nbx2 * mesh.nbx3)
         return t.value
 
     def run(self):

@@ -12,7 +12,7 @@ CPU oracle step from the same arrays.
   (rho, p) = (1, 1) | (0.125, 0.1), Bx = 0.5, By = +1 | -1.
 * ``fm_torus``: Fishbone-Moncrief torus in MKS coordinates, restating
   pangu/problem/fm_torus_mks/problem_generator.cpp:103-558 (ProblemGenerator
-  and MeshPostInitialization) with a seeded numpy generator in place of
+  and MeshPostInitialization) with a seeded counter-based generator in place of
   Kokkos::Random_XorShift64_Pool (whose draw order is not reproducible).
 """
 from __future__ import annotations
@@ -290,6 +290,23 @@ def _state_bsq(P, S, gcov, gcon):
     return np.einsum("...i,...i->...", bcon, bcov)
 
 
+def hash_uniform(seed: int, b: int, shape) -> np.ndarray:
+    """Counter-based uniform numbers in [-1, 1) for the cells of block b:
+    SplitMix64 (Steele, Lea and Flood 2014) of seed * golden + cell index,
+    top 53 bits. The device generator (kernels.cuh) computes the same values,
+    so both give the same perturbation for the same seed."""
+    n = int(np.prod(shape))
+    gold = np.uint64(0x9E3779B97F4A7C15)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) * gold + (np.uint64(b) * np.uint64(n) + np.arange(n, dtype=np.uint64))
+        z = z + gold
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    u = (z >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+    return (2.0 * u - 1.0).reshape(shape)
+
+
 def fm_torus(geo: Geometry, packages, pin: ParameterInput) -> np.ndarray:
     c = packages["core"].params
     m = packages["metric"].params
@@ -304,7 +321,6 @@ def fm_torus(geo: Geometry, packages, pin: ParameterInput) -> np.ndarray:
     beta_target = pin.get_or_add_real("fm_torus", "beta", 100.0)
     cut = pin.get_or_add_real("fm_torus", "aphi_rho_cut", 0.2)
     seed = pin.get_or_add_integer("fm_torus", "seed", 0)
-    rng = np.random.default_rng(seed)
     a2 = a * a
     l = _lfish_calc(rmax, a)
     sthin, cthin = math.sin(math.pi / 2), math.cos(math.pi / 2)
@@ -341,7 +357,7 @@ def fm_torus(geo: Geometry, packages, pin: ParameterInput) -> np.ndarray:
             hm1 = np.exp(lnh) - 1.0
             inside &= hm1 > 0.0
             rho = np.where(inside, (hm1 * (gam - 1.0) / (kappa * gam)) ** (1.0 / (gam - 1.0)), 0.0)
-        rnd = rng.uniform(-1.0, 1.0, size=geo.shape)
+        rnd = hash_uniform(seed, b, geo.shape)
         eint = np.where(inside, kappa * rho ** gam / (gam - 1.0), 0.0) * (1.0 + pert * rnd)
         eint = np.where(inside, eint, 0.0)
         with np.errstate(all="ignore"):
@@ -406,6 +422,20 @@ def fm_torus(geo: Geometry, packages, pin: ParameterInput) -> np.ndarray:
         for key in ("b1", "b2", "b3"):
             P[b, S[key]][inter] *= norm
     return P
+
+
+def problem_struct(name: str, pin: ParameterInput) -> abi.Problem:
+    """The device generator's description of a named problem (pangu_generate):
+    kind plus the <fm_torus> parameters of a torus."""
+    pb = abi.Problem()
+    pb.kind = abi.PROBLEM[name]
+    if pb.kind == abi.PROBLEM["torus"]:
+        g = lambda k, v: pin.get_or_add_real("fm_torus", k, v)  # noqa: E731
+        pb.rin, pb.rmax, pb.kappa = g("rin", 6.0), g("rmax", 12.0), g("kappa", 1.0e-3)
+        pb.perturbation, pb.beta = g("perturbation", 4.0e-2), g("beta", 100.0)
+        pb.aphi_rho_cut = g("aphi_rho_cut", 0.2)
+        pb.seed = pin.get_or_add_integer("fm_torus", "seed", 0)
+    return pb
 
 
 def make_problem(name: str, **kw):

@@ -35,6 +35,8 @@ def structs():
     out = {"pangu_params": abi.Params, "pangu_mesh": abi.Mesh, "pangu_pack": abi.Pack}
     if hasattr(abi, "ServerStats"):
         out["pangu_server_stats"] = abi.ServerStats
+    if hasattr(abi, "Problem"):
+        out["pangu_problem"] = abi.Problem
     return out
 
 
