@@ -364,6 +364,37 @@ class Simulation:
     def primitives(self) -> np.ndarray:
         return self.base.prim.double().cpu().numpy()
 
+    def save(self, path: str):
+        """Checkpoint of the job between cycles, as one .npz: everything the
+        next cycle reads -- both containers' primitives (container "1" holds
+        the stale guesses of C2P) and conserved variables (the mixed form
+        carries its magnetic field in them), the flags (FixRecovery reads
+        ghost flags exchanged in the previous stage), dt and the cycle count --
+        with the inputfile text."""
+        torch = _torch()
+        torch.cuda.synchronize(self.engine.device)
+        np.savez(path, base_prim=self.base.prim.cpu().numpy(),
+                 one_prim=self.one.prim.cpu().numpy(), base_cons=self.base.cons.cpu().numpy(),
+                 one_cons=self.one.cons.cpu().numpy(), flag=self.base.flag.cpu().numpy(),
+                 dt=self.dt.cpu().numpy(), cycle=np.int64(self.cycle),
+                 inputfile=np.array(self.pin.dump()))
+
+    @classmethod
+    def restart(cls, path: str, device=0) -> "Simulation":
+        """A job continued from a checkpoint written by save(): its next
+        cycles give the same bits as the uninterrupted run."""
+        torch = _torch()
+        ck = np.load(path)
+        sim = cls(ParameterInput(str(ck["inputfile"])), device=device)
+        dev = sim.engine.device
+        for name in ("base_prim", "one_prim", "base_cons", "one_cons"):
+            cont, field = name.split("_")
+            getattr(getattr(sim, cont), field).copy_(torch.as_tensor(ck[name], device=dev))
+        sim.base.flag.copy_(torch.as_tensor(ck["flag"], device=dev))
+        sim.dt.copy_(torch.as_tensor(ck["dt"], device=dev))
+        sim.cycle = int(ck["cycle"])
+        return sim
+
 
 class Pool:
     """Many jobs of one block shape and parameter set (metric spin a and h may

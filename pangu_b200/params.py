@@ -75,6 +75,16 @@ class ParameterInput:
     def get_or_add_boolean(self, block, key, default: bool) -> bool:
         return self._get_or_add(block, key, bool(default), _parse_bool)
 
+    def dump(self) -> str:
+        """The parameters as inputfile text (blocks and key = value lines);
+        ParameterInput(p.dump()) gives the same parameters back."""
+        out = []
+        for block, kv in self.blocks.items():
+            out.append(f"<{block}>")
+            out += [f"{k} = {v}" for k, v in kv.items()]
+            out.append("")
+        return "\n".join(out)
+
     def check_required(self, block, key) -> None:
         if not self.has(block, key):
             raise ValueError(f"<{block}>/{key} is required")

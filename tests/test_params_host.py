@@ -106,3 +106,13 @@ def test_mesh_errors():
     pin = prm.ParameterInput(INPUT.replace("ix1_bc = outflow", ""))
     with pytest.raises(ValueError):
         prm.mesh_struct(pin)
+
+
+def test_inputfile_dump_round_trip():
+    pin = prm.ParameterInput(INPUT)
+    pin.set("b200", "precision", "mixed")
+    again = prm.ParameterInput(pin.dump())
+    assert again.blocks == pin.blocks
+    p1 = prm.params_struct(prm.process_packages(pin))
+    p2 = prm.params_struct(prm.process_packages(again))
+    assert bytes(p1) == bytes(p2)
