@@ -872,6 +872,45 @@ __device__ __forceinline__ void source_cell(const Dims &d, const pangu_params &p
                                             double bdt) {
   if (MT == MINKOWSKI) return;  // connection identically zero (christoffel.h:90)
   const double sg = g.sg;
+#if PGK_MIXED
+  if (MT == MKS || MT == BL) {
+    // Mixed form: T^r_c Gamma^c_{dir r} evaluated in FT from the FP32
+    // primitives and the tabulated FP64 metric rounded once; the increment is
+    // accumulated into the FP64 conserved variables.
+    constexpr TabLayout L = tab_layout(MT);
+    const long long vs = d.ncell, q0 = vidx(d, b, 0, k, j, i);
+    FT pf[NPRIM];
+#pragma unroll
+    for (int v = 0; v < NPRIM; ++v) pf[v] = d.pidx[v] >= 0 ? P[q0 + d.pidx[v] * vs] : FT(0);
+    GeoT<FT> gf;
+    geo_cast<MT>(g, gf);
+    StateT<FT> sf;
+    calc_state_t<MT>(pf, gf, sf);
+    const FT gam = (FT)p.adiabatic_index;
+    const FT hh = pf[RHO] + gam * pf[ENY];
+    const FT e_tot = hh + sf.bsq;
+    const FT p_tot = (gam - FT(1)) * pf[ENY] + FT(0.5) * sf.bsq;
+    const long long plane = (long long)d.N2 * d.N1;
+    const double *cn = d.ctab + (long long)b * L.ncen * plane + (long long)j * d.N1 + i +
+                       (long long)L.nmet * plane;
+#pragma unroll
+    for (int dir = 0; dir < 4; ++dir) {
+      FT con = FT(0);
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+          if (L.conn[c][dir][r] >= 0) {
+            const FT T = e_tot * sf.ucon[r] * sf.ucov[c] + p_tot * FT(r == c) -
+                         sf.bcon[r] * sf.bcov[c];
+            con += T * (FT)__ldg(cn + L.conn[c][dir][r] * plane);
+          }
+      const int v = dir == 0 ? d.pidx[ENY] : d.pidx[UX1] + dir - 1;
+      U[q0 + v * vs] += (double)con * sg * bdt;
+    }
+    return;
+  }
+#endif
   double pc[NPRIM];
   load_prim(d, P, b, k, j, i, pc);
   State s;
