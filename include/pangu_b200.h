@@ -67,9 +67,9 @@ extern "C" {
 #define PANGU_HEAT_SHARMA 5
 /* Arithmetic of the engine (no reference counterpart; the reference is
  * FP64 throughout). MIXED stores primitives in FP32 (the pack's prim pointer
- * then addresses floats) and runs reconstruction, Riemann flux and electron
- * heating in FP32; conserved variables, the update, the source term, C2P, the
- * metric and CT stay FP64. The conserved magnetic field is then evolved only
+ * then addresses floats) and runs reconstruction, Riemann flux, electron
+ * heating and the geometric source term (MKS/BL) in FP32; conserved variables
+ * and their update, C2P, the metric and CT stay FP64. The conserved magnetic field is then evolved only
  * by the FP64 CT update: CalculateConservative leaves it unchanged, and
  * pangu_job_start computes it once from the initial primitives. */
 #define PANGU_PRECISION_FP64 0

@@ -1,7 +1,8 @@
 // engine_mixed.cu -- the mixed-precision instantiation of the engine's
 // kernels (namespace pgkmx): primitives stored in FP32; reconstruction,
-// Riemann fluxes and electron heating in FP32; conserved variables, the flux
-// divergence update, the geometric source, C2P, the metric and CT in FP64.
+// Riemann fluxes, electron heating and the geometric source term in FP32;
+// conserved variables and the flux divergence update, C2P, the metric and CT
+// in FP64.
 // Built with FMA contraction on and the CUDA math library's pow/exp/log
 // (the exact build, engine.cu, keeps --fmad=false and correctly rounded
 // functions for bit-exact parity). The device helpers are compiled under

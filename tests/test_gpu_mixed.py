@@ -1,5 +1,6 @@
 """Mixed-precision form: FP32 primitives, reconstruction, Riemann flux and
-electron heating; FP64 conserved update, source, C2P, metric and CT.
+electron heating and the geometric source term; FP64 conserved variables and
+update, C2P, metric and CT.
 
 Errors are measured against the FP64 engine (bit-identical to the CPU
 oracle) on the same inputs. Tolerances (relative L1 per field after the
