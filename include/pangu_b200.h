@@ -330,7 +330,7 @@ int pangu_generate(pangu_engine *e, int32_t job, const pangu_problem *problem,
  * running it alone. */
 typedef struct pangu_server pangu_server;
 typedef struct pangu_server_stats {
-  int64_t jobs, ticks;
+  int64_t jobs, ticks;      /* completed jobs; class ticks                   */
   double wall_s;             /* host time of the whole run                   */
   double zone_cycles;        /* interior cells x cycles, summed over jobs    */
   double zone_cycles_per_s;  /* zone_cycles / wall_s                         */
@@ -362,6 +362,12 @@ int pangu_server_run(pangu_server *s);
 int pangu_server_result(pangu_server *s, int32_t ticket, double *prim_out,
                         double *times_out, uint64_t counters_out[PANGU_NCOUNTERS]);
 int pangu_server_get_stats(const pangu_server *s, pangu_server_stats *out);
+/* Cancels a job at at_s seconds after the start of the next run: a job still
+ * waiting is dropped; a running one is detached at its class's next tick
+ * boundary, with no result. Stats count completed jobs only. */
+int pangu_server_cancel(pangu_server *s, int32_t ticket, double at_s);
+/* 0 waiting, 1 running, 2 done, 3 cancelled (or a negative error). */
+int pangu_server_job_state(const pangu_server *s, int32_t ticket);
 
 #ifdef __cplusplus
 }

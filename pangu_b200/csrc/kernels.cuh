@@ -6,8 +6,18 @@
 #error "define PGK_NS before including kernels.cuh"
 #endif
 
+#include <nvtx3/nvToolsExt.h>
+
 namespace PGK_NS {
 using namespace pgd;
+
+// An NVTX range per task of the stage, named as the reference's tasks (the
+// counterpart of PARTHENON_INSTRUMENT, e.g. laxf.cc:21); free when no
+// profiler is attached.
+struct TaskRange {
+  explicit TaskRange(const char *name) { nvtxRangePushA(name); }
+  ~TaskRange() { nvtxRangePop(); }
+};
 
 // Storage type of the primitives and arithmetic type of reconstruction and
 // Riemann flux: FP64 in the exact build, FP32 in the mixed one.
@@ -1949,23 +1959,56 @@ int dalloc(T **p, size_t n) {
 // One RK stage of Simulator::MakeTaskCollection (ideal_grmhd.cc:23-120).
 int run_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
               double beta, const double *dt, double *dt_est, cudaStream_t s) {
+  TaskRange stage_range(stage == 1 ? "pangu_stage 1" : "pangu_stage 2");
   const pangu_pack *mc0 = stage == 1 ? base : one;
   const pangu_pack *mc1 = stage == 1 ? one : base;
   int rc;
   // FixPrimitive and CalculateConservative in one pass
-  if ((rc = run_fix_primitive(e, mc0, true, s))) return rc;
-  if ((rc = run_fluxes(e, mc0, s))) return rc;
-  if (e->p.enable_B && (rc = run_ct(e, mc0, s))) return rc;
-  if ((rc = run_update(e, base, mc0, mc1, beta, dt, s))) return rc;
-  if ((rc = run_exchange(e, mc1, s))) return rc;
-  if ((rc = run_source(e, mc1, beta, dt, s))) return rc;
+  {
+    TaskRange r("FixPrimitive+CalculateConservative");
+    if ((rc = run_fix_primitive(e, mc0, true, s))) return rc;
+  }
+  {
+    TaskRange r("CalculateFluxes");
+    if ((rc = run_fluxes(e, mc0, s))) return rc;
+  }
+  if (e->p.enable_B) {
+    TaskRange r("ConstraintedTransport");
+    if ((rc = run_ct(e, mc0, s))) return rc;
+  }
+  {
+    TaskRange r("FluxDivergence+UpdateIndependentData");
+    if ((rc = run_update(e, base, mc0, mc1, beta, dt, s))) return rc;
+  }
+  {
+    TaskRange r("GhostExchange");
+    if ((rc = run_exchange(e, mc1, s))) return rc;
+  }
+  {
+    TaskRange r("AddGeometricSource");
+    if ((rc = run_source(e, mc1, beta, dt, s))) return rc;
+  }
   // the retry pass of Recovery lists the cells FixRecovery repairs
-  if ((rc = run_recovery(e, mc1, true, s))) return rc;
-  if ((rc = run_heating(e, mc1, s))) return rc;
-  if (e->p.recovery == PANGU_RECOVERY_CHAINER && (rc = run_fix_recovery(e, mc1, true, s)))
-    return rc;
-  if ((rc = run_bcs(e, mc1, s))) return rc;
-  if (stage == 2 && dt_est && (rc = run_estimate_dt(e, mc1, dt_est, s))) return rc;
+  {
+    TaskRange r("Recovery");
+    if ((rc = run_recovery(e, mc1, true, s))) return rc;
+  }
+  {
+    TaskRange r("ApplyElectronHeating");
+    if ((rc = run_heating(e, mc1, s))) return rc;
+  }
+  if (e->p.recovery == PANGU_RECOVERY_CHAINER) {
+    TaskRange r("FixRecovery");
+    if ((rc = run_fix_recovery(e, mc1, true, s))) return rc;
+  }
+  {
+    TaskRange r("ApplyBoundaryConditions");
+    if ((rc = run_bcs(e, mc1, s))) return rc;
+  }
+  if (stage == 2 && dt_est) {
+    TaskRange r("EstimateTimestep");
+    if ((rc = run_estimate_dt(e, mc1, dt_est, s))) return rc;
+  }
   return PANGU_OK;
 }
 

@@ -56,7 +56,8 @@ struct SJob {
   std::vector<double> prim;  // initial state (unless generated), then the result
   bool generated = false;    // initial state generated on the device
   pangu_problem problem{};
-  int state = 0;             // 0 waiting, 1 running, 2 done
+  int state = 0;             // 0 waiting, 1 running, 2 done, 3 cancelled
+  double cancel_at = 1e300;  // seconds after the start of the run
   int job = -1;
   std::vector<int32_t> slots;
   double t_admit = 0, t_done = 0;
@@ -168,6 +169,16 @@ int admit(SClass &c, SJob &j) {
   if (rc) return rc;
   c.dirty = true;
   ++c.running;
+  return PANGU_OK;
+}
+
+// Detaches a cancelled job without copying anything back. Needs the class
+// idle.
+int drop(SClass &c, SJob &j) {
+  const int rc = pangu_job_detach(c.e, j.job);
+  if (rc) return rc;
+  c.dirty = true;
+  --c.running;
   return PANGU_OK;
 }
 
@@ -362,10 +373,18 @@ int pangu_server_run(pangu_server *s) {
         if (q != cudaSuccess) return PANGU_ECUDA;
         c.inflight = false;
         ++st.ticks;
+        const double tnow = now_s(t0);
         for (SJob &j : s->jobs) {
           if (j.state != 1 || j.cls != ci) continue;
           ++j.done_cycles;
           st.zone_cycles += (double)c.interior * j.slots.size();
+          if (tnow >= j.cancel_at && j.done_cycles < j.cycles) {  // cancelled while running
+            if ((rc = drop(c, j))) return rc;
+            j.state = 3;
+            j.t_done = tnow;
+            ++done;
+            continue;
+          }
           if (j.done_cycles < j.cycles) continue;
           if ((rc = retire(c, j))) return rc;
           j.state = 2;
@@ -376,7 +395,14 @@ int pangu_server_run(pangu_server *s) {
       const double t = now_s(t0);
       for (int q : order) {  // first fit in arrival order
         SJob &j = s->jobs[q];
-        if (j.cls != ci || j.state != 0 || j.arrival > t) continue;
+        if (j.cls != ci || j.state != 0) continue;
+        if (t >= j.cancel_at) {  // cancelled before admission
+          j.state = 3;
+          j.t_done = t;
+          ++done;
+          continue;
+        }
+        if (j.arrival > t) continue;
         rc = admit(c, j);
         if (rc == PANGU_EFULL) continue;
         if (rc) return rc;
@@ -404,12 +430,15 @@ int pangu_server_run(pangu_server *s) {
           next = s->jobs[q].arrival;
           break;
         }
+      for (int q : order)  // a pending cancellation may come first
+        if (s->jobs[q].state == 0 && s->jobs[q].cancel_at < next) next = s->jobs[q].cancel_at;
       if (next > t) std::this_thread::sleep_for(std::chrono::duration<double>(next - t));
     }
   }
   st.wall_s = now_s(t0);
   std::vector<double> lat;
-  for (const SJob &j : s->jobs) lat.push_back(j.t_done - j.arrival);
+  for (const SJob &j : s->jobs)
+    if (j.state == 2) lat.push_back(j.t_done - j.arrival);
   std::sort(lat.begin(), lat.end());
   if (!lat.empty()) {
     auto pct = [&](double f) {
@@ -421,7 +450,7 @@ int pangu_server_run(pangu_server *s) {
     st.p50_s = pct(0.50);
     st.p99_s = pct(0.99);
   }
-  st.jobs = (int64_t)s->jobs.size();
+  st.jobs = (int64_t)lat.size();
   st.zone_cycles_per_s = st.wall_s > 0 ? st.zone_cycles / st.wall_s : 0;
   st.hbm_bytes = s->used;
   return PANGU_OK;
@@ -441,6 +470,19 @@ int pangu_server_result(pangu_server *s, int32_t ticket, double *prim_out, doubl
   if (counters_out)
     for (int q = 0; q < PANGU_NCOUNTERS; ++q) counters_out[q] = j.counters[q];
   return PANGU_OK;
+}
+
+int pangu_server_cancel(pangu_server *s, int32_t ticket, double at_s) {
+  if (!s || ticket < 0 || ticket >= (int)s->jobs.size()) return PANGU_EINVAL;
+  SJob &j = s->jobs[ticket];
+  if (j.state >= 2) return PANGU_EINVAL;
+  j.cancel_at = at_s;
+  return PANGU_OK;
+}
+
+int pangu_server_job_state(const pangu_server *s, int32_t ticket) {
+  if (!s || ticket < 0 || ticket >= (int)s->jobs.size()) return PANGU_EINVAL;
+  return s->jobs[ticket].state;
 }
 
 int pangu_server_get_stats(const pangu_server *s, pangu_server_stats *out) {

@@ -96,6 +96,8 @@ def lib():
     L.pangu_server_result.argtypes = [_P, C.c_int32, C.c_void_p, C.c_void_p,
                                       C.POINTER(C.c_uint64)]
     L.pangu_server_get_stats.argtypes = [_P, C.POINTER(abi.ServerStats)]
+    L.pangu_server_cancel.argtypes = [_P, C.c_int32, C.c_double]
+    L.pangu_server_job_state.argtypes = [_P, C.c_int32]
     _lib = L
     return L
 
@@ -604,6 +606,18 @@ class Server:
                                                   C.byref(t)), "pangu_server_submit_problem")
         self.tickets[t.value] = (cls, mesh.nbx1 * mesh.nbx2 * mesh.nbx3)
         return t.value
+
+    STATES = ("waiting", "running", "done", "cancelled")
+
+    def cancel(self, ticket: int, at_s: float):
+        """Cancels a job at at_s seconds into the run (dropped if still waiting,
+        detached at its class's next tick if running; no result)."""
+        _check(self.L.pangu_server_cancel(self.h, ticket, float(at_s)), "pangu_server_cancel")
+
+    def state(self, ticket: int) -> str:
+        st = self.L.pangu_server_job_state(self.h, ticket)
+        _check(min(st, 0), "pangu_server_job_state")
+        return self.STATES[st]
 
     def run(self):
         torch = _torch()

@@ -76,3 +76,30 @@ def test_server_budget_enforced():
     with pytest.raises(EngineError):
         srv.add_class(pin, 1000, 4)
     srv.add_class(pin, 4, 2)
+
+
+def test_server_cancellation():
+    """A waiting job cancelled before its slots free up is dropped, a running
+    one is detached at a tick boundary; the other jobs finish unaffected."""
+    from pangu_b200.engine import EngineError, Server
+    tb = (32, 16, 1)
+    keep = _job("torus", nx1=64, nx2=32, bx=tb, seed=1)
+    long_job = _job("torus", nx1=32, nx2=16, bx=tb, seed=2)
+    waiting = _job("torus", nx1=64, nx2=32, bx=tb, seed=3)
+    srv = Server(4 << 30)
+    c = srv.add_class(keep[0], 5, 3)
+    t_keep = srv.submit(c, *keep, 6, 0.0)
+    t_long = srv.submit(c, *long_job, 100000, 0.0)  # would run for minutes
+    t_wait = srv.submit(c, *waiting, 3, 0.0)         # 4 blocks: no room until keep ends
+    srv.cancel(t_long, 0.05)
+    srv.cancel(t_wait, 0.0)
+    srv.run()
+    assert srv.state(t_keep) == "done"
+    assert srv.state(t_long) == "cancelled" and srv.state(t_wait) == "cancelled"
+    with pytest.raises(EngineError):
+        srv.result(t_long)
+    ref, ref_cnt = _alone(*keep, 6)
+    got, _, cnt = srv.result(t_keep)
+    np.testing.assert_array_equal(got, ref)
+    np.testing.assert_array_equal(cnt, ref_cnt)
+    assert srv.stats()["jobs"] == 1
