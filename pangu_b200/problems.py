@@ -438,6 +438,54 @@ def problem_struct(name: str, pin: ParameterInput) -> abi.Problem:
     return pb
 
 
+# ---------------------------------------------------------------------------
+# Atmosphere around a spinning hole in Cartesian Kerr-Schild coordinates
+# ---------------------------------------------------------------------------
+def cks_atmosphere_input(n: int = 16, nblock: int | None = None, a: float = 0.5,
+                         r_excise: float = 1.5) -> ParameterInput:
+    """A box around the hole with outflow faces. The box is offset so that no
+    cell centre or face lies on z = 0, where the ring singularity (r = 0 for
+    x^2 + y^2 <= a^2) sits; the hole is excised within r_excise."""
+    pin = ParameterInput()
+    for d in (1, 2, 3):
+        for k, v in {f"nx{d}": n, f"x{d}min": -3.9, f"x{d}max": 4.1,
+                     f"ix{d}_bc": "outflow", f"ox{d}_bc": "outflow"}.items():
+            pin.set("parthenon/mesh", k, v)
+        pin.set("parthenon/meshblock", f"nx{d}", nblock or n)
+    pin.set("parthenon/mesh", "nghost", 2)
+    for k, v in dict(cfl_number=0.3, adiabatic_index=5.0 / 3.0, riemann_solver="laxf",
+                     limiter="mc", recovery="chainer", enable_B=True, enable_heating=False,
+                     density_floor=1e-6, energy_floor=1e-8).items():
+        pin.set("core", k, v)
+    for k, v in dict(type="cks", a=a, excise=True, r_excise=r_excise).items():
+        pin.set("metric", k, v)
+    for k, v in dict(integrator="rk2", dt_init=1e-5, dt_factor=1.3).items():
+        pin.set("parthenon/time", k, v)
+    return pin
+
+
+def cks_atmosphere(geo: Geometry, packages) -> np.ndarray:
+    """rho = 1e-2 r^-1.5, u = 1e-4 r^-2.5 (r the spherical radius of the
+    cell centre, at least 1), zero weighted velocity, uniform B^z = 0.05."""
+    c = packages["core"].params
+    gam = c["adiabatic_index"]
+    S = _slots(c["enable_B"], c["enable_heating"])
+    P = _alloc(geo, _nf(c["enable_B"], c["enable_heating"]))
+    for b in range(geo.nb):
+        x = geo.xc(b, 0)[None, None, :]
+        y = geo.xc(b, 1)[None, :, None]
+        z = geo.xc(b, 2)[:, None, None]
+        r = np.maximum(np.sqrt(x * x + y * y + z * z), 1.0)
+        P[b, S["rho"]] = 1e-2 * r ** -1.5
+        P[b, S["u"]] = 1e-4 * r ** -2.5
+        if c["enable_B"]:
+            P[b, S["b3"]] = 0.05
+        P[b, S["ent"]] = (gam - 1.0) * P[b, S["u"]] * P[b, S["rho"]] ** (-gam)
+        if c["enable_heating"]:
+            P[b, S["kel"]] = c["fel_0"] * P[b, S["ent"]]
+    return P
+
+
 def make_problem(name: str, **kw):
     """Returns (ParameterInput, generator) for a named benchmark problem."""
     if name in ("orszag_tang", "ot"):
@@ -446,4 +494,6 @@ def make_problem(name: str, **kw):
         return brio_wu_input(**kw), lambda geo, pk, pin: brio_wu(geo, pk)
     if name in ("fm_torus", "torus"):
         return fm_torus_input(**kw), fm_torus
+    if name in ("cks_atmosphere", "cks"):
+        return cks_atmosphere_input(**kw), lambda geo, pk, pin: cks_atmosphere(geo, pk)
     raise ValueError(f"unknown problem {name!r}")

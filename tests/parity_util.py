@@ -26,6 +26,7 @@ CASES = {
     "torus3d_blocks": ("torus", dict(nx1=32, nx2=16, nx3=8, bx=(16, 8, 4)), {}),
     "torus3d_hll": ("torus", dict(nx1=32, nx2=16, nx3=8, bx=(16, 8, 8), riemann="hll"), {}),
     "torus_bl": ("torus", dict(nx1=48, nx2=24), {("metric", "type"): "bl"}),
+    "cks_excise": ("cks", dict(n=16, nblock=8), {}),
 }
 
 

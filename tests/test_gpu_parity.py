@@ -24,7 +24,7 @@ pytestmark = pytest.mark.gpu
 
 TASK_CASES = ["ot_mc_laxf", "ot_ppm4_hll_heat", "ot_blocks", "bw_hll", "torus_ppm4_laxf",
               "torus_mc_hll", "torus_robuster", "torus_kawazura", "torus3d_blocks",
-              "torus3d_hll", "torus_bl"]
+              "torus3d_hll", "torus_bl", "cks_excise"]
 
 
 def _engine(case):
@@ -138,7 +138,7 @@ def test_tasks_match_oracle(name):
 
 
 STEP_CASES = ["ot_mc_laxf", "bw_hll", "torus_ppm4_laxf", "torus_mc_hll", "torus3d_blocks",
-              "torus_robuster"]
+              "torus_robuster", "cks_excise"]
 
 
 def _run_both(case, nsteps, fixed_dt):
