@@ -17,7 +17,9 @@ reconstruction, Riemann flux and heating; its lines report the per-field
 relative L1 error against an FP64 run of the same job.
 
 N > 1 runs under torchrun, one independent job per GPU (weak scaling, no
-collective on the data path; the timing is a max over ranks).
+collective on the data path; the timing is a max over ranks). With --shard
+the GPUs instead share one mesh, its blocks split over the ranks (strong
+scaling; halo messages over NCCL point-to-point, dt all-reduced).
 ``--impl reference`` times the CPU restatement of the reference's stage path
 (oracle/) on the host cores for the same workload and metric.
 """
@@ -355,6 +357,77 @@ def run_engine(args):
         dist.destroy_process_group()
     if line is not None:
         print(json.dumps(line), flush=True)
+
+
+def run_sharded(args):
+    """One mesh over all ranks (block sharding, strong scaling): rank r steps
+    its contiguous run of the block lattice, the halo messages move with NCCL
+    point-to-point calls while the middle of each stage runs, and dt is
+    reduced with an all-reduce(min). value = the mesh's cells x cycles / the
+    slowest rank's device time."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    os.environ.setdefault("MASTER_PORT", "29517")
+    os.environ.setdefault("RANK", "0")
+    os.environ.setdefault("WORLD_SIZE", "1")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                            device_id=dev)
+    from pangu_b200.shard import ShardedSimulation
+
+    pin = job_input(args.workload, args.precision, seed=0)  # the same mesh on every rank
+    packages, mesh, geo, prim0 = initial_state(pin)
+    sim = ShardedSimulation(pin, device=local)
+    sim.set_primitives(prim0)
+    n_int = interior_cells(pin)
+    for _ in range(args.warmup):
+        sim.step()
+    torch.cuda.synchronize()
+    dist.barrier()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    launches0 = sim.engine.launches()
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        for s in range(args.steps):
+            starts[s].record()
+            sim.step()
+            ends[s].record()
+        torch.cuda.synchronize()
+    launches = sim.engine.launches() - launches0
+    total_ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
+    total_ms = max_over_ranks(total_ms, dist, dev)
+    halo = 8 * sim.width * (sum(sim.send_counts) + sum(sim.recv_counts))
+    halo = max_over_ranks(halo, dist, dev)
+    counters = sim.total_counters()
+    dist.barrier()
+    dist.destroy_process_group()
+    if rank != 0:
+        return
+    value = n_int * args.steps / (total_ms / 1e3)
+    line = {"metric": METRIC, "value": round(value, 1), "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(total_ms / args.steps, 5), "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32/f64 mixed",
+            "data": "synthetic (seeded initial conditions)",
+            "config": config(args.workload, args.precision,
+                             {"parallelism": f"one mesh, blocks sharded over {world} GPUs",
+                              "halo_bytes_per_stage_max_rank": int(halo),
+                              "l2": "not flushed: each rank's state is larger than L2",
+                              "launch": "host-launched stage parts, NCCL point-to-point halos"}),
+            "e2e": None, "roofline": None, "cpu_baseline": None, "clocks": clk.summary(),
+            "gpu_launches": launches,
+            "c2p_fail_cells": int(counters[6])}
+    print(json.dumps(line), flush=True)
 
 
 def e2e_run(sim, torch, dev, steps):
@@ -738,10 +811,17 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true",
                     help="launch every kernel from the host instead of replaying a CUDA graph")
+    ap.add_argument("--shard", action="store_true",
+                    help="one mesh with its blocks sharded over the GPUs (strong scaling) "
+                         "instead of one independent job per GPU")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         run_reference(args)
+    elif args.shard:
+        if args.workload not in SINGLE:
+            ap.error("--shard takes a single-mesh workload (torus2d, ot, torus3d)")
+        run_sharded(args)
     elif args.workload == "batch48":
         run_batch(args)
     elif args.workload == "serve":

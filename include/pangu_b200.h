@@ -220,6 +220,60 @@ int pangu_stage(pangu_engine *e, int stage, const pangu_pack *base,
                 const pangu_pack *one, double beta, const double *dt,
                 double *dt_est, void *stream);
 
+/* ---- one mesh over several GPUs (block sharding) ----------------------- */
+/* The reference spreads a mesh's blocks over MPI ranks through Parthenon
+ * (ghost exchange at ideal_grmhd.cc:78, dt reduction in
+ * EstimateTimestepMesh, timestep_estimation.cc:13-102). Here rank r's
+ * engine holds the blocks b with block_rank[b] == r (lattice order, x1
+ * fastest). Ghost cells whose source block is on another rank travel as
+ * halo messages: per peer rank q, a contiguous run of entries, each the
+ * Nf primitives and the flag of one cell as FP64 (Nf + 1 doubles); the
+ * k-th entry rank r sends to q is the k-th entry q receives from r. A send
+ * (receive) buffer holds the messages of all peers in rank order.
+ * Every stage of a shard is three calls around the message transfer:
+ *   pangu_stage_begin   FixPrimitive ... update, local ghost exchange, and
+ *                       the halo cells packed into `send`;
+ *   (the caller moves each peer's message, e.g. NCCL send/recv)
+ *   pangu_stage_middle  AddGeometricSource, Recovery, ApplyElectronHeating
+ *                       (these read no ghost cell: they overlap the transfer);
+ *   pangu_stage_end     the received halo cells unpacked from `recv`,
+ *                       FixRecovery, physical BCs, and on stage 2 this
+ *                       shard's dt estimate, which the caller reduces (min)
+ *                       over the ranks before pangu_update_dt.
+ * On an engine without halo entries the three calls equal pangu_stage, and
+ * send / recv may be NULL; pangu_stage returns PANGU_EINVAL on a shard that
+ * has halo entries. */
+int pangu_shard_create(const pangu_params *params, const pangu_mesh *mesh,
+                       const int32_t *block_rank, int32_t nranks, int32_t rank,
+                       pangu_engine **out);
+/* The halo plan of rank `rank` without a GPU: entries per peer
+ * (send_counts[nranks], recv_counts[nranks]) and, when the cell arrays are
+ * non-NULL, the cells in message order as offsets b * ncell + cell of the
+ * whole mesh's block b (ncell = cells of one block with ghosts). */
+int pangu_shard_plan(const pangu_params *params, const pangu_mesh *mesh,
+                     const int32_t *block_rank, int32_t nranks, int32_t rank,
+                     int64_t *send_counts, int64_t *recv_counts,
+                     int64_t *send_cells, int64_t *recv_cells);
+/* Entries per peer of this shard's messages ([nranks] each). */
+int pangu_halo_counts(const pangu_engine *e, int64_t *send_counts,
+                      int64_t *recv_counts);
+/* Pack the halo cells of md into send / unpack recv into md's ghosts (the
+ * initial ghost fill of a shard: pack base, transfer, unpack base, then
+ * pangu_job_start, which adds the local exchange and the physical BCs). */
+int pangu_halo_pack(pangu_engine *e, const pangu_pack *md, double *send,
+                    void *stream);
+int pangu_halo_unpack(pangu_engine *e, const pangu_pack *md,
+                      const double *recv, void *stream);
+int pangu_stage_begin(pangu_engine *e, int stage, const pangu_pack *base,
+                      const pangu_pack *one, double beta, const double *dt,
+                      double *send, void *stream);
+int pangu_stage_middle(pangu_engine *e, int stage, const pangu_pack *base,
+                       const pangu_pack *one, double beta, const double *dt,
+                       void *stream);
+int pangu_stage_end(pangu_engine *e, int stage, const pangu_pack *base,
+                    const pangu_pack *one, const double *recv,
+                    double *dt_est, void *stream);
+
 /* The dt estimate of pangu_estimate_dt without an engine handle and without
  * allocating: for callers that may not call cudaMalloc (their device memory
  * belongs to a pool or a fixed budget, so they cannot create an engine, which

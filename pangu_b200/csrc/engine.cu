@@ -34,6 +34,14 @@ int run_bcs(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
 int run_estimate_dt(pangu_engine *e, const pangu_pack *md, double *dt_out, cudaStream_t s);
 int run_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
               double beta, const double *dt, double *dt_est, cudaStream_t s);
+int run_stage_begin(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
+                    double beta, const double *dt, double *send, cudaStream_t s);
+int run_stage_middle(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
+                     double beta, const double *dt, cudaStream_t s);
+int run_stage_end(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
+                  const double *recv, double *dt_est, cudaStream_t s);
+int run_halo_pack(pangu_engine *e, const pangu_pack *md, double *buf, cudaStream_t s);
+int run_halo_unpack(pangu_engine *e, const pangu_pack *md, const double *buf, cudaStream_t s);
 int run_job_start(pangu_engine *e, int job, const pangu_pack *base, const pangu_pack *one,
                   cudaStream_t s);
 int run_autotune(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
@@ -80,6 +88,8 @@ int pangu_engine_destroy(pangu_engine *e) {
   cudaFree(e->d_genred);
   cudaFree(e->d_fail_vals);
   cudaFree(e->d_dtmin);
+  cudaFree(e->d_hsend);
+  cudaFree(e->d_hrecv);
   delete e;
   return PANGU_OK;
 }
@@ -240,14 +250,21 @@ int pool_rebuild(pangu_engine *e) {
 }
 
 // Places a job's blocks in free slots (lowest first) and builds their
-// coordinate tables, metric tables, BC faces and exchange map.
+// coordinate tables, metric tables, BC faces and exchange map. With
+// block_rank non-null the job is this rank's shard of a mesh spread over
+// e->nranks engines: only the blocks with block_rank[b] == e->rank are
+// placed, and the exchange entries that cross ranks become the halo lists.
 int pool_attach(pangu_engine *e, const pangu_mesh &m, double a, double h, int *job_out,
-                int32_t *slots_out) {
+                int32_t *slots_out, const int32_t *block_rank = nullptr) {
   if (m.nx1 != e->m.nx1 || m.nx2 != e->m.nx2 || m.nx3 != e->m.nx3 || m.ng != e->m.ng)
     return PANGU_EINVAL;
   int rc = validate_mesh(e->p, m);
   if (rc) return rc;
-  const long long nbl = (long long)m.nbx1 * m.nbx2 * m.nbx3;
+  const long long nall = (long long)m.nbx1 * m.nbx2 * m.nbx3;
+  std::vector<int> gb;  // lattice ids of the blocks placed here, in lattice order
+  for (long long b = 0; b < nall; ++b)
+    if (!block_rank || block_rank[b] == e->rank) gb.push_back((int)b);
+  const long long nbl = (long long)gb.size();
   int job = -1;
   for (int q = 0; q < e->max_jobs && job < 0; ++q)
     if (!e->jobs[q].live) job = q;
@@ -256,6 +273,8 @@ int pool_attach(pangu_engine *e, const pangu_mesh &m, double a, double h, int *j
   for (int sl = 0; sl < e->capacity && (long long)slots.size() < nbl; ++sl)
     if (!e->slot_used[sl]) slots.push_back(sl);
   if ((long long)slots.size() < nbl) return PANGU_EFULL;
+  std::vector<long long> slot_of_block(nall, -1);
+  for (long long q = 0; q < nbl; ++q) slot_of_block[gb[q]] = slots[q];
 
   PoolJob J;
   J.m = m;
@@ -270,9 +289,17 @@ int pool_attach(pangu_engine *e, const pangu_mesh &m, double a, double h, int *j
   pgh::build_exchange(m, L, xd, xs);
   const Dims &d = e->d;
   const long long nc = d.ncell;
+  auto to_slot = [&](int64_t c) { return (int64_t)slot_of_block[c / nc] * nc + c % nc; };
+  std::vector<std::vector<int64_t>> hsend, hrecv;
+  if (block_rank) {
+    std::vector<int64_t> ld, ls;
+    pgh::shard_exchange(xd, xs, nc, block_rank, e->nranks, e->rank, ld, ls, hsend, hrecv);
+    xd.swap(ld);
+    xs.swap(ls);
+  }
   for (size_t q = 0; q < xd.size(); ++q) {
-    xd[q] = (int64_t)slots[xd[q] / nc] * nc + xd[q] % nc;
-    xs[q] = (int64_t)slots[xs[q] / nc] * nc + xs[q] % nc;
+    xd[q] = to_slot(xd[q]);
+    xs[q] = to_slot(xs[q]);
   }
   J.xdst.swap(xd);
   J.xsrc.swap(xs);
@@ -281,8 +308,9 @@ int pool_attach(pangu_engine *e, const pangu_mesh &m, double a, double h, int *j
   const int nbv[3] = {m.nbx1, m.nbx2, m.nbx3};
   const int act[3] = {d.o1, d.o2, d.o3};
   bool ok = true;
-  for (long long b = 0; b < nbl; ++b) {
-    const int sl = slots[b];
+  for (long long q = 0; q < nbl; ++q) {
+    const long long b = gb[q];
+    const int sl = slots[q];
     const int bl[3] = {(int)(b % m.nbx1), (int)((b / m.nbx1) % m.nbx2),
                        (int)(b / ((long long)m.nbx1 * m.nbx2))};
     signed char bcf[6];
@@ -302,6 +330,24 @@ int pool_attach(pangu_engine *e, const pangu_mesh &m, double a, double h, int *j
   }
   ok &= cudaMemset(e->d_cnt + (size_t)job * PANGU_NCOUNTERS, 0, PANGU_NCOUNTERS * 8) == cudaSuccess;
   if (!ok) return PANGU_ECUDA;
+  if (block_rank) {
+    // halo lists, per peer in rank order, in slot cell offsets
+    std::vector<int64_t> hs, hr;
+    e->hsend_off.assign(e->nranks + 1, 0);
+    e->hrecv_off.assign(e->nranks + 1, 0);
+    for (int q = 0; q < e->nranks; ++q) {
+      for (int64_t c : hsend[q]) hs.push_back(to_slot(c));
+      for (int64_t c : hrecv[q]) hr.push_back(to_slot(c));
+      e->hsend_off[q + 1] = (long long)hs.size();
+      e->hrecv_off[q + 1] = (long long)hr.size();
+    }
+    if (dalloc(&e->d_hsend, hs.size()) || dalloc(&e->d_hrecv, hr.size())) return PANGU_ENOMEM;
+    if (!hs.empty())
+      ok &= cudaMemcpy(e->d_hsend, hs.data(), hs.size() * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+    if (!hr.empty())
+      ok &= cudaMemcpy(e->d_hrecv, hr.data(), hr.size() * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+    if (!ok) return PANGU_ECUDA;
+  }
   if (e->p.metric_type == PANGU_METRIC_MKS || e->p.metric_type == PANGU_METRIC_BL) {
     // static metric tables of the job's slots, with the job's a and h
     ok = cudaMemcpy(e->d_tmp_slots, slots.data(), slots.size() * sizeof(int),
@@ -327,9 +373,20 @@ int pool_attach(pangu_engine *e, const pangu_mesh &m, double a, double h, int *j
   if (rc) return rc;
   *job_out = job;
   if (slots_out)
-    for (long long b = 0; b < nbl; ++b) slots_out[b] = slots[b];
+    for (long long q = 0; q < nbl; ++q) slots_out[q] = slots[q];
   return PANGU_OK;
 }
+
+int validate_ranks(const pangu_mesh &m, const int32_t *block_rank, int nranks, int rank) {
+  if (!block_rank || nranks < 1 || rank < 0 || rank >= nranks) return PANGU_EINVAL;
+  const long long nall = (long long)m.nbx1 * m.nbx2 * m.nbx3;
+  for (long long b = 0; b < nall; ++b)
+    if (block_rank[b] < 0 || block_rank[b] >= nranks) return PANGU_EINVAL;
+  return PANGU_OK;
+}
+
+bool halo_sends(const pangu_engine *e) { return !e->hsend_off.empty() && e->hsend_off.back() > 0; }
+bool halo_recvs(const pangu_engine *e) { return !e->hrecv_off.empty() && e->hrecv_off.back() > 0; }
 
 }  // namespace
 
@@ -489,6 +546,8 @@ int pangu_generate(pangu_engine *e, int32_t job, const pangu_problem *problem,
   if (problem->kind == PANGU_PROBLEM_FM_TORUS &&
       !(problem->kappa > 0 && problem->beta > 0 && problem->rmax > problem->rin))
     return PANGU_EINVAL;
+  // the torus normalises by maxima over the whole mesh, which a shard does not hold
+  if (problem->kind == PANGU_PROBLEM_FM_TORUS && e->nranks > 1) return PANGU_EINVAL;
   return RUN(run_generate, e, job, *problem, base, S(stream));
 }
 
@@ -506,8 +565,113 @@ int pangu_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_
                 double beta, const double *dt, double *dt_est, void *stream) {
   if (!pack_ok(e, base) || !pack_ok(e, one) || !dt || (stage != 1 && stage != 2))
     return PANGU_EINVAL;
+  if (halo_sends(e) || halo_recvs(e)) return PANGU_EINVAL;  // a shard: the three-part calls
   if (e->d.NB == 0) return PANGU_OK;
   return RUN(run_stage, e, stage, base, one, beta, dt, dt_est, S(stream));
+}
+
+// ---------------------------------------------------------------------------
+// Block sharding of one mesh over several GPUs.
+// ---------------------------------------------------------------------------
+int pangu_shard_plan(const pangu_params *params, const pangu_mesh *mesh, const int32_t *block_rank,
+                     int32_t nranks, int32_t rank, int64_t *send_counts, int64_t *recv_counts,
+                     int64_t *send_cells, int64_t *recv_cells) {
+  if (!params || !mesh || !send_counts || !recv_counts) return PANGU_EINVAL;
+  int rc = validate_params(*params);
+  if (!rc) rc = validate_mesh(*params, *mesh);
+  if (!rc) rc = validate_ranks(*mesh, block_rank, nranks, rank);
+  if (rc) return rc;
+  const pgh::Layout L = pgh::make_layout(*params, *mesh);
+  std::vector<int64_t> xd, xs, ld, ls;
+  pgh::build_exchange(*mesh, L, xd, xs);
+  std::vector<std::vector<int64_t>> snd, rcv;
+  const int64_t nc = (int64_t)L.N[0] * L.N[1] * L.N[2];
+  pgh::shard_exchange(xd, xs, nc, block_rank, nranks, rank, ld, ls, snd, rcv);
+  int64_t ns = 0, nr = 0;
+  for (int q = 0; q < nranks; ++q) {
+    send_counts[q] = (int64_t)snd[q].size();
+    recv_counts[q] = (int64_t)rcv[q].size();
+    for (int64_t c : snd[q])
+      if (send_cells) send_cells[ns++] = c;
+    for (int64_t c : rcv[q])
+      if (recv_cells) recv_cells[nr++] = c;
+  }
+  return PANGU_OK;
+}
+
+int pangu_shard_create(const pangu_params *params, const pangu_mesh *mesh,
+                       const int32_t *block_rank, int32_t nranks, int32_t rank,
+                       pangu_engine **out) {
+  if (!params || !mesh || !out) return PANGU_EINVAL;
+  *out = nullptr;
+  int rc = validate_params(*params);
+  if (!rc) rc = validate_mesh(*params, *mesh);
+  if (!rc) rc = validate_ranks(*mesh, block_rank, nranks, rank);
+  if (rc) return rc;
+  const long long nall = (long long)mesh->nbx1 * mesh->nbx2 * mesh->nbx3;
+  int nloc = 0;
+  for (long long b = 0; b < nall; ++b) nloc += block_rank[b] == rank;
+  if (nloc == 0) return PANGU_EINVAL;
+  pangu_engine *e = new (std::nothrow) pangu_engine;
+  if (!e) return PANGU_ENOMEM;
+  e->p = *params;
+  e->m = *mesh;
+  e->nranks = nranks;
+  e->rank = rank;
+  rc = pool_init(e, nloc, 1);
+  int job = -1;
+  if (!rc) rc = pool_attach(e, *mesh, params->a, params->h, &job, nullptr, block_rank);
+  if (rc) {
+    pangu_engine_destroy(e);
+    return rc;
+  }
+  *out = e;
+  return PANGU_OK;
+}
+
+int pangu_halo_counts(const pangu_engine *e, int64_t *send_counts, int64_t *recv_counts) {
+  if (!e || !send_counts || !recv_counts) return PANGU_EINVAL;
+  for (int q = 0; q < e->nranks; ++q) {
+    send_counts[q] = e->hsend_off.empty() ? 0 : e->hsend_off[q + 1] - e->hsend_off[q];
+    recv_counts[q] = e->hrecv_off.empty() ? 0 : e->hrecv_off[q + 1] - e->hrecv_off[q];
+  }
+  return PANGU_OK;
+}
+
+int pangu_halo_pack(pangu_engine *e, const pangu_pack *md, double *send, void *stream) {
+  if (!pack_ok(e, md) || (halo_sends(e) && !send)) return PANGU_EINVAL;
+  return RUN(run_halo_pack, e, md, send, S(stream));
+}
+
+int pangu_halo_unpack(pangu_engine *e, const pangu_pack *md, const double *recv, void *stream) {
+  if (!pack_ok(e, md) || (halo_recvs(e) && !recv)) return PANGU_EINVAL;
+  return RUN(run_halo_unpack, e, md, recv, S(stream));
+}
+
+int pangu_stage_begin(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
+                      double beta, const double *dt, double *send, void *stream) {
+  if (!pack_ok(e, base) || !pack_ok(e, one) || !dt || (stage != 1 && stage != 2) ||
+      (halo_sends(e) && !send))
+    return PANGU_EINVAL;
+  if (e->d.NB == 0) return PANGU_OK;
+  return RUN(run_stage_begin, e, stage, base, one, beta, dt, send, S(stream));
+}
+
+int pangu_stage_middle(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
+                       double beta, const double *dt, void *stream) {
+  if (!pack_ok(e, base) || !pack_ok(e, one) || !dt || (stage != 1 && stage != 2))
+    return PANGU_EINVAL;
+  if (e->d.NB == 0) return PANGU_OK;
+  return RUN(run_stage_middle, e, stage, base, one, beta, dt, S(stream));
+}
+
+int pangu_stage_end(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
+                    const double *recv, double *dt_est, void *stream) {
+  if (!pack_ok(e, base) || !pack_ok(e, one) || (stage != 1 && stage != 2) ||
+      (halo_recvs(e) && !recv))
+    return PANGU_EINVAL;
+  if (e->d.NB == 0) return PANGU_OK;
+  return RUN(run_stage_end, e, stage, base, one, recv, dt_est, S(stream));
 }
 
 // ---------------------------------------------------------------------------

@@ -28,6 +28,11 @@ void build_tables(const pangu_params &p, const Layout &L, std::vector<double> &t
                   std::vector<double> &t2);
 void build_exchange(const pangu_mesh &m, const Layout &L, std::vector<int64_t> &dst,
                     std::vector<int64_t> &src);
+void shard_exchange(const std::vector<int64_t> &dst, const std::vector<int64_t> &src,
+                    int64_t ncell, const int32_t *block_rank, int nranks, int rank,
+                    std::vector<int64_t> &ldst, std::vector<int64_t> &lsrc,
+                    std::vector<std::vector<int64_t>> &send,
+                    std::vector<std::vector<int64_t>> &recv);
 }  // namespace pgh
 
 // ---------------------------------------------------------------------------
@@ -96,6 +101,12 @@ struct pangu_engine {
   long long fail_cap = 0;
   unsigned long long *d_dtmin = nullptr;  // [capacity][3]
   long long launches = 0;  // kernels launched through this handle
+  // Block sharding (one mesh over several GPUs): this engine holds the blocks
+  // of `rank`; ghost cells whose source block is on another rank travel as
+  // halo messages, per peer in rank order, each entry Nf primitives + flag.
+  int nranks = 1, rank = 0;
+  std::vector<long long> hsend_off, hrecv_off;       // [nranks + 1] entry offsets
+  long long *d_hsend = nullptr, *d_hrecv = nullptr;  // slot cell offsets
   // Tile shapes of the flux kernels per direction: march depth (x2/x3) and
   // CTA size; set by pangu_autotune.
   struct {

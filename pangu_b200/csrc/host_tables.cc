@@ -164,4 +164,33 @@ void build_exchange(const pangu_mesh &m, const Layout &L, std::vector<int64_t> &
   }
 }
 
+// Block sharding of one mesh over several ranks: splits the exchange map for
+// `rank`. Entries with both blocks on `rank` stay local (ldst, lsrc). An entry
+// whose source block is on `rank` and whose destination block is on peer q is
+// sent to q (its source cell appended to send[q]); one whose destination is on
+// `rank` and whose source is on q is received from q (its destination cell
+// appended to recv[q]). Both sides walk the same map in the same order, so the
+// k-th cell that `rank` sends to q is the k-th cell q receives from `rank`.
+void shard_exchange(const std::vector<int64_t> &dst, const std::vector<int64_t> &src,
+                    int64_t ncell, const int32_t *block_rank, int nranks, int rank,
+                    std::vector<int64_t> &ldst, std::vector<int64_t> &lsrc,
+                    std::vector<std::vector<int64_t>> &send,
+                    std::vector<std::vector<int64_t>> &recv) {
+  ldst.clear();
+  lsrc.clear();
+  send.assign(nranks, {});
+  recv.assign(nranks, {});
+  for (size_t q = 0; q < dst.size(); ++q) {
+    const int rd = block_rank[dst[q] / ncell], rs = block_rank[src[q] / ncell];
+    if (rd == rank && rs == rank) {
+      ldst.push_back(dst[q]);
+      lsrc.push_back(src[q]);
+    } else if (rs == rank) {
+      send[rd].push_back(src[q]);
+    } else if (rd == rank) {
+      recv[rs].push_back(dst[q]);
+    }
+  }
+}
+
 }  // namespace pgh

@@ -821,6 +821,36 @@ __global__ void __launch_bounds__(kThreads) k_exchange(Dims d, long long n, cons
   if (flag) flag[dc] = flag[sc];
 }
 
+// Halo messages of a sharded mesh: the cells of the exchange whose other end
+// is on another GPU, as [entry][Nf primitives, flag] in FP64 (an FP32
+// primitive converts to FP64 and back exactly), so a message is a plain
+// contiguous buffer for NCCL or a peer copy.
+__global__ void __launch_bounds__(kThreads) k_halo_pack(Dims d, long long n, const long long *cells,
+                                                        const PT *P, const double *flag,
+                                                        double *buf) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const long long c = cells[t];
+  const long long b = c / d.ncell;
+  const long long q = b * d.NF * d.ncell + (c - b * d.ncell);
+  double *o = buf + t * (d.NF + 1);
+  for (int v = 0; v < d.NF; ++v) o[v] = (double)P[q + v * d.ncell];
+  o[d.NF] = flag ? flag[c] : 0.0;
+}
+
+__global__ void __launch_bounds__(kThreads) k_halo_unpack(Dims d, long long n,
+                                                          const long long *cells, PT *P,
+                                                          double *flag, const double *buf) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const long long c = cells[t];
+  const long long b = c / d.ncell;
+  const long long q = b * d.NF * d.ncell + (c - b * d.ncell);
+  const double *o = buf + t * (d.NF + 1);
+  for (int v = 0; v < d.NF; ++v) P[q + v * d.ncell] = (PT)o[v];
+  if (flag) flag[c] = o[d.NF];
+}
+
 // ---------------------------------------------------------------------------
 // AddGeometricSource (source_term.cc:15-121): Christoffel symbols by central
 // differences of the code metric (christoffel.h:74-148), rounded step by
@@ -1856,6 +1886,22 @@ int run_exchange(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
   return run_exchange_range(e, md, 0, e->nxch, s);
 }
 
+int run_halo_pack(pangu_engine *e, const pangu_pack *md, double *buf, cudaStream_t s) {
+  const long long n = e->hsend_off.empty() ? 0 : e->hsend_off.back();
+  if (n == 0) return PANGU_OK;
+  k_halo_pack<<<grid_for(n), kThreads, 0, s>>>(e->d, n, e->d_hsend, prim_of(md), md->flag, buf);
+  ++e->launches;
+  return check_launch();
+}
+
+int run_halo_unpack(pangu_engine *e, const pangu_pack *md, const double *buf, cudaStream_t s) {
+  const long long n = e->hrecv_off.empty() ? 0 : e->hrecv_off.back();
+  if (n == 0) return PANGU_OK;
+  k_halo_unpack<<<grid_for(n), kThreads, 0, s>>>(e->d, n, e->d_hrecv, prim_of(md), md->flag, buf);
+  ++e->launches;
+  return check_launch();
+}
+
 int run_source(pangu_engine *e, const pangu_pack *md, double beta, const double *dt,
                cudaStream_t s) {
   const Dims &d = e->d;
@@ -1956,10 +2002,14 @@ int dalloc(T **p, size_t n) {
                                                                                    : PANGU_ENOMEM;
 }
 
-// One RK stage of Simulator::MakeTaskCollection (ideal_grmhd.cc:23-120).
-int run_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
-              double beta, const double *dt, double *dt_est, cudaStream_t s) {
-  TaskRange stage_range(stage == 1 ? "pangu_stage 1" : "pangu_stage 2");
+// One RK stage of Simulator::MakeTaskCollection (ideal_grmhd.cc:23-120), in
+// three parts so that a sharded mesh can move its halo messages while the
+// middle part runs: the ghost cells the messages fill are read first by
+// FixRecovery (neighbour means) and by the next stage.
+// Part 1: FixPrimitive + CalculateConservative, fluxes, CT, update, ghost
+// exchange at send time; the halo cells of mc1 go to `send` (sharded only).
+int run_stage_begin(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
+                    double beta, const double *dt, double *send, cudaStream_t s) {
   const pangu_pack *mc0 = stage == 1 ? base : one;
   const pangu_pack *mc1 = stage == 1 ? one : base;
   int rc;
@@ -1983,7 +2033,16 @@ int run_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pa
   {
     TaskRange r("GhostExchange");
     if ((rc = run_exchange(e, mc1, s))) return rc;
+    if (send && (rc = run_halo_pack(e, mc1, send, s))) return rc;
   }
+  return PANGU_OK;
+}
+
+// Part 2: geometric source, Recovery, electron heating (interior cells only).
+int run_stage_middle(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
+                     double beta, const double *dt, cudaStream_t s) {
+  const pangu_pack *mc1 = stage == 1 ? one : base;
+  int rc;
   {
     TaskRange r("AddGeometricSource");
     if ((rc = run_source(e, mc1, beta, dt, s))) return rc;
@@ -1996,6 +2055,19 @@ int run_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pa
   {
     TaskRange r("ApplyElectronHeating");
     if ((rc = run_heating(e, mc1, s))) return rc;
+  }
+  return PANGU_OK;
+}
+
+// Part 3: halo cells from `recv` (sharded only), FixRecovery, physical BCs,
+// and after the last stage the dt estimate.
+int run_stage_end(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
+                  const double *recv, double *dt_est, cudaStream_t s) {
+  const pangu_pack *mc1 = stage == 1 ? one : base;
+  int rc;
+  if (recv) {
+    TaskRange r("GhostExchange (halo)");
+    if ((rc = run_halo_unpack(e, mc1, recv, s))) return rc;
   }
   if (e->p.recovery == PANGU_RECOVERY_CHAINER) {
     TaskRange r("FixRecovery");
@@ -2010,6 +2082,15 @@ int run_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pa
     if ((rc = run_estimate_dt(e, mc1, dt_est, s))) return rc;
   }
   return PANGU_OK;
+}
+
+int run_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
+              double beta, const double *dt, double *dt_est, cudaStream_t s) {
+  TaskRange stage_range(stage == 1 ? "pangu_stage 1" : "pangu_stage 2");
+  int rc = run_stage_begin(e, stage, base, one, beta, dt, nullptr, s);
+  if (!rc) rc = run_stage_middle(e, stage, base, one, beta, dt, s);
+  if (!rc) rc = run_stage_end(e, stage, base, one, nullptr, dt_est, s);
+  return rc;
 }
 
 // Ghost fill of a newly attached job (exchange, then physical BCs) and the

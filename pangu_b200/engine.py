@@ -98,8 +98,24 @@ def lib():
     L.pangu_server_get_stats.argtypes = [_P, C.POINTER(abi.ServerStats)]
     L.pangu_server_cancel.argtypes = [_P, C.c_int32, C.c_double]
     L.pangu_server_job_state.argtypes = [_P, C.c_int32]
+    _I32P, _I64P = C.POINTER(C.c_int32), C.POINTER(C.c_int64)
+    L.pangu_shard_create.argtypes = [C.POINTER(abi.Params), C.POINTER(abi.Mesh), _I32P, C.c_int32,
+                                     C.c_int32, C.POINTER(_P)]
+    L.pangu_shard_plan.argtypes = [C.POINTER(abi.Params), C.POINTER(abi.Mesh), _I32P, C.c_int32,
+                                   C.c_int32, _I64P, _I64P, _I64P, _I64P]
+    L.pangu_halo_counts.argtypes = [_P, _I64P, _I64P]
+    L.pangu_halo_pack.argtypes = [_P, _PK, _DP, _P]
+    L.pangu_halo_unpack.argtypes = [_P, _PK, _DP, _P]
+    L.pangu_stage_begin.argtypes = [_P, C.c_int, _PK, _PK, C.c_double, _DP, _DP, _P]
+    L.pangu_stage_middle.argtypes = [_P, C.c_int, _PK, _PK, C.c_double, _DP, _P]
+    L.pangu_stage_end.argtypes = [_P, C.c_int, _PK, _PK, _DP, _DP, _P]
     _lib = L
     return L
+
+
+def _ptr(t):
+    """Device pointer of a tensor, or NULL for None or an empty tensor."""
+    return t.data_ptr() if t is not None and t.numel() else None
 
 
 def _torch():
@@ -146,21 +162,31 @@ class DeviceContainer:
 class Engine:
     """An engine handle for one parameter set and mesh."""
 
-    def __init__(self, params: abi.Params, mesh: abi.Mesh, device=0, pool=None):
+    def __init__(self, params: abi.Params, mesh: abi.Mesh, device=0, pool=None, shard=None):
         """pool=None: one mesh (pangu_engine_create). pool=(capacity_blocks,
-        max_jobs): an empty block pool of mesh's block shape."""
+        max_jobs): an empty block pool of mesh's block shape.
+        shard=(block_rank, nranks, rank): rank's blocks of a mesh spread
+        over nranks engines (pangu_shard_create)."""
         torch = _torch()
         self.device = torch.device("cuda", device)
         self.L = lib()
         self.params, self.mesh = params, mesh
         h = _P()
         with torch.cuda.device(self.device):
-            if pool is None:
+            if shard is not None:
+                br = np.ascontiguousarray(shard[0], dtype=np.int32)
+                _check(self.L.pangu_shard_create(C.byref(params), C.byref(mesh),
+                                                 br.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                 int(shard[1]), int(shard[2]), C.byref(h)),
+                       "pangu_shard_create")
+                pool = (int((br == int(shard[2])).sum()), 1)
+            elif pool is None:
                 _check(self.L.pangu_engine_create(C.byref(params), C.byref(mesh), C.byref(h)),
                        "pangu_engine_create")
             else:
                 _check(self.L.pangu_pool_create(C.byref(params), C.byref(mesh), int(pool[0]),
                                                 int(pool[1]), C.byref(h)), "pangu_pool_create")
+        self.sharded = shard is not None
         self.h = h
         self.nf = self.L.pangu_num_fields(C.byref(params))
         self.nb = mesh.nbx1 * mesh.nbx2 * mesh.nbx3 if pool is None else int(pool[0])
@@ -224,6 +250,33 @@ class Engine:
         est = dt_est_dev.data_ptr() if dt_est_dev is not None else None
         _check(self.L.pangu_stage(self.h, st, base.pack, one.pack, beta, dt_dev.data_ptr(), est,
                                   self.stream()), "pangu_stage")
+
+    # -- block sharding (pangu_b200.shard drives these) --
+    def halo_counts(self, nranks):
+        snd, rcv = (C.c_int64 * nranks)(), (C.c_int64 * nranks)()
+        _check(self.L.pangu_halo_counts(self.h, snd, rcv), "pangu_halo_counts")
+        return list(snd), list(rcv)
+
+    def halo_pack(self, md, send):
+        _check(self.L.pangu_halo_pack(self.h, md.pack, _ptr(send), self.stream()),
+               "pangu_halo_pack")
+
+    def halo_unpack(self, md, recv):
+        _check(self.L.pangu_halo_unpack(self.h, md.pack, _ptr(recv), self.stream()),
+               "pangu_halo_unpack")
+
+    def stage_begin(self, st, base, one, beta, dt_dev, send):
+        _check(self.L.pangu_stage_begin(self.h, st, base.pack, one.pack, beta, dt_dev.data_ptr(),
+                                        _ptr(send), self.stream()), "pangu_stage_begin")
+
+    def stage_middle(self, st, base, one, beta, dt_dev):
+        _check(self.L.pangu_stage_middle(self.h, st, base.pack, one.pack, beta, dt_dev.data_ptr(),
+                                         self.stream()), "pangu_stage_middle")
+
+    def stage_end(self, st, base, one, recv, dt_est_dev=None):
+        est = dt_est_dev.data_ptr() if dt_est_dev is not None else None
+        _check(self.L.pangu_stage_end(self.h, st, base.pack, one.pack, _ptr(recv), est,
+                                      self.stream()), "pangu_stage_end")
 
     def update_dt(self, dt_dev, dt_est_dev, factor):
         _check(self.L.pangu_update_dt(self.h, dt_dev.data_ptr(), dt_est_dev.data_ptr(), factor,
