@@ -109,15 +109,18 @@ __device__ __forceinline__ void gcov_at(const Dims &d, const pangu_params &p, in
 // on time, so ComputeMetricAtLocation (christoffel.h:53-62) and
 // ComputeChristoffelConnection (christoffel.h:74-148) are evaluated once per
 // (j, i) point by the dense reference arithmetic (k_build_tables) and stored:
-// the structurally non-zero entries of gcov and gcon (upper triangle), gdet,
-// sqrt|gdet|, the lapse 1/sqrt(-gcon00), a validity flag (0 where the
-// inversion is singular) and, at cell centres, the structurally non-zero
-// Christoffel symbols (symmetric in their lower indices). Loads reproduce
-// the dense values bit for bit.
+// the structurally non-zero entries of gcov (upper triangle: the code metric
+// is symmetric bit for bit) and of gcon (every entry: the Gauss-Jordan inverse
+// leaves g^rc and g^cr unequal in the last bits in most cells, and the C2P
+// schemes read both), gdet, sqrt|gdet|, the lapse 1/sqrt(-gcon00), a validity
+// flag (0 where the inversion is singular) and, at cell centres, the
+// structurally non-zero Christoffel symbols (symmetric in their lower
+// indices). Loads reproduce the dense values bit for bit.
 // ---------------------------------------------------------------------------
 struct TabLayout {
-  int nsym, nmet, nconn, ncen;
+  int nsym, ncon, nmet, nconn, ncen;
   int sym[4][4];      // slot of g_rc (r, c symmetric), -1 if structurally zero
+  int con[4][4];      // slot of g^rc (not symmetric), -1 if structurally zero
   int conn[4][4][4];  // slot of Gamma^a_bc (b, c symmetric), -1 if zero
 };
 
@@ -135,7 +138,11 @@ __host__ __device__ constexpr TabLayout tab_layout(int mt) {
         ++n;
       }
   L.nsym = n;
-  L.nmet = 2 * n + 4;
+  int nc = 0;
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) L.con[r][c] = pt.nz[r][c] ? nc++ : -1;
+  L.ncon = nc;
+  L.nmet = L.nsym + L.ncon + 4;
   // derivative directions with non-zero metric derivatives
   bool ddir[4] = {false, true, true, mt == CKS};
   if (mt == MINKOWSKI) ddir[1] = ddir[2] = ddir[3] = false;
@@ -168,23 +175,23 @@ template <int MT>
 __device__ __forceinline__ int load_geo(const double *__restrict__ tab, long long plane,
                                         long long off, Geo &g) {
   constexpr TabLayout L = tab_layout(MT);
-  double cov[L.nsym], con[L.nsym];
+  double cov[L.nsym], con[L.ncon];
 #pragma unroll
-  for (int q = 0; q < L.nsym; ++q) {
-    cov[q] = __ldg(tab + off + q * plane);
-    con[q] = __ldg(tab + off + (L.nsym + q) * plane);
-  }
+  for (int q = 0; q < L.nsym; ++q) cov[q] = __ldg(tab + off + q * plane);
+#pragma unroll
+  for (int q = 0; q < L.ncon; ++q) con[q] = __ldg(tab + off + (L.nsym + q) * plane);
 #pragma unroll
   for (int r = 0; r < 4; ++r)
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       g.gcov[r][c] = L.sym[r][c] >= 0 ? cov[L.sym[r][c]] : 0.0;
-      g.gcon[r][c] = L.sym[r][c] >= 0 ? con[L.sym[r][c]] : 0.0;
+      g.gcon[r][c] = L.con[r][c] >= 0 ? con[L.con[r][c]] : 0.0;
     }
-  g.gdet = __ldg(tab + off + (2 * L.nsym) * plane);
-  g.sg = __ldg(tab + off + (2 * L.nsym + 1) * plane);
-  g.alpha = __ldg(tab + off + (2 * L.nsym + 2) * plane);
-  return __ldg(tab + off + (2 * L.nsym + 3) * plane) != 0.0;
+  const long long s0 = L.nsym + L.ncon;
+  g.gdet = __ldg(tab + off + s0 * plane);
+  g.sg = __ldg(tab + off + (s0 + 1) * plane);
+  g.alpha = __ldg(tab + off + (s0 + 2) * plane);
+  return __ldg(tab + off + (s0 + 3) * plane) != 0.0;
 }
 
 __device__ __forceinline__ void minkowski_geo(Geo &g) {
@@ -1041,15 +1048,15 @@ __global__ void __launch_bounds__(kThreads) k_build_tables(Dims d, pangu_params 
 #pragma unroll
   for (int r = 0; r < 4; ++r)
 #pragma unroll
-    for (int c = r; c < 4; ++c)
-      if (L.sym[r][c] >= 0) {
-        o[L.sym[r][c] * plane] = g.gcov[r][c];
-        o[(L.nsym + L.sym[r][c]) * plane] = g.gcon[r][c];
-      }
-  o[(2 * L.nsym) * plane] = g.gdet;
-  o[(2 * L.nsym + 1) * plane] = g.sg;
-  o[(2 * L.nsym + 2) * plane] = g.alpha;
-  o[(2 * L.nsym + 3) * plane] = ok ? 1.0 : 0.0;
+    for (int c = 0; c < 4; ++c) {
+      if (c >= r && L.sym[r][c] >= 0) o[L.sym[r][c] * plane] = g.gcov[r][c];
+      if (L.con[r][c] >= 0) o[(L.nsym + L.con[r][c]) * plane] = g.gcon[r][c];
+    }
+  const long long s0 = L.nsym + L.ncon;
+  o[s0 * plane] = g.gdet;
+  o[(s0 + 1) * plane] = g.sg;
+  o[(s0 + 2) * plane] = g.alpha;
+  o[(s0 + 3) * plane] = ok ? 1.0 : 0.0;
   if (which == 0) {
     double conn[4][4][4];
     christoffel<MT>(d, p, b, 0, j, i, g, conn);
