@@ -36,6 +36,11 @@ __host__ __forceinline__ PT *prim_of(const Pack *md) {
   return reinterpret_cast<PT *>(md->prim);
 }
 
+// CTA size of the per-cell kernels. FixPrimitive, the geometric source and
+// electron heating are bounded to 4 resident CTAs per SM (64 registers): the
+// extra occupancy outweighs their few spills (measured 2 % per RK2 cycle on
+// the 2D and 3D tori), and 148 x 1024 threads hold a 512 x 256 grid in one
+// wave. The first C2P pass keeps 3 (its Newton loop spills too much at 64).
 constexpr int kThreads = 256;
 constexpr int kT1Rows = 10;  // rows of the x1 table (host_tables.cc)
 
@@ -301,7 +306,7 @@ template <int MT>
 // interior cells from the primitives it has just stored, which is what
 // CalculateConservative (the next task of the stage) would read back
 // (with_b = 0: conserved B left as is, see k_calc_cons).
-__global__ void __launch_bounds__(kThreads) k_fix_primitive(Dims d, pangu_params p, PT *P,
+__global__ void __launch_bounds__(kThreads, 4) k_fix_primitive(Dims d, pangu_params p, PT *P,
                                                             unsigned long long *cnt, double *U,
                                                             int with_b) {
   int b, k, j, i;
@@ -1001,7 +1006,7 @@ __device__ __forceinline__ void source_cell(const Dims &d, const pangu_params &p
 }
 
 template <int MT>
-__global__ void __launch_bounds__(kThreads) k_source(Dims d, pangu_params p, const PT *P,
+__global__ void __launch_bounds__(kThreads, 4) k_source(Dims d, pangu_params p, const PT *P,
                                                      double *U, double beta, const double *dt) {
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1108,7 +1113,7 @@ __device__ __forceinline__ void heat_cell(const Dims &d, const pangu_params &p, 
 }
 
 template <int MT>
-__global__ void __launch_bounds__(kThreads) k_heating(Dims d, pangu_params p, PT *P,
+__global__ void __launch_bounds__(kThreads, 4) k_heating(Dims d, pangu_params p, PT *P,
                                                       const double *U) {
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
