@@ -314,6 +314,10 @@ int pangu_autotune(pangu_engine *e, const pangu_pack *md, void *stream);
 /* Current tile shapes: {march1, threads1, march2, threads2, march3,
  * threads3, tuned}. */
 int pangu_flux_config(const pangu_engine *e, int32_t out[7]);
+/* Sets the tile shapes {march1 (1), threads1, march2, threads2, march3,
+ * threads3}: march 1, 2 or 4, threads 64 or 128 (PANGU_EINVAL otherwise),
+ * e.g. to repeat a configuration the autotuner chose elsewhere. */
+int pangu_set_flux_config(pangu_engine *e, const int32_t cfg[6]);
 
 /* ---- block pool: many jobs stepped by the same launches ---------------- */
 /* No counterpart in the reference, which runs one mesh per process. A pool

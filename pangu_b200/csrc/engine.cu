@@ -88,6 +88,7 @@ int pangu_engine_destroy(pangu_engine *e) {
   cudaFree(e->d_genred);
   cudaFree(e->d_fail_vals);
   cudaFree(e->d_dtmin);
+  cudaFree(e->d_dt_ticket);
   cudaFree(e->d_hsend);
   cudaFree(e->d_hrecv);
   delete e;
@@ -178,6 +179,7 @@ int pool_init(pangu_engine *e, int capacity, int max_jobs) {
   rc |= dalloc(&e->d_fix_list, (size_t)e->fail_cap);
   rc |= dalloc(&e->d_fail_vals, (size_t)e->fail_cap * d.NF);
   rc |= dalloc(&e->d_dtmin, 3 * (size_t)capacity);
+  rc |= dalloc(&e->d_dt_ticket, 1);
   rc |= dalloc(&e->d_tmp_slots, capacity);
   rc |= dalloc(&e->d_genred, 3);
   // every ghost cell of a slot has at most one exchange source
@@ -196,6 +198,9 @@ int pool_init(pangu_engine *e, int capacity, int max_jobs) {
   bool ok = cudaMemset(e->d_cnt, 0, (size_t)max_jobs * PANGU_NCOUNTERS * 8) == cudaSuccess;
   ok &= cudaMemset(e->d_slot_job, 0, (size_t)capacity * sizeof(int)) == cudaSuccess;
   ok &= cudaMemset(e->d_bcf, 0xff, 6 * (size_t)capacity) == cudaSuccess;  // -1: no BC
+  ok &= cudaMemset(e->d_dt_ticket, 0, sizeof(unsigned int)) == cudaSuccess;
+  k_dt_init<<<grid_for(3 * capacity), kThreads>>>(3 * capacity, e->d_dtmin);
+  ok &= cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(0) == cudaSuccess;
   if (!ok) return PANGU_ECUDA;
   d.slot = e->d_active;
   d.slot_job = e->d_slot_job;
@@ -558,6 +563,21 @@ int pangu_flux_config(const pangu_engine *e, int32_t out[7]) {
     out[2 * d + 1] = e->tune.threads[d];
   }
   out[6] = e->tune.tuned;
+  return PANGU_OK;
+}
+
+int pangu_set_flux_config(pangu_engine *e, const int32_t cfg[6]) {
+  if (!e || !cfg) return PANGU_EINVAL;
+  for (int d = 0; d < 3; ++d) {
+    const int m = cfg[2 * d], t = cfg[2 * d + 1];
+    if ((d == 0 ? m != 1 : (m != 1 && m != 2 && m != 4)) || (t != 64 && t != 128))
+      return PANGU_EINVAL;
+  }
+  for (int d = 0; d < 3; ++d) {
+    e->tune.march[d] = cfg[2 * d];
+    e->tune.threads[d] = cfg[2 * d + 1];
+  }
+  e->tune.tuned = 1;
   return PANGU_OK;
 }
 

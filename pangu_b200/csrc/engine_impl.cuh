@@ -100,6 +100,7 @@ struct pangu_engine {
   double *d_fail_vals = nullptr;
   long long fail_cap = 0;
   unsigned long long *d_dtmin = nullptr;  // [capacity][3]
+  unsigned int *d_dt_ticket = nullptr;    // CTAs done in the current dt reduction
   long long launches = 0;  // kernels launched through this handle
   // Block sharding (one mesh over several GPUs): this engine holds the blocks
   // of `rank`; ghost cells whose source block is on another rank travel as

@@ -306,11 +306,17 @@ template <int MT>
 // interior cells from the primitives it has just stored, which is what
 // CalculateConservative (the next task of the stage) would read back
 // (with_b = 0: conserved B left as is, see k_calc_cons).
+// zero0, zero1 (may be null) are list counters of later tasks of the stage,
+// set to 0 here so that the stage needs no memset.
 __global__ void __launch_bounds__(kThreads, 4) k_fix_primitive(Dims d, pangu_params p, PT *P,
                                                             unsigned long long *cnt, double *U,
-                                                            int with_b) {
+                                                            int with_b, int *zero0, int *zero1) {
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0 && zero0) {
+    *zero0 = 0;
+    *zero1 = 0;
+  }
   if (!box_index(t, d.NB, 0, d.N3 - 1, 0, d.N2 - 1, 0, d.N1 - 1, b, k, j, i)) return;
   b = slot_of(d, b);
   const double gam = p.adiabatic_index;
@@ -761,28 +767,36 @@ __global__ void __launch_bounds__(kThreads) k_ct_emf(Dims d, const double *F1, c
   E[aidx(d, b, 2, k, j, i)] = e3;
 }
 
-// Face-B overwrite of direction dir (constrained_transport.cc:78-127).
-__global__ void __launch_bounds__(kThreads) k_ct_faces(Dims d, int dir, double *F,
-                                                       const double *E) {
+// Face-B overwrite (constrained_transport.cc:78-127) of every direction in
+// one launch: a thread at (k, j, i) of the union of the face ranges writes the
+// x1 face (i - 1/2) when j and k are interior, the x2 face when i and k are,
+// and the x3 face when i and j are.
+__global__ void __launch_bounds__(kThreads) k_ct_faces(Dims d, double *F1, double *F2,
+                                                       double *F3, const double *E) {
   int b, k, j, i;
   const int o1 = d.N1 > 1, o2 = d.N2 > 1, o3 = d.N3 > 1;
   const int E1 = o2 && o3, E2 = o3 && o1, E3 = o1 && o2;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int ei = dir == 1 ? o1 : 0, ej = dir == 2 ? o2 : 0, ek = dir == 3 ? o3 : 0;
-  if (!box_index(t, d.NB, d.ks, d.ke + ek, d.js, d.je + ej, d.is, d.ie + ei, b, k, j, i)) return;
+  if (!box_index(t, d.NB, d.ks, d.ke + o3, d.js, d.je + o2, d.is, d.ie + o1, b, k, j, i)) return;
   b = slot_of(d, b);
   const long long sj = d.N1, sk = (long long)d.N1 * d.N2;
   const long long e0 = aidx(d, b, 0, k, j, i), e1 = aidx(d, b, 1, k, j, i),
                   e2 = aidx(d, b, 2, k, j, i);
-  if (dir == 1) {
+  const bool in_i = i <= d.ie, in_j = j <= d.je, in_k = k <= d.ke;
+  if (in_j && in_k) {
+    double *F = F1;
     if (o1) F[vidx(d, b, BX1, k, j, i)] = 0;
     if (E2) F[vidx(d, b, BX3, k, j, i)] = -0.5 * (E[e1] + E[e1 + sk]);
     if (E3) F[vidx(d, b, BX2, k, j, i)] = 0.5 * (E[e2] + E[e2 + sj]);
-  } else if (dir == 2) {
+  }
+  if (d.ndim >= 2 && in_i && in_k) {
+    double *F = F2;
     if (E1) F[vidx(d, b, BX3, k, j, i)] = 0.5 * (E[e0] + E[e0 + sk]);
     if (o2) F[vidx(d, b, BX2, k, j, i)] = 0.;
     if (E3) F[vidx(d, b, BX1, k, j, i)] = -0.5 * (E[e2] + E[e2 + 1]);
-  } else {
+  }
+  if (d.ndim == 3 && in_i && in_j) {
+    double *F = F3;
     if (E1) F[vidx(d, b, BX2, k, j, i)] = -0.5 * (E[e0] + E[e0 + sj]);
     if (E2) F[vidx(d, b, BX1, k, j, i)] = 0.5 * (E[e1] + E[e1 + 1]);
     if (o3) F[vidx(d, b, BX3, k, j, i)] = 0;
@@ -1419,9 +1433,8 @@ __global__ void k_dt_init(int n, unsigned long long *mins) {
 // atomic per CTA and direction. Positive doubles order like their bit
 // patterns; a NaN speed never lowers the minimum (the reference's
 // "if (dt_min > dt)" skips it as well).
-__global__ void __launch_bounds__(kThreads) k_dt_reduce(Dims d, double cfl,
-                                                        const double *alfven,
-                                                        unsigned long long *mins) {
+__device__ __forceinline__ void dt_reduce_cta(const Dims &d, double cfl, const double *alfven,
+                                              unsigned long long *mins) {
   __shared__ unsigned long long red[3][kThreads / 32];
   const int b = slot_of(d, blockIdx.y);
   const int ni = d.ie - d.is + 1, nj = d.je - d.js + 1, nk = d.ke - d.ks + 1;
@@ -1466,13 +1479,19 @@ __global__ void __launch_bounds__(kThreads) k_dt_reduce(Dims d, double cfl,
   }
 }
 
-// One thread per job: the minimum over the job's blocks, active entries
-// jr[3q+1] .. jr[3q+2]-1 of job jr[3q] (the whole domain as job 0 when jr is
-// null), written to dt_out[job].
-__global__ void k_dt_finalize(Dims d, int njobs, const int *jr, const unsigned long long *mins,
-                              double *dt_out) {
-  if (blockIdx.x != 0) return;
-  for (int q = threadIdx.x; q < njobs; q += blockDim.x) {
+__global__ void __launch_bounds__(kThreads) k_dt_reduce(Dims d, double cfl,
+                                                        const double *alfven,
+                                                        unsigned long long *mins) {
+  dt_reduce_cta(d, cfl, alfven, mins);
+}
+
+// The minimum over the job's blocks of 1 / sum_d (1 / min_d), for jobs q =
+// first, first + stride, ... (active entries jr[3q+1] .. jr[3q+2]-1 of job
+// jr[3q]; the whole domain as job 0 when jr is null), written to dt_out[job].
+__device__ __forceinline__ void dt_finalize_jobs(const Dims &d, int njobs, const int *jr,
+                                                 const unsigned long long *mins, double *dt_out,
+                                                 int first, int stride) {
+  for (int q = first; q < njobs; q += stride) {
     const int job = jr ? jr[3 * q] : 0;
     const int s0 = jr ? jr[3 * q + 1] : 0, s1 = jr ? jr[3 * q + 2] : d.NB;
     double gmin = DBL_MAX;
@@ -1486,6 +1505,54 @@ __global__ void k_dt_finalize(Dims d, int njobs, const int *jr, const unsigned l
     }
     dt_out[job] = gmin;
   }
+}
+
+__global__ void k_dt_finalize(Dims d, int njobs, const int *jr, const unsigned long long *mins,
+                              double *dt_out) {
+  if (blockIdx.x != 0) return;
+  dt_finalize_jobs(d, njobs, jr, mins, dt_out, threadIdx.x, blockDim.x);
+}
+
+// The engine's dt estimate in one launch: every CTA reduces its part, and
+// the CTA that finishes last (a ticket taken after a fence, no waiting)
+// finalises every job, then puts the per-block minima back to DBL_MAX and the
+// ticket to 0 for the next call.
+__global__ void __launch_bounds__(kThreads) k_dt_reduce_final(Dims d, double cfl,
+                                                              const double *alfven,
+                                                              unsigned long long *mins,
+                                                              unsigned int *ticket, int njobs,
+                                                              const int *jr, double *dt_out,
+                                                              int nmins) {
+  __shared__ bool last;
+  dt_reduce_cta(d, cfl, alfven, mins);
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned int total = gridDim.x * gridDim.y;
+    last = atomicAdd(ticket, 1u) == total - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // every other CTA's atomics are complete; read the minima past L1
+  const volatile unsigned long long *vm = mins;
+  for (int q = threadIdx.x; q < njobs; q += blockDim.x) {
+    const int job = jr[3 * q];
+    double gmin = DBL_MAX;
+    for (int bb = jr[3 * q + 1]; bb < jr[3 * q + 2]; ++bb) {
+      const int b = slot_of(d, bb);
+      const double m0 = __longlong_as_double((long long)vm[3 * b + 0]);
+      const double m1 = __longlong_as_double((long long)vm[3 * b + 1]);
+      const double m2 = __longlong_as_double((long long)vm[3 * b + 2]);
+      const double bdt = 1.0 / (1.0 / m0 + 1.0 / m1 + 1.0 / m2);
+      if (bdt < gmin) gmin = bdt;
+    }
+    dt_out[job] = gmin;
+  }
+  __syncthreads();
+  const unsigned long long big = (unsigned long long)__double_as_longlong(DBL_MAX);
+  for (int t = threadIdx.x; t < nmins; t += blockDim.x) mins[t] = big;
+  if (threadIdx.x == 0) *ticket = 0u;
 }
 
 __global__ void k_update_dt(int njobs, const int *jr, double *dt, const double *dt_est,
@@ -1729,8 +1796,11 @@ bool pack_ok(const pangu_engine *e, const pangu_pack *md) {
 int run_fix_primitive(pangu_engine *e, const pangu_pack *md, bool with_cons, cudaStream_t s) {
   const Dims &d = e->d;
   const long long n = (long long)d.NB * d.ncell;
+  // on the stage path (with_cons) the C2P retry and FixRecovery list counters
+  // are zeroed here for Recovery
   DISPATCH_MT(e->p.metric_type, k_fix_primitive, grid_for(n), s, d, e->p, prim_of(md), e->d_cnt,
-              with_cons ? md->cons : nullptr, PGK_MIXED ? 0 : 1);
+              with_cons ? md->cons : nullptr, PGK_MIXED ? 0 : 1,
+              with_cons ? e->d_fail_count : nullptr, with_cons ? e->d_fix_count : nullptr);
   ++e->launches;
   return check_launch();
 }
@@ -1865,13 +1935,9 @@ int run_ct(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
   k_ct_emf<<<grid_for(box_count(d.NB, d.ks, d.ke + o3, d.js, d.je + o2, d.is, d.ie + o1)),
              kThreads, 0, s>>>(d, md->flux1, md->flux2, md->flux3, md->efield);
   ++e->launches;
-  double *F[3] = {md->flux1, md->flux2, md->flux3};
-  for (int dir = 1; dir <= d.ndim; ++dir) {
-    const int ei = dir == 1 ? o1 : 0, ej = dir == 2 ? o2 : 0, ek = dir == 3 ? o3 : 0;
-    const long long n = box_count(d.NB, d.ks, d.ke + ek, d.js, d.je + ej, d.is, d.ie + ei);
-    k_ct_faces<<<grid_for(n), kThreads, 0, s>>>(d, dir, F[dir - 1], md->efield);
-    ++e->launches;
-  }
+  k_ct_faces<<<grid_for(box_count(d.NB, d.ks, d.ke + o3, d.js, d.je + o2, d.is, d.ie + o1)),
+               kThreads, 0, s>>>(d, md->flux1, md->flux2, md->flux3, md->efield);
+  ++e->launches;
   return check_launch();
 }
 
@@ -1926,11 +1992,12 @@ int run_source(pangu_engine *e, const pangu_pack *md, double beta, const double 
 
 // Recovery; with list_fix the retry pass also lists the cells FixRecovery
 // repairs (the stage path).
+// list_fix: the stage path, whose FixPrimitive launch has zeroed both list
+// counters; otherwise the retry counter is zeroed here.
 int run_recovery(pangu_engine *e, const pangu_pack *md, bool list_fix, cudaStream_t s) {
   const Dims &d = e->d;
   const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
-  if (cudaMemsetAsync(e->d_fail_count, 0, sizeof(int), s) != cudaSuccess) return PANGU_ECUDA;
-  if (list_fix && cudaMemsetAsync(e->d_fix_count, 0, sizeof(int), s) != cudaSuccess)
+  if (!list_fix && cudaMemsetAsync(e->d_fail_count, 0, sizeof(int), s) != cudaSuccess)
     return PANGU_ECUDA;
   DISPATCH_MT(e->p.metric_type, k_recovery, grid_for(n), s, d, e->p, prim_of(md), md->cons, md->flag,
               e->d_cnt, e->d_fail_count, e->d_fail_list);
@@ -1998,13 +2065,13 @@ int run_bcs(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
 
 int run_estimate_dt(pangu_engine *e, const pangu_pack *md, double *dt_out, cudaStream_t s) {
   const Dims &d = e->d;
-  k_dt_init<<<grid_for(3 * e->capacity), kThreads, 0, s>>>(3 * e->capacity, e->d_dtmin);
   const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
   const unsigned gx = (unsigned)std::min<long long>((n / std::max(1, d.NB) + kThreads - 1) / kThreads, 592);
-  k_dt_reduce<<<dim3(std::max(1u, gx), d.NB), kThreads, 0, s>>>(d, e->p.cfl_number, md->alfven,
-                                                                 e->d_dtmin);
-  k_dt_finalize<<<1, 128, 0, s>>>(d, e->njobs_active, e->d_jr, e->d_dtmin, dt_out);
-  e->launches += 3;
+  // d_dtmin holds DBL_MAX and d_dt_ticket 0 between calls (set at pool_init)
+  k_dt_reduce_final<<<dim3(std::max(1u, gx), d.NB), kThreads, 0, s>>>(
+      d, e->p.cfl_number, md->alfven, e->d_dtmin, e->d_dt_ticket, e->njobs_active, e->d_jr, dt_out,
+      3 * e->capacity);
+  e->launches += 1;
   return check_launch();
 }
 

@@ -85,6 +85,7 @@ def lib():
                                               C.c_double, C.c_double, C.c_int64, C.c_double,
                                               C.POINTER(abi.Problem), C.POINTER(C.c_int32)]
     L.pangu_flux_config.argtypes = [_P, C.POINTER(C.c_int32)]
+    L.pangu_set_flux_config.argtypes = [_P, C.POINTER(C.c_int32)]
     L.pangu_server_create.argtypes = [C.c_uint64, C.POINTER(_P)]
     L.pangu_server_destroy.argtypes = [_P]
     L.pangu_server_add_class.argtypes = [_P, C.POINTER(abi.Params), C.POINTER(abi.Mesh), C.c_int32,
@@ -308,6 +309,12 @@ class Engine:
         v = list(out)
         return {"x1_threads": v[1], "x2_march": v[2], "x2_threads": v[3],
                 "x3_march": v[4], "x3_threads": v[5], "tuned": bool(v[6])}
+
+    def set_flux_config(self, x1_threads=128, x2_march=2, x2_threads=128, x3_march=2,
+                        x3_threads=128, **_):
+        """Sets the flux tile shapes (the keys of flux_config())."""
+        cfg = (C.c_int32 * 6)(1, x1_threads, x2_march, x2_threads, x3_march, x3_threads)
+        _check(self.L.pangu_set_flux_config(self.h, cfg), "pangu_set_flux_config")
 
     # ---- block pool --------------------------------------------------------
     def attach(self, mesh: abi.Mesh, a: float, h: float):
