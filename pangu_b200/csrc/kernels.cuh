@@ -284,6 +284,21 @@ __device__ __forceinline__ bool box_index(long long t, int NB, int k0, int k1, i
   if (ni <= 0 || nj <= 0 || nk <= 0) return false;
   const long long per = ni * nj * nk;
   if (t >= per * NB) return false;
+  if (per * NB <= 0x7fffffffLL) {
+    // 32-bit unsigned division (a 64-bit one is a long software routine)
+    const unsigned ut = (unsigned)t, up = (unsigned)per, uij = (unsigned)(ni * nj),
+                   ui = (unsigned)ni;
+    const unsigned ub = ut / up;
+    unsigned r = ut - ub * up;
+    const unsigned uk = r / uij;
+    r -= uk * uij;
+    const unsigned uj = r / ui;
+    b = (int)ub;
+    k = k0 + (int)uk;
+    j = j0 + (int)uj;
+    i = i0 + (int)(r - uj * ui);
+    return true;
+  }
   b = (int)(t / per);
   long long r = t - (long long)b * per;
   k = k0 + (int)(r / (ni * nj));
@@ -291,6 +306,33 @@ __device__ __forceinline__ bool box_index(long long t, int NB, int k0, int k1, i
   j = j0 + (int)(r / ni);
   i = i0 + (int)(r - (long long)(j - j0) * ni);
   return true;
+}
+
+// q = a / b and r = a % b for a >= 0, b > 0, in 32-bit arithmetic when both
+// fit (a 64-bit division is a long software routine).
+__device__ __forceinline__ long long div_fast(long long a, long long b, long long &r) {
+  if (((a | b) >> 31) == 0) {
+    const unsigned q = (unsigned)a / (unsigned)b;
+    r = (unsigned)a - q * (unsigned)b;
+    return q;
+  }
+  const long long q = a / b;
+  r = a - q * b;
+  return q;
+}
+
+// Block and in-block offset of a cell offset c = b * ncell + o.
+__device__ __forceinline__ void split_cell(long long c, long long ncell, long long &b,
+                                           long long &o) {
+  if (c <= 0x7fffffffLL && ncell <= 0x7fffffffLL) {
+    const unsigned uc = (unsigned)c, un = (unsigned)ncell;
+    const unsigned ub = uc / un;
+    b = ub;
+    o = uc - ub * un;
+  } else {
+    b = c / ncell;
+    o = c - b * ncell;
+  }
 }
 
 inline unsigned grid_for(long long n) {
@@ -648,13 +690,13 @@ __global__ void __launch_bounds__(kFluxThreads, 4) k_flux_x1(Dims d, pangu_param
   const int nseg = (nf + kFacesPerWarp - 1) / kFacesPerWarp;
   const long long nrow = (long long)(k1 - k0 + 1) * (j1 - j0 + 1);
   if (warp >= nrow * d.NB * nseg) return;  // whole warps exit together
-  const int seg = (int)(warp % nseg);
-  const long long row = warp / nseg;
-  const int bb = (int)(row / nrow);
-  const long long rr = row - (long long)bb * nrow;
+  long long seg_l, rr, jr;
+  const long long row = div_fast(warp, nseg, seg_l);
+  const int seg = (int)seg_l;
+  const int bb = (int)div_fast(row, nrow, rr);
   const int b = slot_of(d, bb);
-  const int k = k0 + (int)(rr / (j1 - j0 + 1));
-  const int j = j0 + (int)(rr % (j1 - j0 + 1));
+  const int k = k0 + (int)div_fast(rr, j1 - j0 + 1, jr);
+  const int j = j0 + (int)jr;
   const int c = i0 - 1 + seg * kFacesPerWarp + lane;
   const bool active = c <= i1;  // cell c is needed by face c (and c + 1)
   const bool use_mc = p.limiter == PANGU_LIMITER_MC;
@@ -686,12 +728,13 @@ __device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_param
   const int nruns = (m1 - m0 + 1 + MARCH - 1) / MARCH;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)d.NB * na * nruns * ni) return;
-  const int i = i0 + (int)(t % ni);
-  long long r = t / ni;
-  const int run = (int)(r % nruns);
-  r /= nruns;
-  const int a = a0 + (int)(r % na);
-  const int b = slot_of(d, (int)(r / na));
+  long long ir, runr, ar;
+  long long r = div_fast(t, ni, ir);
+  const int i = i0 + (int)ir;
+  r = div_fast(r, nruns, runr);
+  const int run = (int)runr;
+  const int b = slot_of(d, (int)div_fast(r, na, ar));
+  const int a = a0 + (int)ar;
   const long long stride = DIR == 2 ? (long long)d.N1 : (long long)d.N1 * d.N2;
   const bool use_mc = p.limiter == PANGU_LIMITER_MC;
   const int f0 = m0 + run * MARCH;
@@ -840,9 +883,11 @@ __global__ void __launch_bounds__(kThreads) k_exchange(Dims d, long long n, cons
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const long long dc = dst[t], sc = src[t];
-  const long long db = dc / d.ncell, sb = sc / d.ncell;
-  const long long dp = db * d.NF * d.ncell + (dc - db * d.ncell);
-  const long long sp = sb * d.NF * d.ncell + (sc - sb * d.ncell);
+  long long db, dof, sb, sof;
+  split_cell(dc, d.ncell, db, dof);
+  split_cell(sc, d.ncell, sb, sof);
+  const long long dp = db * d.NF * d.ncell + dof;
+  const long long sp = sb * d.NF * d.ncell + sof;
   for (int v = 0; v < d.NF; ++v) P[dp + v * d.ncell] = P[sp + v * d.ncell];
   if (flag) flag[dc] = flag[sc];
 }
@@ -857,8 +902,9 @@ __global__ void __launch_bounds__(kThreads) k_halo_pack(Dims d, long long n, con
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const long long c = cells[t];
-  const long long b = c / d.ncell;
-  const long long q = b * d.NF * d.ncell + (c - b * d.ncell);
+  long long b, off;
+  split_cell(c, d.ncell, b, off);
+  const long long q = b * d.NF * d.ncell + off;
   double *o = buf + t * (d.NF + 1);
   for (int v = 0; v < d.NF; ++v) o[v] = (double)P[q + v * d.ncell];
   o[d.NF] = flag ? flag[c] : 0.0;
@@ -870,8 +916,9 @@ __global__ void __launch_bounds__(kThreads) k_halo_unpack(Dims d, long long n,
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const long long c = cells[t];
-  const long long b = c / d.ncell;
-  const long long q = b * d.NF * d.ncell + (c - b * d.ncell);
+  long long b, off;
+  split_cell(c, d.ncell, b, off);
+  const long long q = b * d.NF * d.ncell + off;
   const double *o = buf + t * (d.NF + 1);
   for (int v = 0; v < d.NF; ++v) P[q + v * d.ncell] = (PT)o[v];
   if (flag) flag[c] = o[d.NF];
@@ -1371,15 +1418,10 @@ __global__ void __launch_bounds__(kThreads) k_fixrec_write(Dims d, const int *co
 __global__ void __launch_bounds__(kThreads) k_bcs(Dims d, int enable_B, PT *P,
                                                   double *flag) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)d.NB * d.ncell) return;
-  const int bb = (int)(t / d.ncell);
-  long long c = t - (long long)bb * d.ncell;
+  int bb, idx[3];
+  if (!box_index(t, d.NB, 0, d.N3 - 1, 0, d.N2 - 1, 0, d.N1 - 1, bb, idx[2], idx[1], idx[0]))
+    return;
   const int b = slot_of(d, bb);
-  int idx[3];
-  idx[2] = (int)(c / ((long long)d.N2 * d.N1));
-  c -= (long long)idx[2] * d.N2 * d.N1;
-  idx[1] = (int)(c / d.N1);
-  idx[0] = (int)(c % d.N1);
   const signed char *bcf = d.bcf + 6 * b;  // -1 unless the face is a physical boundary
   const int st[3] = {d.is, d.js, d.ks}, en[3] = {d.ie, d.je, d.ke};
   int src[3] = {idx[0], idx[1], idx[2]};
@@ -1446,10 +1488,8 @@ __device__ __forceinline__ void dt_reduce_cta(const Dims &d, double cfl, const d
   const int act[3] = {d.N1 > 1, d.N2 > 1, d.N3 > 1};
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < per;
        t += (long long)gridDim.x * blockDim.x) {
-    const int k = d.ks + (int)(t / ((long long)ni * nj));
-    const long long r = t - (long long)(k - d.ks) * ni * nj;
-    const int j = d.js + (int)(r / ni);
-    const int i = d.is + (int)(r - (long long)(j - d.js) * ni);
+    int bz, k, j, i;
+    box_index(t, 1, d.ks, d.ke, d.js, d.je, d.is, d.ie, bz, k, j, i);
 #pragma unroll
     for (int dir = 0; dir < 3; ++dir) {
       if (!act[dir]) continue;
