@@ -441,6 +441,19 @@ class Simulation:
                  dt=self.dt.cpu().numpy(), cycle=np.int64(self.cycle),
                  inputfile=np.array(self.pin.dump()))
 
+    def write_xdmf(self, prefix: str, time: float = 0.0) -> str:
+        """The primitive fields as <prefix>.bin described by <prefix>.xdmf
+        (pangu_b200.output)."""
+        from .output import write_xdmf
+        return write_xdmf(prefix, self.primitives(), self.mesh, bool(self.params.enable_B),
+                          bool(self.params.enable_heating), self.cycle, time)
+
+    def write_phdf(self, path: str, time: float = 0.0) -> str:
+        """The primitive fields in the Parthenon .phdf layout (needs h5py)."""
+        from .output import write_phdf
+        return write_phdf(path, self.primitives(), self.mesh, bool(self.params.enable_B),
+                          bool(self.params.enable_heating), self.cycle, time)
+
     @classmethod
     def restart(cls, path: str, device=0) -> "Simulation":
         """A job continued from a checkpoint written by save(): its next
