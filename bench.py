@@ -431,36 +431,21 @@ def run_sharded(args):
 
 
 def e2e_run(sim, torch, dev, steps):
-    """Steps with the job state resident on the HOST: every step copies the
-    state in from pinned memory, runs the RK2 cycle and copies it back."""
-    base, one = sim.base, sim.one
-    h_base = torch.empty(base.prim.shape, dtype=base.prim.dtype).pin_memory()
-    h_one = torch.empty(one.prim.shape, dtype=one.prim.dtype).pin_memory()
-    h_flag = torch.empty(base.flag.shape, dtype=torch.float64).pin_memory()
-    h_dt = torch.empty(1, dtype=torch.float64).pin_memory()
-    h_base.copy_(base.prim)
-    h_one.copy_(one.prim)
-    h_flag.copy_(base.flag)
-    h_dt.copy_(sim.dt)
-    torch.cuda.synchronize()
+    """Steps with the job state resident on the HOST, through the public API
+    (Simulation.step_host): every step copies the state in from pinned memory,
+    runs the RK2 cycle and copies it back, the copies overlapped with the
+    kernels that do not need them."""
+    from pangu_b200.engine import HostState
+    host = HostState(sim)
+    sim.pull(host)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(steps):
-        base.prim.copy_(h_base, non_blocking=True)
-        one.prim.copy_(h_one, non_blocking=True)
-        base.flag.copy_(h_flag, non_blocking=True)
-        sim.dt.copy_(h_dt, non_blocking=True)
-        sim.step()
-        h_base.copy_(base.prim, non_blocking=True)
-        h_one.copy_(one.prim, non_blocking=True)
-        h_flag.copy_(base.flag, non_blocking=True)
-        h_dt.copy_(sim.dt, non_blocking=True)
+        sim.step_host(host)
     e1.record()
     torch.cuda.synchronize()
-    nbytes = (h_base.numel() * h_base.element_size() + h_one.numel() * h_one.element_size() +
-              h_flag.numel() * 8 + 8)
-    return {"ms": e0.elapsed_time(e1), "steps": steps, "h2d": nbytes, "d2h": nbytes}
+    return {"ms": e0.elapsed_time(e1), "steps": steps, "h2d": host.nbytes, "d2h": host.nbytes}
 
 
 def task_times(sim, torch, flush, reps=20):

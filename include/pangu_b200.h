@@ -267,6 +267,14 @@ int pangu_halo_unpack(pangu_engine *e, const pangu_pack *md,
 int pangu_stage_begin(pangu_engine *e, int stage, const pangu_pack *base,
                       const pangu_pack *one, double beta, const double *dt,
                       double *send, void *stream);
+/* The first part without its exchange: FixPrimitive + CalculateConservative,
+ * fluxes, CT and the update, which read only mc0 and "base" and write mc1's
+ * conserved variables. pangu_stage_update then pangu_exchange_ghosts (mc1)
+ * equals pangu_stage_begin on an engine without halo entries; a caller that
+ * uploads mc1's primitives and the flags can let that copy run meanwhile. */
+int pangu_stage_update(pangu_engine *e, int stage, const pangu_pack *base,
+                       const pangu_pack *one, double beta, const double *dt,
+                       void *stream);
 int pangu_stage_middle(pangu_engine *e, int stage, const pangu_pack *base,
                        const pangu_pack *one, double beta, const double *dt,
                        void *stream);

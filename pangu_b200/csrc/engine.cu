@@ -36,6 +36,8 @@ int run_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pa
               double beta, const double *dt, double *dt_est, cudaStream_t s);
 int run_stage_begin(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
                     double beta, const double *dt, double *send, cudaStream_t s);
+int run_stage_update(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
+                     double beta, const double *dt, cudaStream_t s);
 int run_stage_middle(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
                      double beta, const double *dt, cudaStream_t s);
 int run_stage_end(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
@@ -675,6 +677,14 @@ int pangu_stage_begin(pangu_engine *e, int stage, const pangu_pack *base, const 
     return PANGU_EINVAL;
   if (e->d.NB == 0) return PANGU_OK;
   return RUN(run_stage_begin, e, stage, base, one, beta, dt, send, S(stream));
+}
+
+int pangu_stage_update(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
+                       double beta, const double *dt, void *stream) {
+  if (!pack_ok(e, base) || !pack_ok(e, one) || !dt || (stage != 1 && stage != 2))
+    return PANGU_EINVAL;
+  if (e->d.NB == 0) return PANGU_OK;
+  return RUN(run_stage_update, e, stage, base, one, beta, dt, S(stream));
 }
 
 int pangu_stage_middle(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,

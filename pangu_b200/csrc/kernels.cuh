@@ -2127,8 +2127,11 @@ int dalloc(T **p, size_t n) {
 // FixRecovery (neighbour means) and by the next stage.
 // Part 1: FixPrimitive + CalculateConservative, fluxes, CT, update, ghost
 // exchange at send time; the halo cells of mc1 go to `send` (sharded only).
-int run_stage_begin(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
-                    double beta, const double *dt, double *send, cudaStream_t s) {
+// Part 1 without the exchange: FixPrimitive + CalculateConservative, fluxes,
+// CT and the update; reads only mc0 and mc_init, writes mc1's conserved
+// variables.
+int run_stage_update(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
+                     double beta, const double *dt, cudaStream_t s) {
   const pangu_pack *mc0 = stage == 1 ? base : one;
   const pangu_pack *mc1 = stage == 1 ? one : base;
   int rc;
@@ -2149,6 +2152,14 @@ int run_stage_begin(pangu_engine *e, int stage, const pangu_pack *base, const pa
     TaskRange r("FluxDivergence+UpdateIndependentData");
     if ((rc = run_update(e, base, mc0, mc1, beta, dt, s))) return rc;
   }
+  return PANGU_OK;
+}
+
+int run_stage_begin(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
+                    double beta, const double *dt, double *send, cudaStream_t s) {
+  const pangu_pack *mc1 = stage == 1 ? one : base;
+  int rc = run_stage_update(e, stage, base, one, beta, dt, s);
+  if (rc) return rc;
   {
     TaskRange r("GhostExchange");
     if ((rc = run_exchange(e, mc1, s))) return rc;

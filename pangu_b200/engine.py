@@ -109,6 +109,7 @@ def lib():
     L.pangu_halo_unpack.argtypes = [_P, _PK, _DP, _P]
     L.pangu_stage_begin.argtypes = [_P, C.c_int, _PK, _PK, C.c_double, _DP, _DP, _P]
     L.pangu_stage_middle.argtypes = [_P, C.c_int, _PK, _PK, C.c_double, _DP, _P]
+    L.pangu_stage_update.argtypes = [_P, C.c_int, _PK, _PK, C.c_double, _DP, _P]
     L.pangu_stage_end.argtypes = [_P, C.c_int, _PK, _PK, _DP, _DP, _P]
     _lib = L
     return L
@@ -270,6 +271,10 @@ class Engine:
         _check(self.L.pangu_stage_begin(self.h, st, base.pack, one.pack, beta, dt_dev.data_ptr(),
                                         _ptr(send), self.stream()), "pangu_stage_begin")
 
+    def stage_update(self, st, base, one, beta, dt_dev):
+        _check(self.L.pangu_stage_update(self.h, st, base.pack, one.pack, beta, dt_dev.data_ptr(),
+                                         self.stream()), "pangu_stage_update")
+
     def stage_middle(self, st, base, one, beta, dt_dev):
         _check(self.L.pangu_stage_middle(self.h, st, base.pack, one.pack, beta, dt_dev.data_ptr(),
                                          self.stream()), "pangu_stage_middle")
@@ -346,6 +351,23 @@ class Engine:
 RK2_BETA = (1.0, 0.5)
 
 
+class HostState:
+    """A job's state in pinned host memory: what one RK2 cycle reads and
+    writes (both containers' primitives, the flags and dt)."""
+
+    def __init__(self, sim: "Simulation"):
+        _torch()
+        import torch
+        pin = lambda t: torch.empty(t.shape, dtype=t.dtype).pin_memory()  # noqa: E731
+        self.base_prim, self.one_prim = pin(sim.base.prim), pin(sim.one.prim)
+        self.flag, self.dt = pin(sim.base.flag), pin(sim.dt)
+
+    @property
+    def nbytes(self) -> int:
+        return sum(t.numel() * t.element_size()
+                   for t in (self.base_prim, self.one_prim, self.flag, self.dt))
+
+
 class Simulation:
     """A job: packages, mesh, the two stage containers and the dt policy.
 
@@ -369,6 +391,7 @@ class Simulation:
         self.dt_est = torch.zeros(1, dtype=torch.float64, device=dev)
         self.cycle = 0
         self._graph = None
+        self._copy_streams = None
 
     def set_primitives(self, prim: np.ndarray):
         """Loads initial primitives (interior values; ghosts are filled here:
@@ -421,6 +444,66 @@ class Simulation:
             self._graph.replay()
         else:
             self._step_launches(fixed_dt)
+        self.cycle += 1
+
+    def pull(self, host: HostState):
+        """Copies the job's state to host memory (synchronous)."""
+        import torch
+        host.base_prim.copy_(self.base.prim)
+        host.one_prim.copy_(self.one.prim)
+        host.flag.copy_(self.base.flag)
+        host.dt.copy_(self.dt)
+        torch.cuda.synchronize(self.engine.device)
+
+    def step_host(self, host: HostState, fixed_dt: bool = False):
+        """One rk2 cycle of a job whose state lives in pinned host memory: the
+        state is copied in, stepped and copied back, with the transfers
+        overlapped with the kernels that do not need them and with each
+        other (host-to-device and device-to-host run at the same time).
+        Container "base" and dt go in first (stage 1 starts from them);
+        container "1" and the flags go in on a second stream while stage 1
+        runs up to its update (pangu_stage_update: the ghost exchange is their
+        first reader). After stage 2's update container "1" is final and goes
+        back on a third stream while the rest of stage 2 runs; then the flags
+        and dt on that stream and "base" on the main one, which the next
+        cycle's inputs of container "1" and the flags overlap. Gives the bits
+        of step() on the device-resident state."""
+        import torch
+        dev = self.engine.device
+        s = torch.cuda.current_stream(dev)
+        if self._copy_streams is None:
+            self._copy_streams = (torch.cuda.Stream(dev), torch.cuda.Stream(dev))
+        cin, cout = self._copy_streams
+        eng, base, one = self.engine, self.base, self.one
+        # the previous cycle's copies back of container "1", the flags and dt
+        # (and every kernel that read or wrote them) are complete
+        cin.wait_stream(cout)
+        s.wait_stream(cout)
+        base.prim.copy_(host.base_prim, non_blocking=True)
+        self.dt.copy_(host.dt, non_blocking=True)
+        with torch.cuda.stream(cin):
+            one.prim.copy_(host.one_prim, non_blocking=True)
+            base.flag.copy_(host.flag, non_blocking=True)
+        eng.stage_update(1, base, one, RK2_BETA[1], self.dt)
+        s.wait_stream(cin)
+        eng.exchange_ghosts(one)
+        eng.stage_middle(1, base, one, RK2_BETA[1], self.dt)
+        eng.stage_end(1, base, one, None)
+        eng.stage_update(2, base, one, RK2_BETA[0], self.dt)
+        cout.wait_stream(s)
+        with torch.cuda.stream(cout):
+            host.one_prim.copy_(one.prim, non_blocking=True)
+        eng.exchange_ghosts(base)
+        eng.stage_middle(2, base, one, RK2_BETA[0], self.dt)
+        eng.stage_end(2, base, one, None, self.dt_est)
+        if not fixed_dt:
+            eng.update_dt(self.dt, self.dt_est, self.dt_factor)
+        cout.wait_stream(s)
+        with torch.cuda.stream(cout):
+            host.flag.copy_(base.flag, non_blocking=True)
+            host.dt.copy_(self.dt, non_blocking=True)
+        host.base_prim.copy_(base.prim, non_blocking=True)
+        s.wait_stream(cout)
         self.cycle += 1
 
     def primitives(self) -> np.ndarray:
