@@ -326,7 +326,9 @@ def run_engine(args):
                 "algorithmic_bytes_per_launch": tb[dom], "launch_ms": round(tasks[dom], 5),
                 "step_algorithmic_bytes": step_bytes,
                 "step_achieved_gbs": round(step_bytes * value / n_int / world / 1e9, 2),
-                "task_ms": {k: round(v, 5) for k, v in tasks.items()}}
+                "task_ms": {k: round(v, 5) for k, v in tasks.items()},
+                "fp64_pipe_active_pct": committed_fp64_pipe(
+                    dom, workload_name(args.workload, args.precision))}
         tiles = sim.engine.flux_config()
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
@@ -488,6 +490,24 @@ def committed_traffic(kernel, workload):
     """DRAM bytes per launch of a task from the committed ncu summary
     (profiles/traffic_<workload>.txt: lines 'task bytes'), or None."""
     path = os.path.join(ROOT, "profiles", f"traffic_{workload}.txt")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for line in f:
+            parts = line.split()
+            if len(parts) >= 2 and parts[0] == kernel:
+                try:
+                    return float(parts[1])
+                except ValueError:
+                    return None
+    return None
+
+
+def committed_fp64_pipe(kernel, workload):
+    """FP64 pipe utilisation of a task's kernels in per cent of peak (ncu
+    sm__pipe_fp64_cycles_active, from the committed full captures in
+    profiles/fp64_pipe_<workload>.txt: lines 'task pct'), or None."""
+    path = os.path.join(ROOT, "profiles", f"fp64_pipe_{workload}.txt")
     if not os.path.exists(path):
         return None
     with open(path) as f:
