@@ -783,7 +783,8 @@ int pangu_update_dt(pangu_engine *e, double *dt, const double *dt_est, double dt
                     void *stream) {
   if (!e || !dt || !dt_est) return PANGU_EINVAL;
   if (e->njobs_active == 0) return PANGU_OK;
-  k_update_dt<<<1, 128, 0, S(stream)>>>(e->njobs_active, e->d_jr, dt, dt_est, dt_factor);
+  launch_pdl(k_update_dt, dim3(1), dim3(128), S(stream), e->njobs_active, (const int *)e->d_jr, dt,
+             dt_est, dt_factor);
   ++e->launches;
   return check_launch();
 }

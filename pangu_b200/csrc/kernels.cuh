@@ -40,8 +40,24 @@ __host__ __forceinline__ PT *prim_of(const Pack *md) {
 // electron heating are bounded to 4 resident CTAs per SM (64 registers): the
 // extra occupancy outweighs their few spills (measured 2 % per RK2 cycle on
 // the 2D and 3D tori), and 148 x 1024 threads hold a 512 x 256 grid in one
-// wave. The first C2P pass keeps 3 (its Newton loop spills too much at 64).
+// wave. The first C2P pass runs in CTAs of 128 threads bounded to 7 per SM
+// (72 registers, a few spills): 148 x 896 threads hold the 512 x 256 grid in
+// one wave (1.2 % per cycle; at 64 registers its Newton loop spills too much).
 constexpr int kThreads = 256;
+constexpr int kRecoveryThreads = 128;
+
+// Programmatic dependent launch: the stage's kernels are launched with
+// programmatic stream serialisation (launch_pdl), so the launch of a kernel
+// overlaps the end of the previous one. Every kernel therefore first waits
+// until the previous grid has completed and its writes are visible
+// (griddepcontrol.wait; a no-op in a normal launch). No kernel triggers its
+// dependents early: measured, an early trigger (dependents' CTAs resident
+// and waiting during the last wave) cost 4 % per cycle on the 2D torus, while
+// the launch overlap alone gains 2.6 % on the 256^2 Orszag-Tang problem and
+// is neutral on the tori.
+__device__ __forceinline__ void pdl_grid_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
 constexpr int kT1Rows = 10;  // rows of the x1 table (host_tables.cc)
 
 __device__ __forceinline__ int slot_of(const Dims &d, int bb) {
@@ -353,6 +369,7 @@ template <int MT>
 __global__ void __launch_bounds__(kThreads, 4) k_fix_primitive(Dims d, pangu_params p, PT *P,
                                                             unsigned long long *cnt, double *U,
                                                             int with_b, int *zero0, int *zero1) {
+  pdl_grid_wait();
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t == 0 && zero0) {
@@ -475,6 +492,7 @@ template <int MT>
 // FP32-stored primitives every stage would add FP32 rounding to div B.
 __global__ void __launch_bounds__(kThreads) k_calc_cons(Dims d, pangu_params p, const PT *P,
                                                         double *U, int with_b) {
+  pdl_grid_wait();
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
@@ -684,6 +702,7 @@ __global__ void __launch_bounds__(kFluxThreads, 4) k_flux_x1(Dims d, pangu_param
                                                       int j0, int j1, int i0, int i1,
                                                       const PT *P, double *F,
                                                       double *alfven) {
+  pdl_grid_wait();
   const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const int nf = i1 - i0 + 1;
@@ -771,6 +790,7 @@ __global__ void __launch_bounds__(kFluxThreads, 4) k_flux_march2(Dims d, pangu_p
                                                           int j0, int j1, int i0, int i1,
                                                           const PT *P, double *F,
                                                           double *alfven) {
+  pdl_grid_wait();
   flux_march_body<MT, 2, MARCH>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
 }
 template <int MT, int MARCH>
@@ -778,6 +798,7 @@ __global__ void __launch_bounds__(kFluxThreads, 4) k_flux_march3(Dims d, pangu_p
                                                           int j0, int j1, int i0, int i1,
                                                           const PT *P, double *F,
                                                           double *alfven) {
+  pdl_grid_wait();
   flux_march_body<MT, 3, MARCH>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
 }
 
@@ -786,6 +807,7 @@ __global__ void __launch_bounds__(kFluxThreads, 4) k_flux_march3(Dims d, pangu_p
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kThreads) k_ct_emf(Dims d, const double *F1, const double *F2,
                                                      const double *F3, double *E) {
+  pdl_grid_wait();
   int b, k, j, i;
   const int o1 = d.N1 > 1, o2 = d.N2 > 1, o3 = d.N3 > 1;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -816,6 +838,7 @@ __global__ void __launch_bounds__(kThreads) k_ct_emf(Dims d, const double *F1, c
 // and the x3 face when i and j are.
 __global__ void __launch_bounds__(kThreads) k_ct_faces(Dims d, double *F1, double *F2,
                                                        double *F3, const double *E) {
+  pdl_grid_wait();
   int b, k, j, i;
   const int o1 = d.N1 > 1, o2 = d.N2 > 1, o3 = d.N3 > 1;
   const int E1 = o2 && o3, E2 = o3 && o1, E3 = o1 && o2;
@@ -853,6 +876,7 @@ __global__ void __launch_bounds__(kThreads) k_flux_div_update(Dims d, const doub
                                                               const double *F2, const double *F3,
                                                               const double *Uinit, double *Uout,
                                                               double beta, const double *dt) {
+  pdl_grid_wait();
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB * d.NF, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
@@ -880,6 +904,7 @@ __global__ void __launch_bounds__(kThreads) k_flux_div_update(Dims d, const doub
 __global__ void __launch_bounds__(kThreads) k_exchange(Dims d, long long n, const long long *dst,
                                                        const long long *src, PT *P,
                                                        double *flag) {
+  pdl_grid_wait();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const long long dc = dst[t], sc = src[t];
@@ -899,6 +924,7 @@ __global__ void __launch_bounds__(kThreads) k_exchange(Dims d, long long n, cons
 __global__ void __launch_bounds__(kThreads) k_halo_pack(Dims d, long long n, const long long *cells,
                                                         const PT *P, const double *flag,
                                                         double *buf) {
+  pdl_grid_wait();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const long long c = cells[t];
@@ -913,6 +939,7 @@ __global__ void __launch_bounds__(kThreads) k_halo_pack(Dims d, long long n, con
 __global__ void __launch_bounds__(kThreads) k_halo_unpack(Dims d, long long n,
                                                           const long long *cells, PT *P,
                                                           double *flag, const double *buf) {
+  pdl_grid_wait();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const long long c = cells[t];
@@ -1069,6 +1096,7 @@ __device__ __forceinline__ void source_cell(const Dims &d, const pangu_params &p
 template <int MT>
 __global__ void __launch_bounds__(kThreads, 4) k_source(Dims d, pangu_params p, const PT *P,
                                                      double *U, double beta, const double *dt) {
+  pdl_grid_wait();
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
@@ -1084,6 +1112,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_source(Dims d, pangu_params p, 
 template <int MT>
 __global__ void __launch_bounds__(kThreads) k_build_tables(Dims d, pangu_params p, double *ctab,
                                                            double *f1tab, double *f2tab) {
+  pdl_grid_wait();
   constexpr TabLayout L = tab_layout(MT);
   const long long pc = (long long)d.N2 * d.N1, p1 = (long long)d.N2 * (d.N1 + 1),
                   p2 = (long long)(d.N2 + 1) * d.N1;
@@ -1176,6 +1205,7 @@ __device__ __forceinline__ void heat_cell(const Dims &d, const pangu_params &p, 
 template <int MT>
 __global__ void __launch_bounds__(kThreads, 4) k_heating(Dims d, pangu_params p, PT *P,
                                                       const double *U) {
+  pdl_grid_wait();
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
@@ -1253,10 +1283,11 @@ __device__ __forceinline__ void c2p_write(const Dims &d, PT *P, int b, int k, in
 // (Folding the geometric source and electron heating into this kernel was
 // measured slower: their registers cut the occupancy of the Newton loops.)
 template <int MT>
-__global__ void __launch_bounds__(kThreads, 3) k_recovery(Dims d, pangu_params p, PT *P,
+__global__ void __launch_bounds__(kRecoveryThreads, 7) k_recovery(Dims d, pangu_params p, PT *P,
                                                        const double *U, double *flag,
                                                        unsigned long long *cnt, int *nretry,
                                                        long long *retry) {
+  pdl_grid_wait();
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
@@ -1307,6 +1338,7 @@ __global__ void __launch_bounds__(kThreads) k_recovery_retry(Dims d, pangu_param
                                                              const int *nretry,
                                                              const long long *retry,
                                                              int *nfix, long long *fix) {
+  pdl_grid_wait();
   const int n = *nretry;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x) {
@@ -1342,6 +1374,7 @@ __global__ void __launch_bounds__(kThreads) k_recovery_retry(Dims d, pangu_param
 __global__ void __launch_bounds__(kThreads) k_fixrec_scan(Dims d, pangu_params p,
                                                           const double *flag, int *count_out,
                                                           long long *list) {
+  pdl_grid_wait();
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
@@ -1363,6 +1396,7 @@ __global__ void __launch_bounds__(kThreads) k_fixrec_compute(Dims d, const int *
                                                              const long long *list,
                                                              const PT *P, const double *flag,
                                                              double *vals) {
+  pdl_grid_wait();
   const int n = *count_in;
   const int off2 = d.js != d.je ? 1 : 0;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
@@ -1394,6 +1428,7 @@ __global__ void __launch_bounds__(kThreads) k_fixrec_write(Dims d, const int *co
                                                            const double *vals, PT *P,
                                                            double *flag,
                                                            unsigned long long *cnt) {
+  pdl_grid_wait();
   const int n = *count_in;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x) {
@@ -1417,6 +1452,7 @@ __global__ void __launch_bounds__(kThreads) k_fixrec_write(Dims d, const int *co
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kThreads) k_bcs(Dims d, int enable_B, PT *P,
                                                   double *flag) {
+  pdl_grid_wait();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int bb, idx[3];
   if (!box_index(t, d.NB, 0, d.N3 - 1, 0, d.N2 - 1, 0, d.N1 - 1, bb, idx[2], idx[1], idx[0]))
@@ -1467,6 +1503,7 @@ __global__ void __launch_bounds__(kThreads) k_bcs(Dims d, int enable_B, PT *P,
 // EstimateTimestepMesh (timestep_estimation.cc:13-102).
 // ---------------------------------------------------------------------------
 __global__ void k_dt_init(int n, unsigned long long *mins) {
+  pdl_grid_wait();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) mins[t] = (unsigned long long)__double_as_longlong(DBL_MAX);
 }
@@ -1522,6 +1559,7 @@ __device__ __forceinline__ void dt_reduce_cta(const Dims &d, double cfl, const d
 __global__ void __launch_bounds__(kThreads) k_dt_reduce(Dims d, double cfl,
                                                         const double *alfven,
                                                         unsigned long long *mins) {
+  pdl_grid_wait();
   dt_reduce_cta(d, cfl, alfven, mins);
 }
 
@@ -1549,6 +1587,7 @@ __device__ __forceinline__ void dt_finalize_jobs(const Dims &d, int njobs, const
 
 __global__ void k_dt_finalize(Dims d, int njobs, const int *jr, const unsigned long long *mins,
                               double *dt_out) {
+  pdl_grid_wait();
   if (blockIdx.x != 0) return;
   dt_finalize_jobs(d, njobs, jr, mins, dt_out, threadIdx.x, blockDim.x);
 }
@@ -1563,6 +1602,7 @@ __global__ void __launch_bounds__(kThreads) k_dt_reduce_final(Dims d, double cfl
                                                               unsigned int *ticket, int njobs,
                                                               const int *jr, double *dt_out,
                                                               int nmins) {
+  pdl_grid_wait();
   __shared__ bool last;
   dt_reduce_cta(d, cfl, alfven, mins);
   __threadfence();
@@ -1597,6 +1637,7 @@ __global__ void __launch_bounds__(kThreads) k_dt_reduce_final(Dims d, double cfl
 
 __global__ void k_update_dt(int njobs, const int *jr, double *dt, const double *dt_est,
                             double factor) {
+  pdl_grid_wait();
   if (blockIdx.x != 0) return;
   for (int q = threadIdx.x; q < njobs; q += blockDim.x) {
     const int job = jr ? jr[3 * q] : 0;
@@ -1639,6 +1680,7 @@ __device__ __forceinline__ void atomic_max_pos(unsigned long long *m, double v) 
 template <int MT>
 __global__ void __launch_bounds__(kThreads) k_gen_cells(Dims d, pangu_params p, GenArgs ga, PT *P,
                                                         unsigned long long *red) {
+  pdl_grid_wait();
   int bb, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, 0, d.N3 - 1, 0, d.N2 - 1, 0, d.N1 - 1, bb, k, j, i)) return;
@@ -1724,6 +1766,7 @@ __global__ void __launch_bounds__(kThreads) k_gen_cells(Dims d, pangu_params p, 
 // Torus: density and energy divided by the maximum density (all cells).
 __global__ void __launch_bounds__(kThreads) k_gen_normalize(Dims d, PT *P,
                                                             const unsigned long long *red) {
+  pdl_grid_wait();
   int bb, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, 0, d.N3 - 1, 0, d.N2 - 1, 0, d.N1 - 1, bb, k, j, i)) return;
@@ -1739,6 +1782,7 @@ __global__ void __launch_bounds__(kThreads) k_gen_normalize(Dims d, PT *P,
 template <int MT>
 __global__ void __launch_bounds__(kThreads) k_gen_bfield(Dims d, pangu_params p, GenArgs ga, PT *P,
                                                          unsigned long long *red) {
+  pdl_grid_wait();
   int bb, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, bb, k, j, i)) return;
@@ -1768,6 +1812,7 @@ __global__ void __launch_bounds__(kThreads) k_gen_bfield(Dims d, pangu_params p,
 // Torus field normalised to the target plasma beta (interior cells).
 __global__ void __launch_bounds__(kThreads) k_gen_scale(Dims d, double gam, double beta,
                                                         PT *P, const unsigned long long *red) {
+  pdl_grid_wait();
   int bb, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, bb, k, j, i)) return;
@@ -1799,23 +1844,42 @@ inline long long box_count(int NB, int k0, int k1, int j0, int j1, int i0, int i
   return (long long)NB * (k1 - k0 + 1) * (j1 - j0 + 1) * (i1 - i0 + 1);
 }
 
+// Launch with programmatic stream serialisation: the kernel may be scheduled
+// while the previous kernel of the stream drains; it waits for it in
+// pdl_grid_wait() before touching memory.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t s,
+                              Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 #define DISPATCH_MT(mt, KERNEL, grid, stream, ...)                          \
   do {                                                                      \
     switch (mt) {                                                           \
-      case PANGU_METRIC_MKS: KERNEL<MKS><<<grid, kThreads, 0, stream>>>(__VA_ARGS__); break; \
-      case PANGU_METRIC_BL: KERNEL<BL><<<grid, kThreads, 0, stream>>>(__VA_ARGS__); break;   \
-      case PANGU_METRIC_CKS: KERNEL<CKS><<<grid, kThreads, 0, stream>>>(__VA_ARGS__); break; \
-      default: KERNEL<MINKOWSKI><<<grid, kThreads, 0, stream>>>(__VA_ARGS__); break;         \
+      case PANGU_METRIC_MKS: launch_pdl(KERNEL<MKS>, dim3(grid), dim3(kThreads), stream, __VA_ARGS__); break; \
+      case PANGU_METRIC_BL: launch_pdl(KERNEL<BL>, dim3(grid), dim3(kThreads), stream, __VA_ARGS__); break; \
+      case PANGU_METRIC_CKS: launch_pdl(KERNEL<CKS>, dim3(grid), dim3(kThreads), stream, __VA_ARGS__); break; \
+      default: launch_pdl(KERNEL<MINKOWSKI>, dim3(grid), dim3(kThreads), stream, __VA_ARGS__); break; \
     }                                                                       \
   } while (0)
 
 #define DISPATCH_MT_T(mt, KERNEL, grid, threads, stream, ...)                                 \
   do {                                                                                       \
     switch (mt) {                                                                            \
-      case PANGU_METRIC_MKS: KERNEL<MKS><<<grid, threads, 0, stream>>>(__VA_ARGS__); break;   \
-      case PANGU_METRIC_BL: KERNEL<BL><<<grid, threads, 0, stream>>>(__VA_ARGS__); break;     \
-      case PANGU_METRIC_CKS: KERNEL<CKS><<<grid, threads, 0, stream>>>(__VA_ARGS__); break;   \
-      default: KERNEL<MINKOWSKI><<<grid, threads, 0, stream>>>(__VA_ARGS__); break;           \
+      case PANGU_METRIC_MKS: launch_pdl(KERNEL<MKS>, dim3(grid), dim3(threads), stream, __VA_ARGS__); break; \
+      case PANGU_METRIC_BL: launch_pdl(KERNEL<BL>, dim3(grid), dim3(threads), stream, __VA_ARGS__); break; \
+      case PANGU_METRIC_CKS: launch_pdl(KERNEL<CKS>, dim3(grid), dim3(threads), stream, __VA_ARGS__); break; \
+      default: launch_pdl(KERNEL<MINKOWSKI>, dim3(grid), dim3(threads), stream, __VA_ARGS__); break; \
     }                                                                                        \
   } while (0)
 
@@ -1882,8 +1946,8 @@ void launch_flux_dir(const pangu_engine *e, const pangu_pack *md, int dir, int m
   if (dir == 1) {
     const int nseg = (i1 - i0 + 1 + kFacesPerWarp - 1) / kFacesPerWarp;
     const long long warps = (long long)d.NB * (k1 - k0 + 1) * (j1 - j0 + 1) * nseg;
-    k_flux_x1<MT><<<grid_flux(32 * warps, threads), threads, 0, s>>>(d, e->p, k0, k1, j0, j1, i0,
-                                                                     i1, P, F, md->alfven);
+    launch_pdl(k_flux_x1<MT>, dim3(grid_flux(32 * warps, threads)), dim3(threads), s, d, e->p, k0,
+               k1, j0, j1, i0, i1, P, F, md->alfven);
     return;
   }
   const int m = dir == 2 ? (j1 - j0 + 1) : (k1 - k0 + 1);
@@ -1892,9 +1956,11 @@ void launch_flux_dir(const pangu_engine *e, const pangu_pack *md, int dir, int m
   const unsigned g = grid_flux(n, threads);
 #define PGK_MARCH(M)                                                                         \
   if (dir == 2)                                                                              \
-    k_flux_march2<MT, M><<<g, threads, 0, s>>>(d, e->p, k0, k1, j0, j1, i0, i1, P, F, md->alfven); \
+    launch_pdl(k_flux_march2<MT, M>, dim3(g), dim3(threads), s, d, e->p, k0, k1, j0, j1, i0, i1, \
+               P, F, md->alfven);                                                            \
   else                                                                                       \
-    k_flux_march3<MT, M><<<g, threads, 0, s>>>(d, e->p, k0, k1, j0, j1, i0, i1, P, F, md->alfven);
+    launch_pdl(k_flux_march3<MT, M>, dim3(g), dim3(threads), s, d, e->p, k0, k1, j0, j1, i0, i1, \
+               P, F, md->alfven);
   switch (march) {
     case 1: PGK_MARCH(1) break;
     case 2: PGK_MARCH(2) break;
@@ -1972,11 +2038,13 @@ int run_autotune(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
 int run_ct(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
   const Dims &d = e->d;
   const int o1 = d.N1 > 1, o2 = d.N2 > 1, o3 = d.N3 > 1;
-  k_ct_emf<<<grid_for(box_count(d.NB, d.ks, d.ke + o3, d.js, d.je + o2, d.is, d.ie + o1)),
-             kThreads, 0, s>>>(d, md->flux1, md->flux2, md->flux3, md->efield);
+  launch_pdl(k_ct_emf, dim3(grid_for(box_count(d.NB, d.ks, d.ke + o3, d.js, d.je + o2, d.is,
+                                                d.ie + o1))),
+             dim3(kThreads), s, d, md->flux1, md->flux2, md->flux3, md->efield);
   ++e->launches;
-  k_ct_faces<<<grid_for(box_count(d.NB, d.ks, d.ke + o3, d.js, d.je + o2, d.is, d.ie + o1)),
-               kThreads, 0, s>>>(d, md->flux1, md->flux2, md->flux3, md->efield);
+  launch_pdl(k_ct_faces, dim3(grid_for(box_count(d.NB, d.ks, d.ke + o3, d.js, d.je + o2, d.is,
+                                                  d.ie + o1))),
+             dim3(kThreads), s, d, md->flux1, md->flux2, md->flux3, md->efield);
   ++e->launches;
   return check_launch();
 }
@@ -1985,8 +2053,8 @@ int run_update(pangu_engine *e, const pangu_pack *mi, const pangu_pack *m0, cons
                double beta, const double *dt, cudaStream_t s) {
   const Dims &d = e->d;
   const long long n = box_count(d.NB * d.NF, d.ks, d.ke, d.js, d.je, d.is, d.ie);
-  k_flux_div_update<<<grid_for(n), kThreads, 0, s>>>(d, m0->flux1, m0->flux2, m0->flux3,
-                                                     mi->cons, m1->cons, beta, dt);
+  launch_pdl(k_flux_div_update, dim3(grid_for(n)), dim3(kThreads), s, d, m0->flux1, m0->flux2,
+             m0->flux3, mi->cons, m1->cons, beta, dt);
   ++e->launches;
   return check_launch();
 }
@@ -1994,8 +2062,8 @@ int run_update(pangu_engine *e, const pangu_pack *mi, const pangu_pack *m0, cons
 int run_exchange_range(pangu_engine *e, const pangu_pack *md, long long off, long long n,
                        cudaStream_t s) {
   if (n == 0) return PANGU_OK;
-  k_exchange<<<grid_for(n), kThreads, 0, s>>>(e->d, n, e->d_xdst + off, e->d_xsrc + off, prim_of(md),
-                                              md->flag);
+  launch_pdl(k_exchange, dim3(grid_for(n)), dim3(kThreads), s, e->d, n, e->d_xdst + off,
+             e->d_xsrc + off, prim_of(md), md->flag);
   ++e->launches;
   return check_launch();
 }
@@ -2007,7 +2075,8 @@ int run_exchange(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
 int run_halo_pack(pangu_engine *e, const pangu_pack *md, double *buf, cudaStream_t s) {
   const long long n = e->hsend_off.empty() ? 0 : e->hsend_off.back();
   if (n == 0) return PANGU_OK;
-  k_halo_pack<<<grid_for(n), kThreads, 0, s>>>(e->d, n, e->d_hsend, prim_of(md), md->flag, buf);
+  launch_pdl(k_halo_pack, dim3(grid_for(n)), dim3(kThreads), s, e->d, n, e->d_hsend, prim_of(md),
+             md->flag, buf);
   ++e->launches;
   return check_launch();
 }
@@ -2015,7 +2084,8 @@ int run_halo_pack(pangu_engine *e, const pangu_pack *md, double *buf, cudaStream
 int run_halo_unpack(pangu_engine *e, const pangu_pack *md, const double *buf, cudaStream_t s) {
   const long long n = e->hrecv_off.empty() ? 0 : e->hrecv_off.back();
   if (n == 0) return PANGU_OK;
-  k_halo_unpack<<<grid_for(n), kThreads, 0, s>>>(e->d, n, e->d_hrecv, prim_of(md), md->flag, buf);
+  launch_pdl(k_halo_unpack, dim3(grid_for(n)), dim3(kThreads), s, e->d, n, e->d_hrecv, prim_of(md),
+             md->flag, buf);
   ++e->launches;
   return check_launch();
 }
@@ -2039,7 +2109,9 @@ int run_recovery(pangu_engine *e, const pangu_pack *md, bool list_fix, cudaStrea
   const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
   if (!list_fix && cudaMemsetAsync(e->d_fail_count, 0, sizeof(int), s) != cudaSuccess)
     return PANGU_ECUDA;
-  DISPATCH_MT(e->p.metric_type, k_recovery, grid_for(n), s, d, e->p, prim_of(md), md->cons, md->flag,
+  DISPATCH_MT_T(e->p.metric_type, k_recovery,
+                (unsigned)((n + kRecoveryThreads - 1) / kRecoveryThreads), kRecoveryThreads, s, d,
+                e->p, prim_of(md), md->cons, md->flag,
               e->d_cnt, e->d_fail_count, e->d_fail_list);
   ++e->launches;
   if (e->p.recovery == PANGU_RECOVERY_CHAINER) {
@@ -2079,9 +2151,10 @@ int run_fix_recovery(pangu_engine *e, const pangu_pack *md, bool listed, cudaStr
     ++e->launches;
   }
   const unsigned g = 2 * 148;
-  k_fixrec_compute<<<g, kThreads, 0, s>>>(d, count, list, prim_of(md), md->flag, e->d_fail_vals);
-  k_fixrec_write<<<g, kThreads, 0, s>>>(d, count, list, e->d_fail_vals, prim_of(md), md->flag,
-                                        e->d_cnt);
+  launch_pdl(k_fixrec_compute, dim3(g), dim3(kThreads), s, d, count, list, prim_of(md), md->flag,
+             e->d_fail_vals);
+  launch_pdl(k_fixrec_write, dim3(g), dim3(kThreads), s, d, count, list, e->d_fail_vals,
+             prim_of(md), md->flag, e->d_cnt);
   e->launches += 2;
   return check_launch();
 }
@@ -2093,8 +2166,8 @@ int run_fix_recovery(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
 // Physical BCs of the blocks of d (all active blocks, or one job's).
 int run_bcs(pangu_engine *e, const Dims &d, bool any_bc, const pangu_pack *md, cudaStream_t s) {
   if (!any_bc || d.NB == 0) return PANGU_OK;
-  k_bcs<<<grid_for((long long)d.NB * d.ncell), kThreads, 0, s>>>(d, e->p.enable_B, prim_of(md),
-                                                                md->flag);
+  launch_pdl(k_bcs, dim3(grid_for((long long)d.NB * d.ncell)), dim3(kThreads), s, d, e->p.enable_B,
+             prim_of(md), md->flag);
   ++e->launches;
   return check_launch();
 }
@@ -2108,9 +2181,9 @@ int run_estimate_dt(pangu_engine *e, const pangu_pack *md, double *dt_out, cudaS
   const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
   const unsigned gx = (unsigned)std::min<long long>((n / std::max(1, d.NB) + kThreads - 1) / kThreads, 592);
   // d_dtmin holds DBL_MAX and d_dt_ticket 0 between calls (set at pool_init)
-  k_dt_reduce_final<<<dim3(std::max(1u, gx), d.NB), kThreads, 0, s>>>(
-      d, e->p.cfl_number, md->alfven, e->d_dtmin, e->d_dt_ticket, e->njobs_active, e->d_jr, dt_out,
-      3 * e->capacity);
+  launch_pdl(k_dt_reduce_final, dim3(std::max(1u, gx), d.NB), dim3(kThreads), s, d,
+             e->p.cfl_number, md->alfven, e->d_dtmin, e->d_dt_ticket, e->njobs_active, e->d_jr,
+             dt_out, 3 * e->capacity);
   e->launches += 1;
   return check_launch();
 }
