@@ -695,7 +695,10 @@ __device__ __forceinline__ void face_flux(const Dims &d, const pangu_params &p, 
 // reconstructs cell c = f0 - 1 + l; face c takes its left state from lane
 // l - 1 (upper-face value of cell c - 1) and its right state from lane l.
 constexpr int kFacesPerWarp = 31;
-constexpr int kFluxThreads = 128;  // flux kernels use ~160 registers: 3 CTAs of 4 warps per SM
+// Flux kernels: at most 128 registers (4 CTAs of 4 warps per SM, a few
+// spills). Bounds of 3 CTAs (168 registers) and of 5 or 6 (96 or 80) were
+// measured slower on the 2D torus (the latter two faster on the 3D one).
+constexpr int kFluxThreads = 128;
 
 template <int MT>
 __global__ void __launch_bounds__(kFluxThreads, 4) k_flux_x1(Dims d, pangu_params p, int k0, int k1,
