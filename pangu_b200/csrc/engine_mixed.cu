@@ -3,9 +3,11 @@
 // Riemann fluxes, electron heating and the geometric source term in FP32;
 // conserved variables and the flux divergence update, C2P, the metric and CT
 // in FP64.
-// Built with FMA contraction on and the CUDA math library's pow/exp/log
-// (the exact build, engine.cu, keeps --fmad=false and correctly rounded
-// functions for bit-exact parity). The device helpers are compiled under
+// Built with --use_fast_math (FMA contraction, approximate FP32 division,
+// square root and math functions, FP32 denormals flushed; FP64 arithmetic is
+// unaffected) and the CUDA math library's pow/exp/log (the exact build,
+// engine.cu, keeps --fmad=false and correctly rounded functions for
+// bit-exact parity). The device helpers are compiled under
 // their own namespace name so the two builds never share a definition.
 #define pgd pgd_mixed
 #define PGD_POW ::pow
