@@ -2201,11 +2201,10 @@ int dalloc(T **p, size_t n) {
 // three parts so that a sharded mesh can move its halo messages while the
 // middle part runs: the ghost cells the messages fill are read first by
 // FixRecovery (neighbour means) and by the next stage.
-// Part 1: FixPrimitive + CalculateConservative, fluxes, CT, update, ghost
-// exchange at send time; the halo cells of mc1 go to `send` (sharded only).
-// Part 1 without the exchange: FixPrimitive + CalculateConservative, fluxes,
-// CT and the update; reads only mc0 and mc_init, writes mc1's conserved
-// variables.
+// Part 1 (run_stage_begin) is run_stage_update followed by the ghost exchange
+// at send time, whose halo cells of mc1 go to `send` (sharded only).
+// run_stage_update: FixPrimitive + CalculateConservative, fluxes, CT and the
+// update; reads only mc0 and mc_init, writes mc1's conserved variables.
 int run_stage_update(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
                      double beta, const double *dt, cudaStream_t s) {
   const pangu_pack *mc0 = stage == 1 ? base : one;
