@@ -312,7 +312,8 @@ long long pangu_launches(const pangu_engine *e);
 
 /* Autotuner of the flux kernels' tile shapes (no counterpart in the
  * reference): times each candidate shape of every direction -- CTA size 64
- * or 128, and for x2/x3 a march depth of 1, 2 or 4 faces per thread -- on
+ * or 128, and for x2/x3 a march depth of 1, 2 or 4 faces per thread or a
+ * shared-memory tile of 32 x 4 or 32 x 8 faces -- on
  * the pack's own data and keeps the fastest for this engine. Every candidate
  * computes each face identically, so results never depend on the choice.
  * Overwrites the pack's fluxes and alfven (which every stage recomputes
@@ -323,8 +324,10 @@ int pangu_autotune(pangu_engine *e, const pangu_pack *md, void *stream);
  * threads3, tuned}. */
 int pangu_flux_config(const pangu_engine *e, int32_t out[7]);
 /* Sets the tile shapes {march1 (1), threads1, march2, threads2, march3,
- * threads3}: march 1, 2 or 4, threads 64 or 128 (PANGU_EINVAL otherwise),
- * e.g. to repeat a configuration the autotuner chose elsewhere. */
+ * threads3}: march 1, 2 or 4 with threads 64 or 128, or for x2 and x3 march
+ * 0 (tiles of 32 x threads/32 faces, each cell reconstructed once) with
+ * threads 128 or 256 (PANGU_EINVAL otherwise), e.g. to repeat a configuration
+ * the autotuner chose elsewhere. */
 int pangu_set_flux_config(pangu_engine *e, const int32_t cfg[6]);
 
 /* ---- block pool: many jobs stepped by the same launches ---------------- */

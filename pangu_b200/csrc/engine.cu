@@ -572,8 +572,9 @@ int pangu_set_flux_config(pangu_engine *e, const int32_t cfg[6]) {
   if (!e || !cfg) return PANGU_EINVAL;
   for (int d = 0; d < 3; ++d) {
     const int m = cfg[2 * d], t = cfg[2 * d + 1];
-    if ((d == 0 ? m != 1 : (m != 1 && m != 2 && m != 4)) || (t != 64 && t != 128))
-      return PANGU_EINVAL;
+    const bool march_ok = d == 0 ? m == 1 : (m == 0 || m == 1 || m == 2 || m == 4);
+    const bool threads_ok = m == 0 ? (t == 128 || t == 256) : (t == 64 || t == 128);
+    if (!march_ok || !threads_ok) return PANGU_EINVAL;
   }
   for (int d = 0; d < 3; ++d) {
     e->tune.march[d] = cfg[2 * d];

@@ -788,6 +788,69 @@ __device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_param
   }
 }
 
+// x2 / x3 faces by tiles: a CTA of 32 x TF threads reconstructs each cell of
+// a tile of 32 consecutive i by TF + 1 cells along the face direction once,
+// into shared memory, then computes the TF x 32 faces from the stored upper
+// and lower values (a march reconstructs (MARCH + 1) / MARCH cells per face,
+// a tile (TF + 1) / TF). The face arithmetic is face_flux's, so the results
+// are those of the march kernels.
+template <int MT, int DIR, int TF>
+__device__ __forceinline__ void flux_tile_body(const Dims &d, const pangu_params &p, int k0, int k1,
+                                               int j0, int j1, int i0, int i1, const PT *P,
+                                               double *F, double *alfven) {
+  __shared__ FT sup[TF + 1][NPRIM][32], slo[TF + 1][NPRIM][32];
+  const int m0 = DIR == 2 ? j0 : k0, m1 = DIR == 2 ? j1 : k1;
+  const int a0 = DIR == 2 ? k0 : j0, a1 = DIR == 2 ? k1 : j1;
+  const int ni = i1 - i0 + 1, na = a1 - a0 + 1, nm = m1 - m0 + 1;
+  const int nti = (ni + 31) / 32, ntm = (nm + TF - 1) / TF;
+  long long ti, tm, al;
+  long long r = div_fast(blockIdx.x, nti, ti);
+  r = div_fast(r, ntm, tm);
+  const long long bb = div_fast(r, na, al);
+  if (bb >= d.NB) return;  // whole CTAs exit together
+  const int b = slot_of(d, (int)bb);
+  const int a = a0 + (int)al;
+  const int mt0 = m0 + (int)tm * TF;
+  const int lane = threadIdx.x & 31, row = threadIdx.x >> 5;
+  const int i = i0 + (int)ti * 32 + lane;
+  const long long stride = DIR == 2 ? (long long)d.N1 : (long long)d.N1 * d.N2;
+  const bool use_mc = p.limiter == PANGU_LIMITER_MC;
+  // cells mt0 - 1 .. mt0 + TF - 1: the lower neighbour of every face of the tile
+  for (int cr = row; cr <= TF; cr += TF) {
+    const int c = mt0 - 1 + cr;
+    if (i <= i1 && c <= m1) {
+      const int kk = DIR == 2 ? a : c, jj = DIR == 2 ? c : a;
+#pragma unroll
+      for (int s = 0; s < NPRIM; ++s) {
+        FT up = 0, lo = 0;
+        if (d.pidx[s] >= 0) recon_cell(use_mc, P + vidx(d, b, d.pidx[s], kk, jj, i), stride, up, lo);
+        sup[cr][s][lane] = up;
+        slo[cr][s][lane] = lo;
+      }
+    }
+  }
+  __syncthreads();
+  const int f = mt0 + row;
+  if (i > i1 || f > m1) return;
+  FT PL[NPRIM], PR[NPRIM];
+#pragma unroll
+  for (int s = 0; s < NPRIM; ++s) {
+    PL[s] = sup[row][s][lane];
+    PR[s] = slo[row + 1][s][lane];
+  }
+  const int kk = DIR == 2 ? a : f, jj = DIR == 2 ? f : a;
+  face_flux<MT, DIR>(d, p, b, kk, jj, i, PL, PR, F, alfven);
+}
+
+template <int MT, int DIR, int TF>
+__global__ void __launch_bounds__(32 * TF, TF == 4 ? 4 : 2) k_flux_tile(Dims d, pangu_params p, int k0,
+                                                                     int k1, int j0, int j1, int i0,
+                                                                     int i1, const PT *P, double *F,
+                                                                     double *alfven) {
+  pdl_grid_wait();
+  flux_tile_body<MT, DIR, TF>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
+}
+
 template <int MT, int MARCH>
 __global__ void __launch_bounds__(kFluxThreads, 4) k_flux_march2(Dims d, pangu_params p, int k0, int k1,
                                                           int j0, int j1, int i0, int i1,
@@ -1955,6 +2018,20 @@ void launch_flux_dir(const pangu_engine *e, const pangu_pack *md, int dir, int m
   }
   const int m = dir == 2 ? (j1 - j0 + 1) : (k1 - k0 + 1);
   const int na = dir == 2 ? (k1 - k0 + 1) : (j1 - j0 + 1);
+  if (march == 0) {  // tiles of 32 x (threads / 32) faces
+    const long long nt = (long long)d.NB * na * ((m + threads / 32 - 1) / (threads / 32)) *
+                         ((i1 - i0 + 1 + 31) / 32);
+#define PGK_TILE(D, TF)                                                                     \
+  launch_pdl(k_flux_tile<MT, D, TF>, dim3((unsigned)nt), dim3(32 * TF), s, d, e->p, k0, k1, j0, \
+             j1, i0, i1, P, F, md->alfven)
+    if (dir == 2) {
+      if (threads == 128) PGK_TILE(2, 4); else PGK_TILE(2, 8);
+    } else {
+      if (threads == 128) PGK_TILE(3, 4); else PGK_TILE(3, 8);
+    }
+#undef PGK_TILE
+    return;
+  }
   const long long n = (long long)d.NB * na * ((m + march - 1) / march) * (i1 - i0 + 1);
   const unsigned g = grid_flux(n, threads);
 #define PGK_MARCH(M)                                                                         \
@@ -2005,16 +2082,21 @@ int run_autotune(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
     return PANGU_ECUDA;
   }
   int rc = PANGU_OK;
-  const int thread_opts[2] = {64, 128};
-  const int march_opts[3] = {1, 2, 4};
+  // candidates {march, CTA size}; march 0 is the tiled kernel (tiles of 32 x
+  // CTA size / 32 faces)
+  const int cand[8][2] = {{1, 64}, {1, 128}, {2, 64}, {2, 128}, {4, 64}, {4, 128}, {0, 128},
+                          {0, 256}};
+  // Each candidate's time is the minimum over two interleaved rounds of five
+  // launches after one warm-up launch, so that clock ramps and cache states
+  // do not favour whichever candidate runs first.
   for (int dir = 1; dir <= e->d.ndim && !rc; ++dir) {
-    float best = 1e30f;
-    const int nm = dir == 1 ? 1 : 3;
-    for (int mi = 0; mi < nm && !rc; ++mi)
-      for (int ti = 0; ti < 2 && !rc; ++ti) {
-        const int march = dir == 1 ? 1 : march_opts[mi], threads = thread_opts[ti];
-        float t = 1e30f;
-        for (int rep = 0; rep < 4 && !rc; ++rep) {
+    const int nc = dir == 1 ? 2 : 8;
+    float t[8];
+    for (int ci = 0; ci < nc; ++ci) t[ci] = 1e30f;
+    for (int round = 0; round < 2 && !rc; ++round)
+      for (int ci = 0; ci < nc && !rc; ++ci) {
+        const int march = cand[ci][0], threads = cand[ci][1];
+        for (int rep = 0; rep < 6 && !rc; ++rep) {
           if (cudaEventRecord(ev[0], s) != cudaSuccess) rc = PANGU_ECUDA;
           if (!rc) rc = run_flux_dir(e, md, dir, march, threads, s);
           if (!rc && (cudaEventRecord(ev[1], s) != cudaSuccess ||
@@ -2022,13 +2104,15 @@ int run_autotune(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
             rc = PANGU_ECUDA;
           float ms = 0;
           if (!rc && cudaEventElapsedTime(&ms, ev[0], ev[1]) != cudaSuccess) rc = PANGU_ECUDA;
-          if (!rc && rep > 0) t = std::min(t, ms);
+          if (!rc && rep > 0) t[ci] = std::min(t[ci], ms);
         }
-        if (!rc && t < best) {
-          best = t;
-          e->tune.march[dir - 1] = march;
-          e->tune.threads[dir - 1] = threads;
-        }
+      }
+    float best = 1e30f;
+    for (int ci = 0; ci < nc && !rc; ++ci)
+      if (t[ci] < best) {
+        best = t[ci];
+        e->tune.march[dir - 1] = cand[ci][0];
+        e->tune.threads[dir - 1] = cand[ci][1];
       }
   }
   if (!rc) e->tune.tuned = 1;

@@ -1,5 +1,6 @@
-"""The flux kernels' tile shapes (CTA size, march depth) change how faces
-are distributed over threads, never what is computed for a face: every shape
+"""The flux kernels' tile shapes (CTA size, march depth, shared-memory
+tiles) change how faces are distributed over threads, never what is computed
+for a face: every shape
 the autotuner may pick gives bit-identical results, in FP64 and in the mixed
 form, so a job's result does not depend on the tuning of the engine (or pool,
 or server class) that runs it."""
@@ -33,10 +34,12 @@ def test_every_tile_shape_gives_the_same_result(precision, three_d):
     pin.set("b200", "precision", precision)
     prim0 = gen(problems.Geometry(prm.mesh_struct(pin)), prm.process_packages(pin), pin)
     ref = None
-    marches = (1, 2, 4)
-    for t1, m2, t2 in itertools.product((64, 128), marches, (64, 128)):
-        m3 = m2 if three_d else 2
-        cfg = dict(x1_threads=t1, x2_march=m2, x2_threads=t2, x3_march=m3, x3_threads=t2)
+    # (march, CTA size): march 1, 2, 4 faces per thread, or march 0: shared-memory
+    # tiles of 32 x (CTA size / 32) faces
+    shapes = [(1, 64), (1, 128), (2, 64), (2, 128), (4, 64), (4, 128), (0, 128), (0, 256)]
+    for t1, (m2, t2) in itertools.product((64, 128), shapes):
+        m3, t3 = (m2, t2) if three_d else (2, 128)
+        cfg = dict(x1_threads=t1, x2_march=m2, x2_threads=t2, x3_march=m3, x3_threads=t3)
         got = _run(pin, prim0, cfg)
         if ref is None:
             ref = got
