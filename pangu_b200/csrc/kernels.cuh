@@ -2088,7 +2088,9 @@ int run_autotune(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
                           {0, 256}};
   // Each candidate's time is the minimum over two interleaved rounds of five
   // launches after one warm-up launch, so that clock ramps and cache states
-  // do not favour whichever candidate runs first.
+  // do not favour whichever candidate runs first. A candidate of x2 (x3) is
+  // timed behind the chosen x1 (and x2) launches, as it runs in a stage, so
+  // that it meets the caches those leave.
   for (int dir = 1; dir <= e->d.ndim && !rc; ++dir) {
     const int nc = dir == 1 ? 2 : 8;
     float t[8];
@@ -2098,6 +2100,8 @@ int run_autotune(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
         const int march = cand[ci][0], threads = cand[ci][1];
         for (int rep = 0; rep < 6 && !rc; ++rep) {
           if (cudaEventRecord(ev[0], s) != cudaSuccess) rc = PANGU_ECUDA;
+          for (int lower = 1; lower < dir && !rc; ++lower)
+            rc = run_flux_dir(e, md, lower, e->tune.march[lower - 1], e->tune.threads[lower - 1], s);
           if (!rc) rc = run_flux_dir(e, md, dir, march, threads, s);
           if (!rc && (cudaEventRecord(ev[1], s) != cudaSuccess ||
                       cudaEventSynchronize(ev[1]) != cudaSuccess))
