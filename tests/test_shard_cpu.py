@@ -174,3 +174,26 @@ def test_halo_transfer_over_gloo(tmp_path, name, world):
                                       ref_flag.reshape(nb, -1)[b, c])
         assert float(open(tmp_path / f"dt{r}.txt").read()) == 1.0e-3 * (3 - (world - 1))
     assert total > 0
+
+
+def test_plan_rejects_bad_assignments():
+    """pangu_shard_plan validates its arguments before any work (no GPU)."""
+    import ctypes as C
+    from pangu_b200 import abi
+    from pangu_b200.engine import lib
+    case = Case("ot_blocks")
+    L = lib()
+    nb = case.oracle.nb
+    counts = (C.c_int64 * 4)()
+    def plan(br, nranks, rank):
+        a = np.ascontiguousarray(br, dtype=np.int32)
+        return L.pangu_shard_plan(C.byref(case.params), C.byref(case.mesh),
+                                  a.ctypes.data_as(C.POINTER(C.c_int32)), nranks, rank,
+                                  counts, counts, None, None)
+    ok = (np.arange(nb) % 2).astype(np.int32)
+    assert plan(ok, 2, 0) == abi.PANGU_OK
+    assert plan(ok, 2, 2) == abi.PANGU_EINVAL           # rank out of range
+    assert plan(ok + 5, 2, 0) == abi.PANGU_EINVAL       # block on a rank that does not exist
+    assert plan(ok, 0, 0) == abi.PANGU_EINVAL           # no ranks
+    assert L.pangu_shard_plan(C.byref(case.params), C.byref(case.mesh), None, 2, 0, counts,
+                              counts, None, None) == abi.PANGU_EINVAL
