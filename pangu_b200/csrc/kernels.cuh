@@ -1632,9 +1632,10 @@ __global__ void __launch_bounds__(kThreads) k_dt_reduce(Dims d, double cfl,
 // The minimum over the job's blocks of 1 / sum_d (1 / min_d), for jobs q =
 // first, first + stride, ... (active entries jr[3q+1] .. jr[3q+2]-1 of job
 // jr[3q]; the whole domain as job 0 when jr is null), written to dt_out[job].
+template <class Mins>
 __device__ __forceinline__ void dt_finalize_jobs(const Dims &d, int njobs, const int *jr,
-                                                 const unsigned long long *mins, double *dt_out,
-                                                 int first, int stride) {
+                                                 Mins mins, double *dt_out, int first,
+                                                 int stride) {
   for (int q = first; q < njobs; q += stride) {
     const int job = jr ? jr[3 * q] : 0;
     const int s0 = jr ? jr[3 * q + 1] : 0, s1 = jr ? jr[3 * q + 2] : d.NB;
@@ -1682,19 +1683,7 @@ __global__ void __launch_bounds__(kThreads) k_dt_reduce_final(Dims d, double cfl
   __threadfence();
   // every other CTA's atomics are complete; read the minima past L1
   const volatile unsigned long long *vm = mins;
-  for (int q = threadIdx.x; q < njobs; q += blockDim.x) {
-    const int job = jr[3 * q];
-    double gmin = DBL_MAX;
-    for (int bb = jr[3 * q + 1]; bb < jr[3 * q + 2]; ++bb) {
-      const int b = slot_of(d, bb);
-      const double m0 = __longlong_as_double((long long)vm[3 * b + 0]);
-      const double m1 = __longlong_as_double((long long)vm[3 * b + 1]);
-      const double m2 = __longlong_as_double((long long)vm[3 * b + 2]);
-      const double bdt = 1.0 / (1.0 / m0 + 1.0 / m1 + 1.0 / m2);
-      if (bdt < gmin) gmin = bdt;
-    }
-    dt_out[job] = gmin;
-  }
+  dt_finalize_jobs(d, njobs, jr, vm, dt_out, threadIdx.x, blockDim.x);
   __syncthreads();
   const unsigned long long big = (unsigned long long)__double_as_longlong(DBL_MAX);
   for (int t = threadIdx.x; t < nmins; t += blockDim.x) mins[t] = big;
