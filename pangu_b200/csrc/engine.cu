@@ -75,6 +75,7 @@ int pangu_engine_destroy(pangu_engine *e) {
   cudaFree(e->d_bcf);
   cudaFree(e->d_t1);
   cudaFree(e->d_ctab);
+  cudaFree(e->d_ctab32);
   cudaFree(e->d_f1tab);
   cudaFree(e->d_f2tab);
   cudaFree(e->d_t2);
@@ -195,6 +196,8 @@ int pool_init(pangu_engine *e, int capacity, int max_jobs) {
     rc |= dalloc(&e->d_ctab, (size_t)capacity * T.ncen * pc);
     rc |= dalloc(&e->d_f1tab, (size_t)capacity * T.nmet * p1);
     rc |= dalloc(&e->d_f2tab, (size_t)capacity * T.nmet * p2);
+    if (p.precision == PANGU_PRECISION_MIXED)
+      rc |= dalloc(&e->d_ctab32, (size_t)capacity * T.nconn * pc);
   }
   if (rc != PANGU_OK) return PANGU_ENOMEM;
   bool ok = cudaMemset(e->d_cnt, 0, (size_t)max_jobs * PANGU_NCOUNTERS * 8) == cudaSuccess;
@@ -212,6 +215,7 @@ int pool_init(pangu_engine *e, int capacity, int max_jobs) {
   d.t2 = e->d_t2;
   d.origin = e->d_origin;
   d.ctab = e->d_ctab;
+  d.ctab32 = e->d_ctab32;
   d.f1tab = e->d_f1tab;
   d.f2tab = e->d_f2tab;
   return PANGU_OK;
@@ -369,6 +373,14 @@ int pool_attach(pangu_engine *e, const pangu_mesh &m, double a, double h, int *j
         k_build_tables<MKS><<<grid_for(n), kThreads>>>(dj, J.p, e->d_ctab, e->d_f1tab, e->d_f2tab);
       else
         k_build_tables<BL><<<grid_for(n), kThreads>>>(dj, J.p, e->d_ctab, e->d_f1tab, e->d_f2tab);
+      if (e->d_ctab32) {
+        const TabLayout T = e->p.metric_type == PANGU_METRIC_MKS ? tab_layout(MKS) : tab_layout(BL);
+        const long long nc = (long long)dj.NB * T.nconn * d.N2 * d.N1;
+        if (e->p.metric_type == PANGU_METRIC_MKS)
+          k_conn_to_f32<MKS><<<grid_for(nc), kThreads>>>(dj, e->d_ctab32);
+        else
+          k_conn_to_f32<BL><<<grid_for(nc), kThreads>>>(dj, e->d_ctab32);
+      }
       ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(0) == cudaSuccess;
     }
     if (!ok) return PANGU_ECUDA;

@@ -59,6 +59,9 @@ struct Dims {
   // component planes of [NB][comp][N2][N1] (centres), [NB][comp][N2][N1+1]
   // (x1 faces) and [NB][comp][N2+1][N1] (x2 faces); x3 faces use the centres.
   const double *ctab, *f1tab, *f2tab;
+  // Mixed form only: the centre table's Christoffel planes rounded once to
+  // FP32, [slot][nconn][N2][N1], read by the FP32 source term; null otherwise.
+  const float *ctab32;
 };
 
 // A job: one mesh of equal meshblocks, placed in pool slots.
@@ -88,6 +91,7 @@ struct pangu_engine {
   signed char *d_bcf = nullptr; // [capacity][6]
   double *d_t1 = nullptr, *d_t2 = nullptr, *d_origin = nullptr;
   double *d_ctab = nullptr, *d_f1tab = nullptr, *d_f2tab = nullptr;
+  float *d_ctab32 = nullptr;  // mixed form: FP32 Christoffel planes
   long long *d_xdst = nullptr, *d_xsrc = nullptr;  // [capacity x ghost cells per block]
   long long nxch = 0, xch_cap = 0;
   int *d_tmp_slots = nullptr;  // [capacity] slots of a job being attached

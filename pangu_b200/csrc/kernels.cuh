@@ -1097,8 +1097,8 @@ __device__ __forceinline__ void source_cell(const Dims &d, const pangu_params &p
     const FT e_tot = hh + sf.bsq;
     const FT p_tot = (gam - FT(1)) * pf[ENY] + FT(0.5) * sf.bsq;
     const long long plane = (long long)d.N2 * d.N1;
-    const double *cn = d.ctab + (long long)b * L.ncen * plane + (long long)j * d.N1 + i +
-                       (long long)L.nmet * plane;
+    // the FP32 Christoffel planes (pool_init builds them for every mixed engine)
+    const float *cn = d.ctab32 + (long long)b * L.nconn * plane + (long long)j * d.N1 + i;
 #pragma unroll
     for (int dir = 0; dir < 4; ++dir) {
       FT con = FT(0);
@@ -1229,6 +1229,24 @@ __global__ void __launch_bounds__(kThreads) k_build_tables(Dims d, pangu_params 
         for (int kk = jj; kk < 4; ++kk)
           if (L.conn[a][jj][kk] >= 0) o[(L.nmet + L.conn[a][jj][kk]) * plane] = conn[a][jj][kk];
   }
+}
+
+// Mixed form: the centre table's Christoffel planes of the job's slots
+// rounded once to FP32 (what the FP32 source term converts each value to
+// anyway), so that the source term reads half the bytes.
+template <int MT>
+__global__ void __launch_bounds__(kThreads) k_conn_to_f32(Dims d, float *out) {
+  pdl_grid_wait();
+  constexpr TabLayout L = tab_layout(MT);
+  const long long plane = (long long)d.N2 * d.N1;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)d.NB * L.nconn * plane) return;
+  long long off, q;
+  const long long bq = div_fast(t, plane, off);
+  const int bb = (int)div_fast(bq, L.nconn, q);
+  const long long sl = slot_of(d, bb);
+  out[(sl * L.nconn + q) * plane + off] =
+      (float)d.ctab[(sl * L.ncen + L.nmet + q) * plane + off];
 }
 
 // ---------------------------------------------------------------------------
