@@ -76,6 +76,8 @@ int pangu_engine_destroy(pangu_engine *e) {
   cudaFree(e->d_t1);
   cudaFree(e->d_ctab);
   cudaFree(e->d_ctab32);
+  cudaFree(e->d_f1tab32);
+  cudaFree(e->d_f2tab32);
   cudaFree(e->d_f1tab);
   cudaFree(e->d_f2tab);
   cudaFree(e->d_t2);
@@ -196,8 +198,11 @@ int pool_init(pangu_engine *e, int capacity, int max_jobs) {
     rc |= dalloc(&e->d_ctab, (size_t)capacity * T.ncen * pc);
     rc |= dalloc(&e->d_f1tab, (size_t)capacity * T.nmet * p1);
     rc |= dalloc(&e->d_f2tab, (size_t)capacity * T.nmet * p2);
-    if (p.precision == PANGU_PRECISION_MIXED)
+    if (p.precision == PANGU_PRECISION_MIXED) {
       rc |= dalloc(&e->d_ctab32, (size_t)capacity * T.nconn * pc);
+      rc |= dalloc(&e->d_f1tab32, (size_t)capacity * T.nmet * p1);
+      rc |= dalloc(&e->d_f2tab32, (size_t)capacity * T.nmet * p2);
+    }
   }
   if (rc != PANGU_OK) return PANGU_ENOMEM;
   bool ok = cudaMemset(e->d_cnt, 0, (size_t)max_jobs * PANGU_NCOUNTERS * 8) == cudaSuccess;
@@ -216,6 +221,8 @@ int pool_init(pangu_engine *e, int capacity, int max_jobs) {
   d.origin = e->d_origin;
   d.ctab = e->d_ctab;
   d.ctab32 = e->d_ctab32;
+  d.f1tab32 = e->d_f1tab32;
+  d.f2tab32 = e->d_f2tab32;
   d.f1tab = e->d_f1tab;
   d.f2tab = e->d_f2tab;
   return PANGU_OK;
@@ -380,6 +387,11 @@ int pool_attach(pangu_engine *e, const pangu_mesh &m, double a, double h, int *j
           k_conn_to_f32<MKS><<<grid_for(nc), kThreads>>>(dj, e->d_ctab32);
         else
           k_conn_to_f32<BL><<<grid_for(nc), kThreads>>>(dj, e->d_ctab32);
+        const long long p1 = (long long)d.N2 * (d.N1 + 1), p2 = (long long)(d.N2 + 1) * d.N1;
+        k_planes_to_f32<<<grid_for((long long)dj.NB * T.nmet * p1), kThreads>>>(
+            dj, e->d_f1tab, e->d_f1tab32, T.nmet, p1);
+        k_planes_to_f32<<<grid_for((long long)dj.NB * T.nmet * p2), kThreads>>>(
+            dj, e->d_f2tab, e->d_f2tab32, T.nmet, p2);
       }
       ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(0) == cudaSuccess;
     }

@@ -62,6 +62,9 @@ struct Dims {
   // Mixed form only: the centre table's Christoffel planes rounded once to
   // FP32, [slot][nconn][N2][N1], read by the FP32 source term; null otherwise.
   const float *ctab32;
+  // Mixed form only: the x1- and x2-face tables rounded once to FP32 (the
+  // FP32 face fluxes read these); null otherwise.
+  const float *f1tab32, *f2tab32;
 };
 
 // A job: one mesh of equal meshblocks, placed in pool slots.
@@ -92,6 +95,7 @@ struct pangu_engine {
   double *d_t1 = nullptr, *d_t2 = nullptr, *d_origin = nullptr;
   double *d_ctab = nullptr, *d_f1tab = nullptr, *d_f2tab = nullptr;
   float *d_ctab32 = nullptr;  // mixed form: FP32 Christoffel planes
+  float *d_f1tab32 = nullptr, *d_f2tab32 = nullptr;  // mixed form: FP32 face tables
   long long *d_xdst = nullptr, *d_xsrc = nullptr;  // [capacity x ghost cells per block]
   long long nxch = 0, xch_cap = 0;
   int *d_tmp_slots = nullptr;  // [capacity] slots of a job being attached

@@ -215,6 +215,32 @@ __device__ __forceinline__ int load_geo(const double *__restrict__ tab, long lon
   return __ldg(tab + off + (s0 + 3) * plane) != 0.0;
 }
 
+#if PGK_MIXED
+// load_geo from an FP32 copy of a table: the values geo_cast would give.
+template <int MT>
+__device__ __forceinline__ int load_geo_f32(const float *__restrict__ tab, long long plane,
+                                            long long off, GeoT<float> &g) {
+  constexpr TabLayout L = tab_layout(MT);
+  float cov[L.nsym], con[L.ncon];
+#pragma unroll
+  for (int q = 0; q < L.nsym; ++q) cov[q] = __ldg(tab + off + q * plane);
+#pragma unroll
+  for (int q = 0; q < L.ncon; ++q) con[q] = __ldg(tab + off + (L.nsym + q) * plane);
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      g.gcov[r][c] = L.sym[r][c] >= 0 ? cov[L.sym[r][c]] : 0.0f;
+      g.gcon[r][c] = L.con[r][c] >= 0 ? con[L.con[r][c]] : 0.0f;
+    }
+  const long long s0 = L.nsym + L.ncon;
+  g.gdet = __ldg(tab + off + s0 * plane);
+  g.sg = __ldg(tab + off + (s0 + 1) * plane);
+  g.alpha = __ldg(tab + off + (s0 + 2) * plane);
+  return __ldg(tab + off + (s0 + 3) * plane) != 0.0f;
+}
+#endif
+
 __device__ __forceinline__ void minkowski_geo(Geo &g) {
   minkowski_gcov(g.gcov);
   minkowski_gcov(g.gcon);
@@ -589,17 +615,33 @@ template <int MT, int DIR>
 __device__ __forceinline__ void face_flux(const Dims &d, const pangu_params &p, int b, int k, int j,
                                           int i, const FT PL[NPRIM], const FT PR[NPRIM],
                                           double *F, double *alfven) {
-  Geo g64;
   const long long fo = vidx(d, b, 0, k, j, i);
-  if (!face_metric<MT>(d, p, DIR, b, k, j, i, g64)) {
+  GeoT<FT> g;
+  int ok;
+  if ((MT == MKS || MT == BL) && DIR != 3) {
+    // the FP32 face tables (pool_init builds them for every mixed engine)
+    constexpr TabLayout L = tab_layout(MT);
+    if (DIR == 1) {
+      const long long plane = (long long)d.N2 * (d.N1 + 1);
+      ok = load_geo_f32<MT>(d.f1tab32, plane,
+                            (long long)b * L.nmet * plane + (long long)j * (d.N1 + 1) + i, g);
+    } else {
+      const long long plane = (long long)(d.N2 + 1) * d.N1;
+      ok = load_geo_f32<MT>(d.f2tab32, plane, (long long)b * L.nmet * plane + (long long)j * d.N1 + i,
+                            g);
+    }
+  } else {
+    Geo g64;
+    ok = face_metric<MT>(d, p, DIR, b, k, j, i, g64);
+    if (ok) geo_cast<MT>(g64, g);
+  }
+  if (!ok) {
     alfven[aidx(d, b, DIR - 1, k, j, i)] = 0.0;
 #pragma unroll
     for (int s = 0; s < NPRIM; ++s)
       if (d.pidx[s] >= 0) F[fo + d.pidx[s] * d.ncell] = 0.0;
     return;
   }
-  GeoT<FT> g;
-  geo_cast<MT>(g64, g);
   const FT gam = (FT)p.adiabatic_index;
   const FT sg = g.sg;
   StateT<FT> sL, sR;
@@ -1229,6 +1271,20 @@ __global__ void __launch_bounds__(kThreads) k_build_tables(Dims d, pangu_params 
         for (int kk = jj; kk < 4; ++kk)
           if (L.conn[a][jj][kk] >= 0) o[(L.nmet + L.conn[a][jj][kk]) * plane] = conn[a][jj][kk];
   }
+}
+
+// Mixed form: ncomp planes of a slot-major table, for the job's slots,
+// rounded once to FP32.
+__global__ void __launch_bounds__(kThreads) k_planes_to_f32(Dims d, const double *src, float *dst,
+                                                            int ncomp, long long plane) {
+  pdl_grid_wait();
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)d.NB * ncomp * plane) return;
+  long long off, q;
+  const long long bq = div_fast(t, plane, off);
+  const int bb = (int)div_fast(bq, ncomp, q);
+  const long long at = ((long long)slot_of(d, bb) * ncomp + q) * plane + off;
+  dst[at] = (float)src[at];
 }
 
 // Mixed form: the centre table's Christoffel planes of the job's slots
