@@ -31,6 +31,11 @@ using FT = double;
 #define PGK_POW pgm::pow
 #endif
 
+// The FP64 flux kernels of curved metrics evaluate the two sides of a face
+// one after the other through shared memory (face_flux_split); the others
+// hold both states in registers (face_flux).
+#define PGK_SPLIT_FACES (!PGK_MIXED)
+
 template <class Pack>
 __host__ __forceinline__ PT *prim_of(const Pack *md) {
   return reinterpret_cast<PT *>(md->prim);
@@ -731,6 +736,89 @@ __device__ __forceinline__ void face_flux(const Dims &d, const pangu_params &p, 
   PGD_FACE_COMPONENT(KEL)
 #undef PGD_FACE_COMPONENT
 }
+
+// face_flux with the two sides evaluated one after the other through shared
+// memory, so that only one side's state is held in registers at a time.
+// On entry sl[s * ss] holds the left state and sr[s * ss] the right one; the
+// left side's fluxes go to sl (over its state) and its conserved values to
+// su, and the right side combines them with its own. Every value is the one
+// face_flux computes, from the same operations on the same operands.
+template <int MT, int DIR>
+__device__ __forceinline__ void face_flux_split(const Dims &d, const pangu_params &p, int b, int k,
+                                                int j, int i, double *sl, const double *sr,
+                                                double *su, int ss, double *F, double *alfven) {
+  Geo g;
+  const long long fo = vidx(d, b, 0, k, j, i);
+  if (!face_metric<MT>(d, p, DIR, b, k, j, i, g)) {
+    alfven[aidx(d, b, DIR - 1, k, j, i)] = 0.0;
+#pragma unroll
+    for (int s = 0; s < NPRIM; ++s)
+      if (d.pidx[s] >= 0) F[fo + d.pidx[s] * d.ncell] = 0.0;
+    return;
+  }
+  const double gam = p.adiabatic_index;
+  const double sg = g.sg;
+  double vmaxL, vminL;
+  {
+    double P[NPRIM];
+#pragma unroll
+    for (int s = 0; s < NPRIM; ++s) P[s] = sl[s * ss];
+    State st;
+    calc_state<MT>(P, g, st);
+    fast_speed_from_state(gam, P, g, st, DIR, vmaxL, vminL);
+#define PGD_LEFT_COMPONENT(C)                                 \
+  if (d.pidx[C] >= 0) {                                       \
+    sl[C * ss] = flux_component<C>(gam, P, st, sg, DIR);      \
+    su[C * ss] = flux_component<C>(gam, P, st, sg, 0);        \
+  }
+    PGD_LEFT_COMPONENT(RHO)
+    PGD_LEFT_COMPONENT(ENY)
+    PGD_LEFT_COMPONENT(UX1)
+    PGD_LEFT_COMPONENT(UX2)
+    PGD_LEFT_COMPONENT(UX3)
+    PGD_LEFT_COMPONENT(BX1)
+    PGD_LEFT_COMPONENT(BX2)
+    PGD_LEFT_COMPONENT(BX3)
+    PGD_LEFT_COMPONENT(ENT)
+    PGD_LEFT_COMPONENT(KEL)
+#undef PGD_LEFT_COMPONENT
+  }
+  // the right side reads the left side's results back from shared memory
+  asm volatile("" ::: "memory");
+  double P[NPRIM];
+#pragma unroll
+  for (int s = 0; s < NPRIM; ++s) P[s] = sr[s * ss];
+  State st;
+  calc_state<MT>(P, g, st);
+  double vmaxR, vminR;
+  fast_speed_from_state(gam, P, g, st, DIR, vmaxR, vminR);
+  const double cmax = fabs(kmax(kmax(0., vmaxL), vmaxR));
+  const double cmin = fabs(kmax(kmax(0., -vminL), -vminR));
+  const double cms = kmax(cmax, cmin);
+  alfven[aidx(d, b, DIR - 1, k, j, i)] = cms;
+  const bool hll = p.riemann_solver == PANGU_RIEMANN_HLL;
+#define PGD_RIGHT_COMPONENT(C)                                                        \
+  if (d.pidx[C] >= 0) {                                                               \
+    const double fl = sl[C * ss];                                                     \
+    const double fr = flux_component<C>(gam, P, st, sg, DIR);                         \
+    const double ul = su[C * ss];                                                     \
+    const double ur = flux_component<C>(gam, P, st, sg, 0);                           \
+    F[fo + d.pidx[C] * d.ncell] =                                                     \
+        hll ? (cmax * fl + cmin * fr - cmax * cmin * (ur - ul)) / (cmax + cmin + 1e-20) \
+            : 0.5 * (fl + fr - cms * (ur - ul));                                      \
+  }
+  PGD_RIGHT_COMPONENT(RHO)
+  PGD_RIGHT_COMPONENT(ENY)
+  PGD_RIGHT_COMPONENT(UX1)
+  PGD_RIGHT_COMPONENT(UX2)
+  PGD_RIGHT_COMPONENT(UX3)
+  PGD_RIGHT_COMPONENT(BX1)
+  PGD_RIGHT_COMPONENT(BX2)
+  PGD_RIGHT_COMPONENT(BX3)
+  PGD_RIGHT_COMPONENT(ENT)
+  PGD_RIGHT_COMPONENT(KEL)
+#undef PGD_RIGHT_COMPONENT
+}
 #endif
 
 // x1 faces: a warp covers 31 consecutive faces of one row. Lane l
@@ -741,9 +829,16 @@ constexpr int kFacesPerWarp = 31;
 // spills). Bounds of 3 CTAs (168 registers) and of 5 or 6 (96 or 80) were
 // measured slower on the 2D torus (the latter two faster on the 3D one).
 constexpr int kFluxThreads = 128;
+// With one side's state in registers at a time (FP64, curved metrics) the
+// flux kernels run at 5 CTAs per SM (96 registers): measured 1.1 % faster per
+// cycle on the 2D and the 3D torus than both states at 4 CTAs (at 4 CTAs the
+// split alone gained nothing); on Minkowski (Orszag-Tang) it cost 1.6 %, so
+// it is not used there.
+constexpr bool split_faces(int mt) { return PGK_SPLIT_FACES && mt != MINKOWSKI; }
+constexpr int flux_blocks(int mt) { return split_faces(mt) ? 5 : 4; }
 
 template <int MT>
-__global__ void __launch_bounds__(kFluxThreads, 4) k_flux_x1(Dims d, pangu_params p, int k0, int k1,
+__global__ void __launch_bounds__(kFluxThreads, flux_blocks(MT)) k_flux_x1(Dims d, pangu_params p, int k0, int k1,
                                                       int j0, int j1, int i0, int i1,
                                                       const PT *P, double *F,
                                                       double *alfven) {
@@ -764,6 +859,29 @@ __global__ void __launch_bounds__(kFluxThreads, 4) k_flux_x1(Dims d, pangu_param
   const int c = i0 - 1 + seg * kFacesPerWarp + lane;
   const bool active = c <= i1;  // cell c is needed by face c (and c + 1)
   const bool use_mc = p.limiter == PANGU_LIMITER_MC;
+#if PGK_SPLIT_FACES
+  if (split_faces(MT)) {
+    // [3][NPRIM][blockDim.x]: upper-face values, lower-face values, and the
+    // left side's conserved values of face c. Face c reads the upper-face
+    // values of lane - 1, which no other lane reads, and writes its left
+    // fluxes over them.
+    extern __shared__ double fsm[];
+    const int ss = blockDim.x, t = threadIdx.x;
+#pragma unroll
+    for (int s = 0; s < NPRIM; ++s) {
+      FT up = 0, lo = 0;
+      if (d.pidx[s] >= 0 && active)
+        recon_cell(use_mc, P + vidx(d, b, d.pidx[s], k, j, c), 1, up, lo);
+      fsm[s * ss + t] = up;
+      fsm[(NPRIM + s) * ss + t] = lo;
+    }
+    __syncwarp();
+    if (lane == 0 || !active) return;
+    face_flux_split<MT, 1>(d, p, b, k, j, c, fsm + t - 1, fsm + NPRIM * ss + t,
+                           fsm + 2 * NPRIM * ss + t, ss, F, alfven);
+    return;
+  }
+#endif
   FT PL[NPRIM], PR[NPRIM];
 #pragma unroll
   for (int s = 0; s < NPRIM; ++s) {
@@ -803,6 +921,45 @@ __device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_param
   const bool use_mc = p.limiter == PANGU_LIMITER_MC;
   const int f0 = m0 + run * MARCH;
   const int f1 = min(f0 + MARCH - 1, m1);
+#if PGK_SPLIT_FACES
+  if (split_faces(MT)) {
+    // [4][NPRIM][blockDim.x], each thread's own: the upper-face values of the
+    // previous cell (then the left fluxes), the lower-face values of this
+    // cell, the left conserved values, and the upper-face values of this cell.
+    extern __shared__ double fsm[];
+    const int ss = blockDim.x;
+    double *carry = fsm + threadIdx.x, *next = fsm + 3 * NPRIM * ss + threadIdx.x;
+    double *lower = fsm + NPRIM * ss + threadIdx.x;
+    double *left_u = fsm + 2 * NPRIM * ss + threadIdx.x;
+    {
+      const int c = f0 - 1;
+      const int kk = DIR == 2 ? a : c, jj = DIR == 2 ? c : a;
+#pragma unroll
+      for (int s = 0; s < NPRIM; ++s) {
+        FT up = 0, lo;
+        if (d.pidx[s] >= 0)
+          recon_cell(use_mc, P + vidx(d, b, d.pidx[s], kk, jj, i), stride, up, lo);
+        carry[s * ss] = up;
+      }
+    }
+    for (int f = f0; f <= f1; ++f) {
+      const int kk = DIR == 2 ? a : f, jj = DIR == 2 ? f : a;
+#pragma unroll
+      for (int s = 0; s < NPRIM; ++s) {
+        FT up = 0, lo = 0;
+        if (d.pidx[s] >= 0)
+          recon_cell(use_mc, P + vidx(d, b, d.pidx[s], kk, jj, i), stride, up, lo);
+        next[s * ss] = up;
+        lower[s * ss] = lo;
+      }
+      face_flux_split<MT, DIR>(d, p, b, kk, jj, i, carry, lower, left_u, ss, F, alfven);
+      double *tmp = carry;
+      carry = next;
+      next = tmp;
+    }
+    return;
+  }
+#endif
   FT carry[NPRIM];
   {
     const int c = f0 - 1;
@@ -874,18 +1031,30 @@ __device__ __forceinline__ void flux_tile_body(const Dims &d, const pangu_params
   __syncthreads();
   const int f = mt0 + row;
   if (i > i1 || f > m1) return;
+  const int kk = DIR == 2 ? a : f, jj = DIR == 2 ? f : a;
+#if PGK_SPLIT_FACES
+  // sup[row][.][lane] and slo[row + 1][.][lane] are read by this thread only.
+  // Tiles of 8 rows keep both states in registers (their static shared
+  // memory would pass 48 KB).
+  constexpr bool split = split_faces(MT) && TF <= 4;
+  __shared__ double sul[split ? TF : 1][NPRIM][32];
+  if (split) {
+    face_flux_split<MT, DIR>(d, p, b, kk, jj, i, &sup[row][0][lane], &slo[row + 1][0][lane],
+                             &sul[split ? row : 0][0][lane], 32, F, alfven);
+    return;
+  }
+#endif
   FT PL[NPRIM], PR[NPRIM];
 #pragma unroll
   for (int s = 0; s < NPRIM; ++s) {
     PL[s] = sup[row][s][lane];
     PR[s] = slo[row + 1][s][lane];
   }
-  const int kk = DIR == 2 ? a : f, jj = DIR == 2 ? f : a;
   face_flux<MT, DIR>(d, p, b, kk, jj, i, PL, PR, F, alfven);
 }
 
 template <int MT, int DIR, int TF>
-__global__ void __launch_bounds__(32 * TF, TF == 4 ? 4 : 2) k_flux_tile(Dims d, pangu_params p, int k0,
+__global__ void __launch_bounds__(32 * TF, TF == 4 ? flux_blocks(MT) : 2) k_flux_tile(Dims d, pangu_params p, int k0,
                                                                      int k1, int j0, int j1, int i0,
                                                                      int i1, const PT *P, double *F,
                                                                      double *alfven) {
@@ -894,7 +1063,7 @@ __global__ void __launch_bounds__(32 * TF, TF == 4 ? 4 : 2) k_flux_tile(Dims d, 
 }
 
 template <int MT, int MARCH>
-__global__ void __launch_bounds__(kFluxThreads, 4) k_flux_march2(Dims d, pangu_params p, int k0, int k1,
+__global__ void __launch_bounds__(kFluxThreads, flux_blocks(MT)) k_flux_march2(Dims d, pangu_params p, int k0, int k1,
                                                           int j0, int j1, int i0, int i1,
                                                           const PT *P, double *F,
                                                           double *alfven) {
@@ -902,7 +1071,7 @@ __global__ void __launch_bounds__(kFluxThreads, 4) k_flux_march2(Dims d, pangu_p
   flux_march_body<MT, 2, MARCH>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
 }
 template <int MT, int MARCH>
-__global__ void __launch_bounds__(kFluxThreads, 4) k_flux_march3(Dims d, pangu_params p, int k0, int k1,
+__global__ void __launch_bounds__(kFluxThreads, flux_blocks(MT)) k_flux_march3(Dims d, pangu_params p, int k0, int k1,
                                                           int j0, int j1, int i0, int i1,
                                                           const PT *P, double *F,
                                                           double *alfven) {
@@ -1977,12 +2146,12 @@ inline long long box_count(int NB, int k0, int k1, int j0, int j1, int i0, int i
 // while the previous kernel of the stream drains; it waits for it in
 // pdl_grid_wait() before touching memory.
 template <typename... KArgs, typename... Args>
-inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t s,
-                              Args... args) {
+inline cudaError_t launch_pdl_smem(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                                   cudaStream_t s, Args... args) {
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = grid;
   cfg.blockDim = block;
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -1990,6 +2159,11 @@ inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, c
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t s,
+                              Args... args) {
+  return launch_pdl_smem(kernel, grid, block, 0, s, args...);
 }
 
 #define DISPATCH_MT(mt, KERNEL, grid, stream, ...)                          \
@@ -2075,8 +2249,9 @@ void launch_flux_dir(const pangu_engine *e, const pangu_pack *md, int dir, int m
   if (dir == 1) {
     const int nseg = (i1 - i0 + 1 + kFacesPerWarp - 1) / kFacesPerWarp;
     const long long warps = (long long)d.NB * (k1 - k0 + 1) * (j1 - j0 + 1) * nseg;
-    launch_pdl(k_flux_x1<MT>, dim3(grid_flux(32 * warps, threads)), dim3(threads), s, d, e->p, k0,
-               k1, j0, j1, i0, i1, P, F, md->alfven);
+    launch_pdl_smem(k_flux_x1<MT>, dim3(grid_flux(32 * warps, threads)), dim3(threads),
+                    split_faces(MT) ? 3 * NPRIM * threads * sizeof(double) : 0, s, d, e->p, k0,
+                    k1, j0, j1, i0, i1, P, F, md->alfven);
     return;
   }
   const int m = dir == 2 ? (j1 - j0 + 1) : (k1 - k0 + 1);
@@ -2097,13 +2272,14 @@ void launch_flux_dir(const pangu_engine *e, const pangu_pack *md, int dir, int m
   }
   const long long n = (long long)d.NB * na * ((m + march - 1) / march) * (i1 - i0 + 1);
   const unsigned g = grid_flux(n, threads);
-#define PGK_MARCH(M)                                                                         \
-  if (dir == 2)                                                                              \
-    launch_pdl(k_flux_march2<MT, M>, dim3(g), dim3(threads), s, d, e->p, k0, k1, j0, j1, i0, i1, \
-               P, F, md->alfven);                                                            \
-  else                                                                                       \
-    launch_pdl(k_flux_march3<MT, M>, dim3(g), dim3(threads), s, d, e->p, k0, k1, j0, j1, i0, i1, \
-               P, F, md->alfven);
+  const size_t msm = split_faces(MT) ? 4 * NPRIM * threads * sizeof(double) : 0;
+#define PGK_MARCH(M)                                                                           \
+  if (dir == 2)                                                                                \
+    launch_pdl_smem(k_flux_march2<MT, M>, dim3(g), dim3(threads), msm, s, d, e->p, k0, k1, j0, \
+                    j1, i0, i1, P, F, md->alfven);                                             \
+  else                                                                                         \
+    launch_pdl_smem(k_flux_march3<MT, M>, dim3(g), dim3(threads), msm, s, d, e->p, k0, k1, j0, \
+                    j1, i0, i1, P, F, md->alfven);
   switch (march) {
     case 1: PGK_MARCH(1) break;
     case 2: PGK_MARCH(2) break;
