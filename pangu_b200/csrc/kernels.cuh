@@ -551,6 +551,22 @@ __global__ void __launch_bounds__(kThreads) k_calc_cons(Dims d, pangu_params p, 
 // from the two states, in the reference's operation order.
 // ---------------------------------------------------------------------------
 
+// Riemann solver and limiter of an FP64 flux kernel instance, fixed at
+// compile time so that the other option's arithmetic is not in the kernel
+// (measured 3.4 % per RK2 cycle on the 3D torus against runtime flags): bit 0
+// HLL (else LAXF), bit 1 MC (else PPM4). The mixed form keeps runtime flags
+// (one instance, OPT 0): compiled in, the options change ptxas's contraction
+// choices there, and its errors against FP64 came out larger (entropies
+// 2.0e-2 against 6.9e-3 on the MC/HLL torus after 10 cycles).
+constexpr int kFluxHLL = 1, kFluxMC = 2;
+#if PGK_MIXED
+#define PGK_FLUX_HLL(p) ((p).riemann_solver == PANGU_RIEMANN_HLL)
+#define PGK_FLUX_MC(p) ((p).limiter == PANGU_LIMITER_MC)
+#else
+#define PGK_FLUX_HLL(p) ((OPT & kFluxHLL) != 0)
+#define PGK_FLUX_MC(p) ((OPT & kFluxMC) != 0)
+#endif
+
 // Reconstruction of one variable in cell q (stride s along the direction):
 // ql_ip1 = value at the upper face, qr_i = value at the lower face
 // (interpolater_mc.h:38-48, interpolater_ppm4.h:29-67).
@@ -616,7 +632,7 @@ __device__ __forceinline__ FT flux_component_t(FT gam, const FT P[NPRIM], const 
 
 // Riemann flux and fast speed at the lower face of (b, k, j, i) along DIR in
 // FT arithmetic; the metric is evaluated in FP64 and rounded once.
-template <int MT, int DIR>
+template <int MT, int DIR, int OPT>
 __device__ __forceinline__ void face_flux(const Dims &d, const pangu_params &p, int b, int k, int j,
                                           int i, const FT PL[NPRIM], const FT PR[NPRIM],
                                           double *F, double *alfven) {
@@ -659,7 +675,7 @@ __device__ __forceinline__ void face_flux(const Dims &d, const pangu_params &p, 
   const FT cmin = fabs(tmax(tmax(FT(0), -vminL), -vminR));
   const FT cms = tmax(cmax, cmin);
   alfven[aidx(d, b, DIR - 1, k, j, i)] = cms;
-  const bool hll = p.riemann_solver == PANGU_RIEMANN_HLL;
+  const bool hll = PGK_FLUX_HLL(p);
   const FT ihll = FT(1) / (cmax + cmin + FT(1e-20));
 #define PGD_FACE_COMPONENT(C)                                                         \
   if (d.pidx[C] >= 0) {                                                               \
@@ -686,7 +702,7 @@ __device__ __forceinline__ void face_flux(const Dims &d, const pangu_params &p, 
 #else
 // Riemann flux and fast speed at the lower face of (b, k, j, i) along DIR
 // from the left and right states.
-template <int MT, int DIR>
+template <int MT, int DIR, int OPT>
 __device__ __forceinline__ void face_flux(const Dims &d, const pangu_params &p, int b, int k, int j,
                                           int i, const double PL[NPRIM], const double PR[NPRIM],
                                           double *F, double *alfven) {
@@ -713,7 +729,7 @@ __device__ __forceinline__ void face_flux(const Dims &d, const pangu_params &p, 
   const double cmin = fabs(kmax(kmax(0., -vminL), -vminR));
   const double cms = kmax(cmax, cmin);
   alfven[aidx(d, b, DIR - 1, k, j, i)] = cms;
-  const bool hll = p.riemann_solver == PANGU_RIEMANN_HLL;
+  const bool hll = PGK_FLUX_HLL(p);
 #define PGD_FACE_COMPONENT(C)                                                         \
   if (d.pidx[C] >= 0) {                                                               \
     const double fl = flux_component<C>(gam, PL, sL, sg, DIR);                        \
@@ -743,7 +759,7 @@ __device__ __forceinline__ void face_flux(const Dims &d, const pangu_params &p, 
 // left side's fluxes go to sl (over its state) and its conserved values to
 // su, and the right side combines them with its own. Every value is the one
 // face_flux computes, from the same operations on the same operands.
-template <int MT, int DIR>
+template <int MT, int DIR, int OPT>
 __device__ __forceinline__ void face_flux_split(const Dims &d, const pangu_params &p, int b, int k,
                                                 int j, int i, double *sl, const double *sr,
                                                 double *su, int ss, double *F, double *alfven) {
@@ -796,7 +812,7 @@ __device__ __forceinline__ void face_flux_split(const Dims &d, const pangu_param
   const double cmin = fabs(kmax(kmax(0., -vminL), -vminR));
   const double cms = kmax(cmax, cmin);
   alfven[aidx(d, b, DIR - 1, k, j, i)] = cms;
-  const bool hll = p.riemann_solver == PANGU_RIEMANN_HLL;
+  const bool hll = PGK_FLUX_HLL(p);
 #define PGD_RIGHT_COMPONENT(C)                                                        \
   if (d.pidx[C] >= 0) {                                                               \
     const double fl = sl[C * ss];                                                     \
@@ -837,7 +853,7 @@ constexpr int kFluxThreads = 128;
 constexpr bool split_faces(int mt) { return PGK_SPLIT_FACES && mt != MINKOWSKI; }
 constexpr int flux_blocks(int mt) { return split_faces(mt) ? 5 : 4; }
 
-template <int MT>
+template <int MT, int OPT>
 __global__ void __launch_bounds__(kFluxThreads, flux_blocks(MT)) k_flux_x1(Dims d, pangu_params p, int k0, int k1,
                                                       int j0, int j1, int i0, int i1,
                                                       const PT *P, double *F,
@@ -858,7 +874,7 @@ __global__ void __launch_bounds__(kFluxThreads, flux_blocks(MT)) k_flux_x1(Dims 
   const int j = j0 + (int)jr;
   const int c = i0 - 1 + seg * kFacesPerWarp + lane;
   const bool active = c <= i1;  // cell c is needed by face c (and c + 1)
-  const bool use_mc = p.limiter == PANGU_LIMITER_MC;
+  const bool use_mc = PGK_FLUX_MC(p);
 #if PGK_SPLIT_FACES
   if (split_faces(MT)) {
     // [3][NPRIM][blockDim.x]: upper-face values, lower-face values, and the
@@ -877,7 +893,7 @@ __global__ void __launch_bounds__(kFluxThreads, flux_blocks(MT)) k_flux_x1(Dims 
     }
     __syncwarp();
     if (lane == 0 || !active) return;
-    face_flux_split<MT, 1>(d, p, b, k, j, c, fsm + t - 1, fsm + NPRIM * ss + t,
+    face_flux_split<MT, 1, OPT>(d, p, b, k, j, c, fsm + t - 1, fsm + NPRIM * ss + t,
                            fsm + 2 * NPRIM * ss + t, ss, F, alfven);
     return;
   }
@@ -892,14 +908,14 @@ __global__ void __launch_bounds__(kFluxThreads, flux_blocks(MT)) k_flux_x1(Dims 
     PR[s] = lo;
   }
   if (lane == 0 || !active) return;
-  face_flux<MT, 1>(d, p, b, k, j, c, PL, PR, F, alfven);
+  face_flux<MT, 1, OPT>(d, p, b, k, j, c, PL, PR, F, alfven);
 }
 
 // x2 / x3 faces: a thread marches over MARCH consecutive faces of one
 // column, carrying the upper-face value of the previous cell. A deeper march
 // reconstructs fewer cells twice but gives fewer threads; the autotuner picks
 // the depth (and the CTA size) for the engine's grid.
-template <int MT, int DIR, int MARCH>
+template <int MT, int DIR, int MARCH, int OPT>
 __device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_params &p, int k0,
                                                 int k1, int j0, int j1, int i0, int i1,
                                                 const PT *P, double *F, double *alfven) {
@@ -918,7 +934,7 @@ __device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_param
   const int b = slot_of(d, (int)div_fast(r, na, ar));
   const int a = a0 + (int)ar;
   const long long stride = DIR == 2 ? (long long)d.N1 : (long long)d.N1 * d.N2;
-  const bool use_mc = p.limiter == PANGU_LIMITER_MC;
+  const bool use_mc = PGK_FLUX_MC(p);
   const int f0 = m0 + run * MARCH;
   const int f1 = min(f0 + MARCH - 1, m1);
 #if PGK_SPLIT_FACES
@@ -952,7 +968,7 @@ __device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_param
         next[s * ss] = up;
         lower[s * ss] = lo;
       }
-      face_flux_split<MT, DIR>(d, p, b, kk, jj, i, carry, lower, left_u, ss, F, alfven);
+      face_flux_split<MT, DIR, OPT>(d, p, b, kk, jj, i, carry, lower, left_u, ss, F, alfven);
       double *tmp = carry;
       carry = next;
       next = tmp;
@@ -981,7 +997,7 @@ __device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_param
       if (d.pidx[s] >= 0)
         recon_cell(use_mc, P + vidx(d, b, d.pidx[s], kk, jj, i), stride, up[s], PR[s]);
     }
-    face_flux<MT, DIR>(d, p, b, kk, jj, i, carry, PR, F, alfven);
+    face_flux<MT, DIR, OPT>(d, p, b, kk, jj, i, carry, PR, F, alfven);
 #pragma unroll
     for (int s = 0; s < NPRIM; ++s) carry[s] = up[s];
   }
@@ -993,7 +1009,7 @@ __device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_param
 // and lower values (a march reconstructs (MARCH + 1) / MARCH cells per face,
 // a tile (TF + 1) / TF). The face arithmetic is face_flux's, so the results
 // are those of the march kernels.
-template <int MT, int DIR, int TF>
+template <int MT, int DIR, int TF, int OPT>
 __device__ __forceinline__ void flux_tile_body(const Dims &d, const pangu_params &p, int k0, int k1,
                                                int j0, int j1, int i0, int i1, const PT *P,
                                                double *F, double *alfven) {
@@ -1013,7 +1029,7 @@ __device__ __forceinline__ void flux_tile_body(const Dims &d, const pangu_params
   const int lane = threadIdx.x & 31, row = threadIdx.x >> 5;
   const int i = i0 + (int)ti * 32 + lane;
   const long long stride = DIR == 2 ? (long long)d.N1 : (long long)d.N1 * d.N2;
-  const bool use_mc = p.limiter == PANGU_LIMITER_MC;
+  const bool use_mc = PGK_FLUX_MC(p);
   // cells mt0 - 1 .. mt0 + TF - 1: the lower neighbour of every face of the tile
   for (int cr = row; cr <= TF; cr += TF) {
     const int c = mt0 - 1 + cr;
@@ -1039,7 +1055,7 @@ __device__ __forceinline__ void flux_tile_body(const Dims &d, const pangu_params
   constexpr bool split = split_faces(MT) && TF <= 4;
   __shared__ double sul[split ? TF : 1][NPRIM][32];
   if (split) {
-    face_flux_split<MT, DIR>(d, p, b, kk, jj, i, &sup[row][0][lane], &slo[row + 1][0][lane],
+    face_flux_split<MT, DIR, OPT>(d, p, b, kk, jj, i, &sup[row][0][lane], &slo[row + 1][0][lane],
                              &sul[split ? row : 0][0][lane], 32, F, alfven);
     return;
   }
@@ -1050,33 +1066,33 @@ __device__ __forceinline__ void flux_tile_body(const Dims &d, const pangu_params
     PL[s] = sup[row][s][lane];
     PR[s] = slo[row + 1][s][lane];
   }
-  face_flux<MT, DIR>(d, p, b, kk, jj, i, PL, PR, F, alfven);
+  face_flux<MT, DIR, OPT>(d, p, b, kk, jj, i, PL, PR, F, alfven);
 }
 
-template <int MT, int DIR, int TF>
+template <int MT, int DIR, int TF, int OPT>
 __global__ void __launch_bounds__(32 * TF, TF == 4 ? flux_blocks(MT) : 2) k_flux_tile(Dims d, pangu_params p, int k0,
                                                                      int k1, int j0, int j1, int i0,
                                                                      int i1, const PT *P, double *F,
                                                                      double *alfven) {
   pdl_grid_wait();
-  flux_tile_body<MT, DIR, TF>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
+  flux_tile_body<MT, DIR, TF, OPT>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
 }
 
-template <int MT, int MARCH>
+template <int MT, int MARCH, int OPT>
 __global__ void __launch_bounds__(kFluxThreads, flux_blocks(MT)) k_flux_march2(Dims d, pangu_params p, int k0, int k1,
                                                           int j0, int j1, int i0, int i1,
                                                           const PT *P, double *F,
                                                           double *alfven) {
   pdl_grid_wait();
-  flux_march_body<MT, 2, MARCH>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
+  flux_march_body<MT, 2, MARCH, OPT>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
 }
-template <int MT, int MARCH>
+template <int MT, int MARCH, int OPT>
 __global__ void __launch_bounds__(kFluxThreads, flux_blocks(MT)) k_flux_march3(Dims d, pangu_params p, int k0, int k1,
                                                           int j0, int j1, int i0, int i1,
                                                           const PT *P, double *F,
                                                           double *alfven) {
   pdl_grid_wait();
-  flux_march_body<MT, 3, MARCH>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
+  flux_march_body<MT, 3, MARCH, OPT>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
 }
 
 // ---------------------------------------------------------------------------
@@ -2231,7 +2247,7 @@ int run_calc_cons(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
 
 // Launches the flux kernel of one direction with a given march depth
 // (x2/x3) and CTA size.
-template <int MT>
+template <int MT, int OPT>
 void launch_flux_dir(const pangu_engine *e, const pangu_pack *md, int dir, int march, int threads,
                      cudaStream_t s) {
   const Dims &d = e->d;
@@ -2249,7 +2265,7 @@ void launch_flux_dir(const pangu_engine *e, const pangu_pack *md, int dir, int m
   if (dir == 1) {
     const int nseg = (i1 - i0 + 1 + kFacesPerWarp - 1) / kFacesPerWarp;
     const long long warps = (long long)d.NB * (k1 - k0 + 1) * (j1 - j0 + 1) * nseg;
-    launch_pdl_smem(k_flux_x1<MT>, dim3(grid_flux(32 * warps, threads)), dim3(threads),
+    launch_pdl_smem(k_flux_x1<MT, OPT>, dim3(grid_flux(32 * warps, threads)), dim3(threads),
                     split_faces(MT) ? 3 * NPRIM * threads * sizeof(double) : 0, s, d, e->p, k0,
                     k1, j0, j1, i0, i1, P, F, md->alfven);
     return;
@@ -2260,7 +2276,7 @@ void launch_flux_dir(const pangu_engine *e, const pangu_pack *md, int dir, int m
     const long long nt = (long long)d.NB * na * ((m + threads / 32 - 1) / (threads / 32)) *
                          ((i1 - i0 + 1 + 31) / 32);
 #define PGK_TILE(D, TF)                                                                     \
-  launch_pdl(k_flux_tile<MT, D, TF>, dim3((unsigned)nt), dim3(32 * TF), s, d, e->p, k0, k1, j0, \
+  launch_pdl(k_flux_tile<MT, D, TF, OPT>, dim3((unsigned)nt), dim3(32 * TF), s, d, e->p, k0, k1, j0, \
              j1, i0, i1, P, F, md->alfven)
     if (dir == 2) {
       if (threads == 128) PGK_TILE(2, 4); else PGK_TILE(2, 8);
@@ -2275,10 +2291,10 @@ void launch_flux_dir(const pangu_engine *e, const pangu_pack *md, int dir, int m
   const size_t msm = split_faces(MT) ? 4 * NPRIM * threads * sizeof(double) : 0;
 #define PGK_MARCH(M)                                                                           \
   if (dir == 2)                                                                                \
-    launch_pdl_smem(k_flux_march2<MT, M>, dim3(g), dim3(threads), msm, s, d, e->p, k0, k1, j0, \
+    launch_pdl_smem(k_flux_march2<MT, M, OPT>, dim3(g), dim3(threads), msm, s, d, e->p, k0, k1, j0, \
                     j1, i0, i1, P, F, md->alfven);                                             \
   else                                                                                         \
-    launch_pdl_smem(k_flux_march3<MT, M>, dim3(g), dim3(threads), msm, s, d, e->p, k0, k1, j0, \
+    launch_pdl_smem(k_flux_march3<MT, M, OPT>, dim3(g), dim3(threads), msm, s, d, e->p, k0, k1, j0, \
                     j1, i0, i1, P, F, md->alfven);
   switch (march) {
     case 1: PGK_MARCH(1) break;
@@ -2288,13 +2304,30 @@ void launch_flux_dir(const pangu_engine *e, const pangu_pack *md, int dir, int m
 #undef PGK_MARCH
 }
 
+template <int MT>
+void launch_flux_opt(const pangu_engine *e, const pangu_pack *md, int dir, int march, int threads,
+                     cudaStream_t s) {
+#if PGK_MIXED
+  launch_flux_dir<MT, 0>(e, md, dir, march, threads, s);  // options read at run time
+#else
+  const int opt = (e->p.riemann_solver == PANGU_RIEMANN_HLL ? kFluxHLL : 0) |
+                  (e->p.limiter == PANGU_LIMITER_MC ? kFluxMC : 0);
+  switch (opt) {
+    case 0: launch_flux_dir<MT, 0>(e, md, dir, march, threads, s); break;
+    case kFluxHLL: launch_flux_dir<MT, kFluxHLL>(e, md, dir, march, threads, s); break;
+    case kFluxMC: launch_flux_dir<MT, kFluxMC>(e, md, dir, march, threads, s); break;
+    default: launch_flux_dir<MT, kFluxHLL | kFluxMC>(e, md, dir, march, threads, s); break;
+  }
+#endif
+}
+
 int run_flux_dir(pangu_engine *e, const pangu_pack *md, int dir, int march, int threads,
                  cudaStream_t s) {
   switch (e->p.metric_type) {
-    case PANGU_METRIC_MKS: launch_flux_dir<MKS>(e, md, dir, march, threads, s); break;
-    case PANGU_METRIC_BL: launch_flux_dir<BL>(e, md, dir, march, threads, s); break;
-    case PANGU_METRIC_CKS: launch_flux_dir<CKS>(e, md, dir, march, threads, s); break;
-    default: launch_flux_dir<MINKOWSKI>(e, md, dir, march, threads, s); break;
+    case PANGU_METRIC_MKS: launch_flux_opt<MKS>(e, md, dir, march, threads, s); break;
+    case PANGU_METRIC_BL: launch_flux_opt<BL>(e, md, dir, march, threads, s); break;
+    case PANGU_METRIC_CKS: launch_flux_opt<CKS>(e, md, dir, march, threads, s); break;
+    default: launch_flux_opt<MINKOWSKI>(e, md, dir, march, threads, s); break;
   }
   ++e->launches;
   return check_launch();
