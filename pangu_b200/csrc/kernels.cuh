@@ -841,9 +841,10 @@ __device__ __forceinline__ void face_flux_split(const Dims &d, const pangu_param
 // reconstructs cell c = f0 - 1 + l; face c takes its left state from lane
 // l - 1 (upper-face value of cell c - 1) and its right state from lane l.
 constexpr int kFacesPerWarp = 31;
-// Flux kernels: at most 128 registers (4 CTAs of 4 warps per SM, a few
-// spills). Bounds of 3 CTAs (168 registers) and of 5 or 6 (96 or 80) were
-// measured slower on the 2D torus (the latter two faster on the 3D one).
+// Flux kernels holding both states of a face in registers: at most 128
+// registers (4 CTAs of 4 warps per SM, a few spills). For them, bounds of 3
+// CTAs (168 registers) and of 5 or 6 (96 or 80) were measured slower on the
+// 2D torus (the latter two faster on the 3D one).
 constexpr int kFluxThreads = 128;
 // With one side's state in registers at a time (FP64, curved metrics) the
 // flux kernels run at 5 CTAs per SM (96 registers): measured 1.1 % faster per
