@@ -7,8 +7,8 @@ operation as the oracle does (no contraction, the oracle's operation order,
 the metric tables holding the dense values bit for bit, the shared pow), so
 every task is compared bit for bit over the whole index domain, and so are
 whole RK2 steps (primitives, conserved variables, flags, dt, counters). The
-north star's tolerances (relative L1 <= 1e-12 after one step, <= 1e-9 after
-ten) are asserted as well, as the contract's own statement.
+FP64 accuracy targets (relative L1 <= 1e-12 after one step, <= 1e-9 after
+ten) are asserted as well, as a statement of their own.
 """
 import numpy as np
 import pytest
