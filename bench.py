@@ -45,24 +45,9 @@ from pangu_b200 import problems  # noqa: E402
 
 METRIC = "zone-cycles/s"
 
-# single-job workloads: input builder, job length (RK2 cycles), config keys
-SINGLE = {
-    "torus2d": (lambda seed: problems.fm_torus_input(nx1=512, nx2=256, seed=seed), 200,
-                {"grid": "512x256", "meshblocks": 1, "limiter": "ppm4",
-                 "riemann_solver": "laxf", "recovery": "chainer", "electron_heating": True,
-                 "metric": "mks a=0.9375 h=0.7"}),
-    "ot": (lambda seed: problems.orszag_tang_input(n=256), 100,
-           {"grid": "256x256", "meshblocks": 1, "limiter": "mc", "riemann_solver": "laxf",
-            "recovery": "chainer", "electron_heating": False, "metric": "minkowski"}),
-    "torus3d": (lambda seed: problems.fm_torus_input(nx1=256, nx2=128, nx3=128,
-                                                     bx=(64, 64, 64), seed=seed), 50,
-                {"grid": "256x128x128", "meshblocks": "16 x 64^3", "limiter": "ppm4",
-                 "riemann_solver": "laxf", "recovery": "chainer", "electron_heating": True,
-                 "metric": "mks a=0.9375 h=0.7"}),
-}
-WORKLOAD_NAMES = {"torus2d": "fm_torus_mks_2d_512x256", "ot": "orszag_tang_2d_256x256",
-                  "torus3d": "fm_torus_mks_3d_256x128x128", "batch48": "fm_torus_mks_2d_batch48",
-                  "serve": "serving_stream_bw_ot_torus"}
+from pangu_b200.workloads import (BATCH_BLOCK, SINGLE, WORKLOAD_NAMES,  # noqa: E402,F401
+                                  batch_jobs, initial_state, interior_cells, job_input,
+                                  serve_jobs)
 
 
 def peaks():
@@ -74,32 +59,8 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def job_input(workload, precision="fp64", seed=0):
-    pin = SINGLE[workload][0](seed)
-    pin.set("b200", "precision", precision)
-    return pin
-
-
 def workload_input(seed=0):
     return job_input("torus2d", "fp64", seed)
-
-
-def initial_state(pin):
-    packages = prm.process_packages(pin)
-    mesh = prm.mesh_struct(pin)
-    geo = problems.Geometry(mesh)
-    if packages["metric"].params["metric_type"] == "minkowski":
-        gam = packages["core"].params["adiabatic_index"]
-        prim = (problems.brio_wu(geo, packages) if gam == 2.0
-                else problems.orszag_tang(geo, packages))
-    else:
-        prim = problems.fm_torus(geo, packages, pin)
-    return packages, mesh, geo, prim
-
-
-def interior_cells(pin):
-    return int(np.prod([pin.get_or_add_integer("parthenon/mesh", f"nx{d}", 1)
-                        for d in (1, 2, 3)]))
 
 
 def workload_name(workload, precision):
@@ -564,34 +525,6 @@ def cpu_baseline(pin, prim0, budget_s=15.0, max_steps=None):
 # ---------------------------------------------------------------------------
 # batch of 48 tori in one block pool
 # ---------------------------------------------------------------------------
-BATCH_BLOCK = (128, 64, 1)
-
-
-def batch_jobs(precision, n=48, seed=1234, states=False):
-    """48 MKS tori: grids drawn from {128x64, 256x128, 384x192, 512x256}, spin
-    a ~ U[0, 0.98], beta ~ logU[30, 300], rmax ~ U[10, 14] (seeded). A draw
-    with no bound torus (low spin with rmax near 10 for rin = 6) is redrawn.
-    Returns the inputs, or (inputs, initial states) with states=True."""
-    rng = np.random.default_rng(seed)
-    grids = [(128, 64), (256, 128), (384, 192), (512, 256)]
-    jobs, prims = [], []
-    while len(jobs) < n:
-        nx1, nx2 = grids[int(rng.integers(len(grids)))]
-        a = float(rng.uniform(0.0, 0.98))
-        beta = float(math.exp(rng.uniform(math.log(30.0), math.log(300.0))))
-        rmax = float(rng.uniform(10.0, 14.0))
-        pin = problems.fm_torus_input(nx1=nx1, nx2=nx2, bx=BATCH_BLOCK, a=a, beta=beta,
-                                      rmax=rmax, seed=len(jobs))
-        pin.set("b200", "precision", precision)
-        try:
-            prim = initial_state(pin)[3]
-        except ValueError:
-            continue
-        jobs.append(pin)
-        prims.append(prim)
-    return (jobs, prims) if states else jobs
-
-
 def run_batch(args):
     import torch
     from pangu_b200.engine import Pool
@@ -668,31 +601,6 @@ def run_batch(args):
 # ---------------------------------------------------------------------------
 # serving stream
 # ---------------------------------------------------------------------------
-def serve_jobs(precision, n, rate, seed=7):
-    """Poisson arrivals (rate per second) of Brio-Wu tubes (1024-8192 cells,
-    blocks of 1024), Orszag-Tang vortices (128^2-512^2, blocks of 128^2) and
-    MKS tori (256x128-512x256, blocks of 128x64) at 200-2000 RK2 cycles."""
-    rng = np.random.default_rng(seed)
-    t = 0.0
-    jobs = []
-    for q in range(n):
-        t += float(rng.exponential(1.0 / rate))
-        kind = ("bw", "ot", "torus")[q % 3]
-        if kind == "bw":
-            pin = problems.brio_wu_input(n=int(rng.choice([1024, 2048, 4096, 8192])),
-                                         nblock=1024)
-        elif kind == "ot":
-            pin = problems.orszag_tang_input(n=int(rng.choice([128, 256, 384, 512])),
-                                             nblock=128)
-        else:
-            nx1, nx2 = [(256, 128), (384, 192), (512, 256)][int(rng.integers(3))]
-            pin = problems.fm_torus_input(nx1=nx1, nx2=nx2, bx=BATCH_BLOCK,
-                                          a=float(rng.uniform(0.0, 0.98)), seed=q)
-        pin.set("b200", "precision", precision)
-        jobs.append((kind, pin, int(rng.integers(200, 2001)), t))
-    return jobs
-
-
 def run_serve(args):
     import torch  # noqa: F401  (initialises the CUDA context)
     from pangu_b200.engine import Server

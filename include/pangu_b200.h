@@ -291,11 +291,25 @@ int pangu_stage_end(pangu_engine *e, int stage, const pangu_pack *base,
  * array of 3 x 4096 minima (96 KiB on every GPU that loads the library, held
  * until exit): meshes with more than 4096 blocks get PANGU_ETOOBIG. The first
  * call on a device looks the array's address up (cudaGetSymbolAddress) with
- * that device current; make that first call before any stream capture. All
- * calls share the array: calls that overlap on the GPU (other streams or
- * devices sharing a context) race, so serialise them. */
+ * that device current and keeps it for the life of the process; make that
+ * first call before any stream capture, and do not reset the device or its
+ * primary context (cudaDeviceReset) between calls, which would leave the
+ * kept address stale. Calls on the same device share the array: calls whose
+ * execution overlaps (e.g. on different streams) race, so serialise them.
+ * Calls on different devices are independent (each GPU holds its own copy). */
 int pangu_estimate_dt_noalloc(const pangu_params *params, const pangu_mesh *mesh,
                               const double *alfven, double *dt_out, void *stream);
+
+/* ---- measurement ------------------------------------------------------- */
+/* FP64 fused multiply-add throughput of the current device (no counterpart
+ * in the reference): launches `ctas` CTAs of 256 threads, each thread running
+ * eight independent DFMA chains of `iters` steps; the caller times the launch
+ * with CUDA events on `stream` and divides pangu_fp64_peak_flops(ctas, iters)
+ * by its duration. sink: a device double[ctas] that is never written in
+ * practice. This is the FP64 roofline's denominator: the stage kernels are
+ * bound by FP64 issue and latency, not by HBM bandwidth. */
+int pangu_fp64_peak(int ctas, int iters, double *sink, void *stream);
+double pangu_fp64_peak_flops(int ctas, int iters);
 
 /* Device dt policy applied after each cycle, per active job:
  * dt[job] = min(dt_factor*dt[job], dt_est[job]). */

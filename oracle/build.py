@@ -6,6 +6,11 @@
   where they lie, through the stand-in headers of ``oracle/refshim``. Only
   when the reference sources are present (this container); the built file
   travels with the repository snapshot like any other built library.
+* ``oracle/_ref/libpangu_reftasks.so`` -- the reference's own stage tasks
+  (REF_TASK_SOURCES below, compiled from where they lie) over the host-only
+  Parthenon stand-in of ``oracle/refshim/parthenon/package.hpp``, with the
+  driver ``ref_tasks.cc``; pow is the correctly rounded one of pgmath.h
+  (-DPANGU_REFSHIM_CR_POW). Only when the reference sources are present.
 
 Both are compiled -O2 -ffp-contract=off: no fused multiply-add anywhere, so
 the restatement and the reference's host code round identically.
@@ -18,10 +23,23 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-REFERENCE_SRC = "/root/reference/pangu/src"
+# The reference's solver sources (pangu/src of the PANGU tree): from the
+# PANGU_REFERENCE_SRC environment variable, else the read-only checkout this
+# repository was built beside.
+REFERENCE_SRC = os.environ.get("PANGU_REFERENCE_SRC", "/root/reference/pangu/src")
 
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 REFCELL_SO = os.path.join(HERE, "_ref", "libpangu_refcell.so")
+REFTASKS_SO = os.path.join(HERE, "_ref", "libpangu_reftasks.so")
+
+# The reference's stage-task sources (paths under pangu/src).
+REF_TASK_SOURCES = (
+    "fixer/primitive_fixer.cc", "fixer/recovery_fixer.cc",
+    "riemann_solver/conservative.cc", "riemann_solver/laxf.cc", "riemann_solver/hll.cc",
+    "riemann_solver/riemann_solver.cc", "riemann_solver/source_term.cc",
+    "riemann_solver/electron_heating.cc", "constrained_transport/constrained_transport.cc",
+    "recovery/invertor.cc", "initialization/timestep_estimation.cc",
+)
 
 COMMON = ["-O2", "-ffp-contract=off", "-std=c++17", "-shared", "-fPIC"]
 
@@ -59,7 +77,26 @@ def build_refcell(force: bool = False) -> str | None:
     return REFCELL_SO
 
 
+def build_reftasks(force: bool = False) -> str | None:
+    if not os.path.isdir(REFERENCE_SRC):
+        return REFTASKS_SO if os.path.exists(REFTASKS_SO) else None
+    shim = os.path.join(HERE, "refshim")
+    src = [os.path.join(HERE, "ref_tasks.cc"), os.path.join(shim, "parthenon", "package.hpp"),
+           os.path.join(shim, "Kokkos_Core.hpp"),
+           os.path.join(ROOT, "pangu_b200", "csrc", "pgmath.h")]
+    ref = [os.path.join(REFERENCE_SRC, f) for f in REF_TASK_SOURCES]
+    if not force and _newer(REFTASKS_SO, src + ref):
+        return REFTASKS_SO
+    os.makedirs(os.path.dirname(REFTASKS_SO), exist_ok=True)
+    cmd = ["g++", *COMMON, "-DPANGU_REFSHIM_CR_POW", "-I", shim,
+           "-I", os.path.join(ROOT, "pangu_b200", "csrc"), "-I", os.path.join(ROOT, "include"),
+           "-I", REFERENCE_SRC, src[0], *ref, "-o", REFTASKS_SO]
+    subprocess.check_call(cmd)
+    return REFTASKS_SO
+
+
 if __name__ == "__main__":
     force = "--force" in sys.argv
     print(build_oracle(force))
     print(build_refcell(force))
+    print(build_reftasks(force))

@@ -88,6 +88,49 @@ def reflib():
     return _reflib
 
 
+_reftasks = None
+
+# task ids of ref_tasks.cc
+REF_TASKS = {"fix_primitive": 0, "calculate_conservative": 1, "calculate_fluxes": 2,
+             "constrained_transport": 3, "add_geometric_source": 4, "recovery": 5,
+             "apply_electron_heating": 6, "fix_recovery": 7, "estimate_dt": 8}
+
+
+def reftasks():
+    """The reference's own stage tasks over the Parthenon stand-in (only
+    where its sources exist, or where the built library travelled)."""
+    global _reftasks
+    if _reftasks is None:
+        path = _build.build_reftasks()
+        if path is None or not os.path.exists(path):
+            return None
+        L = C.CDLL(path)
+        L.ref_task.restype = C.c_int
+        L.ref_task.argtypes = [C.POINTER(abi.Params), C.POINTER(abi.Mesh), C.POINTER(abi.Pack),
+                               C.c_int, C.c_double, _D]
+        _reftasks = L
+    return _reftasks
+
+
+class RefTasks:
+    """The reference's task functions on host containers (HostContainer)."""
+
+    def __init__(self, params: abi.Params, mesh: abi.Mesh):
+        self.L = reftasks()
+        if self.L is None:
+            raise RuntimeError("the reference's task library is not built")
+        self.params, self.mesh = params, mesh
+
+    def run(self, name, c, dt=0.0):
+        p = c.pack()
+        out = C.c_double(0.0)
+        rc = self.L.ref_task(C.byref(self.params), C.byref(self.mesh), C.byref(p),
+                             REF_TASKS[name], dt, C.byref(out))
+        if rc != 0:
+            raise RuntimeError(f"reference task {name} failed")
+        return out.value
+
+
 def dptr(a: np.ndarray):
     assert a.dtype == np.float64 and a.flags.c_contiguous
     return a.ctypes.data_as(_D)

@@ -1828,23 +1828,36 @@ __global__ void __launch_bounds__(kThreads) k_bcs(Dims d, int enable_B, PT *P,
 // ---------------------------------------------------------------------------
 // EstimateTimestepMesh (timestep_estimation.cc:13-102).
 // ---------------------------------------------------------------------------
+// Per-cell dt values are reduced as order-preserving 64-bit keys: the sign
+// bit is set on non-negative doubles and every bit is flipped on negative
+// ones, so unsigned comparison of keys orders the doubles (negative values
+// included) and atomicMin works on them. The reference's
+// "if (timestep > dt) timestep = dt" (timestep_estimation.cc:56-92) takes a
+// negative dt as well and skips a NaN, which never compares below.
+__device__ __forceinline__ unsigned long long dt_key(double v) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double dt_unkey(unsigned long long k) {
+  const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+  return __longlong_as_double((long long)b);
+}
+
 __global__ void k_dt_init(int n, unsigned long long *mins) {
   pdl_grid_wait();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) mins[t] = (unsigned long long)__double_as_longlong(DBL_MAX);
+  if (t < n) mins[t] = dt_key(DBL_MAX);
 }
 
 // One CTA row per mesh block (blockIdx.y); warp and CTA minima, then one
-// atomic per CTA and direction. Positive doubles order like their bit
-// patterns; a NaN speed never lowers the minimum (the reference's
-// "if (dt_min > dt)" skips it as well).
+// atomic per CTA and direction.
 __device__ __forceinline__ void dt_reduce_cta(const Dims &d, double cfl, const double *alfven,
                                               unsigned long long *mins) {
   __shared__ unsigned long long red[3][kThreads / 32];
   const int b = slot_of(d, blockIdx.y);
   const int ni = d.ie - d.is + 1, nj = d.je - d.js + 1, nk = d.ke - d.ks + 1;
   const long long per = (long long)ni * nj * nk;
-  const unsigned long long big = (unsigned long long)__double_as_longlong(DBL_MAX);
+  const unsigned long long big = dt_key(DBL_MAX);
   unsigned long long m[3] = {big, big, big};
   const double cdx[3] = {MUL(cfl, dx_of(d, b, 0)), MUL(cfl, dx_of(d, b, 1)),
                          MUL(cfl, dx_of(d, b, 2))};
@@ -1857,9 +1870,9 @@ __device__ __forceinline__ void dt_reduce_cta(const Dims &d, double cfl, const d
     for (int dir = 0; dir < 3; ++dir) {
       if (!act[dir]) continue;
       const double dt = cdx[dir] / alfven[aidx(d, b, dir, k, j, i)];
-      if (dt >= 0.0) {
-        const unsigned long long bits = (unsigned long long)__double_as_longlong(dt);
-        m[dir] = bits < m[dir] ? bits : m[dir];
+      if (dt == dt) {
+        const unsigned long long key = dt_key(dt);
+        m[dir] = key < m[dir] ? key : m[dir];
       }
     }
   }
@@ -1902,9 +1915,9 @@ __device__ __forceinline__ void dt_finalize_jobs(const Dims &d, int njobs, const
     double gmin = DBL_MAX;
     for (int bb = s0; bb < s1; ++bb) {
       const int b = slot_of(d, bb);
-      const double m0 = __longlong_as_double((long long)mins[3 * b + 0]);
-      const double m1 = __longlong_as_double((long long)mins[3 * b + 1]);
-      const double m2 = __longlong_as_double((long long)mins[3 * b + 2]);
+      const double m0 = dt_unkey(mins[3 * b + 0]);
+      const double m1 = dt_unkey(mins[3 * b + 1]);
+      const double m2 = dt_unkey(mins[3 * b + 2]);
       const double bdt = 1.0 / (1.0 / m0 + 1.0 / m1 + 1.0 / m2);
       if (bdt < gmin) gmin = bdt;
     }
@@ -1945,7 +1958,7 @@ __global__ void __launch_bounds__(kThreads) k_dt_reduce_final(Dims d, double cfl
   const volatile unsigned long long *vm = mins;
   dt_finalize_jobs(d, njobs, jr, vm, dt_out, threadIdx.x, blockDim.x);
   __syncthreads();
-  const unsigned long long big = (unsigned long long)__double_as_longlong(DBL_MAX);
+  const unsigned long long big = dt_key(DBL_MAX);
   for (int t = threadIdx.x; t < nmins; t += blockDim.x) mins[t] = big;
   if (threadIdx.x == 0) *ticket = 0u;
 }
@@ -2544,7 +2557,7 @@ int run_estimate_dt(pangu_engine *e, const pangu_pack *md, double *dt_out, cudaS
   const Dims &d = e->d;
   const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
   const unsigned gx = (unsigned)std::min<long long>((n / std::max(1, d.NB) + kThreads - 1) / kThreads, 592);
-  // d_dtmin holds DBL_MAX and d_dt_ticket 0 between calls (set at pool_init)
+  // d_dtmin holds the key of DBL_MAX and d_dt_ticket 0 between calls (set at pool_init)
   launch_pdl(k_dt_reduce_final, dim3(std::max(1u, gx), d.NB), dim3(kThreads), s, d,
              e->p.cfl_number, md->alfven, e->d_dtmin, e->d_dt_ticket, e->njobs_active, e->d_jr,
              dt_out, 3 * e->capacity);

@@ -421,8 +421,10 @@ class Simulation:
 
     def autotune(self):
         """Tunes the flux kernels' tile shapes on this job's current state
-        (call between cycles, before capture)."""
+        (call between cycles). A captured cycle graph holds the old shapes,
+        so it is dropped; the next capture() records the tuned launches."""
         self.engine.autotune(self.base)
+        self._graph = None
 
     def capture(self):
         """Captures one RK2 cycle (both stages and the device dt policy) as a

@@ -1,0 +1,116 @@
+"""Runs a benchmark workload on the GPU for a given number of RK2 cycles.
+
+    python -m pangu_b200.run [--workload torus2d|ot|torus3d|batch48]
+                             [--precision fp64|mixed] [--cycles N]
+                             [--graph-cycles G] [--tiles X1,M2,T2,M3,T3]
+
+First ``--cycles`` cycles are launched from the host (every stage kernel once
+per stage, in a fixed order), then ``--graph-cycles`` cycles are captured once
+as a CUDA graph and replayed. ``--tiles`` pins the flux kernels' tile shapes
+(x1 threads, x2 march, x2 threads, x3 march, x3 threads; march 0 = a
+shared-memory tile) instead of the engine's defaults; nothing is autotuned, so
+the sequence of launches depends only on the arguments. That makes the run a
+fixed target for a profiler: the n-th launch of a kernel is always the same
+stage of the same cycle. ``--profile-cycle K`` brackets host cycle K (from 0)
+with cudaProfilerStart/Stop, so a profiler started with profiling off (ncu
+``--profile-from-start off``) sees exactly the launches of that cycle.
+Prints one JSON line: launches per host cycle, the device time per replayed
+cycle and the job's counters.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+from . import workloads
+
+
+def _set_tiles(engine, tiles):
+    if tiles:
+        x1, m2, t2, m3, t3 = (int(v) for v in tiles.split(","))
+        engine.set_flux_config(x1_threads=x1, x2_march=m2, x2_threads=t2, x3_march=m3,
+                               x3_threads=t3)
+
+
+def run(workload="torus2d", precision="fp64", cycles=40, graph_cycles=0, tiles=None,
+        profile_cycle=None, device=0):
+    import torch
+
+    from .engine import Pool, Simulation
+    torch.cuda.set_device(device)
+    if workload == "batch48":
+        pins, states = workloads.batch_jobs(precision, states=True)
+        nblocks = sum(st.shape[0] for st in states)
+        job = Pool(pins[0], nblocks, len(pins), device=device)
+        for pin, st in zip(pins, states):
+            job.attach(pin, st)
+        cells = sum(workloads.interior_cells(p) for p in pins)
+        host_step = lambda: job.step(graph=False)  # noqa: E731
+        graph_step = lambda: job.step(graph=True)  # noqa: E731
+    else:
+        pin = workloads.job_input(workload, precision)
+        prim0 = workloads.initial_state(pin)[3]
+        job = Simulation(pin, device=device)
+        job.set_primitives(prim0)
+        cells = workloads.interior_cells(pin)
+        host_step = job.step
+        graph_step = job.step
+    eng = job.engine
+    _set_tiles(eng, tiles)
+    torch.cuda.synchronize()
+    l0 = eng.launches()
+    t0 = time.perf_counter()
+    for c in range(cycles):
+        if c == profile_cycle:
+            torch.cuda.synchronize()
+            torch.cuda.profiler.start()
+        host_step()
+        if c == profile_cycle:
+            torch.cuda.synchronize()
+            torch.cuda.profiler.stop()
+    torch.cuda.synchronize()
+    host_s = time.perf_counter() - t0
+    per_cycle = (eng.launches() - l0) // max(cycles, 1)
+    out = {"workload": workload, "precision": precision, "interior_cells": cells,
+           "host_cycles": cycles, "launches_per_host_cycle": per_cycle,
+           "host_cycle_ms_wall": round(1e3 * host_s / max(cycles, 1), 4),
+           "flux_tiles": eng.flux_config()}
+    if graph_cycles > 0:
+        if workload != "batch48":
+            job.capture()
+        graph_step()  # the batch pool captures on its first graph step
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(graph_cycles - 1):
+            graph_step()
+        e1.record()
+        torch.cuda.synchronize()
+        n = max(graph_cycles - 1, 1)
+        ms = e0.elapsed_time(e1) / n
+        out.update({"graph_cycles": graph_cycles, "graph_cycle_ms": round(ms, 5),
+                    "zone_cycles_per_s": round(cells / (ms / 1e3), 1)})
+    out["counters"] = [int(v) for v in eng.counters()]
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", choices=["torus2d", "ot", "torus3d", "batch48"],
+                    default="torus2d")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--cycles", type=int, default=40)
+    ap.add_argument("--graph-cycles", type=int, default=0)
+    ap.add_argument("--tiles", default=None,
+                    help="x1_threads,x2_march,x2_threads,x3_march,x3_threads")
+    ap.add_argument("--profile-cycle", type=int, default=None,
+                    help="host cycle bracketed by cudaProfilerStart/Stop")
+    args = ap.parse_args()
+    print(json.dumps(run(args.workload, args.precision, args.cycles, args.graph_cycles,
+                         args.tiles, args.profile_cycle)), flush=True)
+
+
+if __name__ == "__main__":
+    main()
