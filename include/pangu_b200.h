@@ -324,10 +324,18 @@ int pangu_reset_counters(pangu_engine *e, void *stream);
 /* Number of CUDA kernels this handle has launched so far (host-side count). */
 long long pangu_launches(const pangu_engine *e);
 
+/* 1 if a kernel of this handle gave up a bounded wait (the TMA-staged flux
+ * kernels wait on an mbarrier for their copy, with a limit far beyond any
+ * copy's completion) and returned without its results, else 0 (host copy,
+ * synchronous). No counterpart in the reference. */
+int pangu_device_error(const pangu_engine *e, int32_t *flag_out);
+
 /* Autotuner of the flux kernels' tile shapes (no counterpart in the
  * reference): times each candidate shape of every direction -- CTA size 64
  * or 128, and for x2/x3 a march depth of 1, 2 or 4 faces per thread or a
- * shared-memory tile of 32 x 4 or 32 x 8 faces -- on
+ * shared-memory tile of 32 x 4 or 32 x 8 faces, and for every direction the
+ * form whose primitives one TMA copy per CTA stages into shared memory where
+ * the rows are whole 16-byte units -- on
  * the pack's own data and keeps the fastest for this engine. Every candidate
  * computes each face identically, so results never depend on the choice.
  * Overwrites the pack's fluxes and alfven (which every stage recomputes
@@ -337,10 +345,12 @@ int pangu_autotune(pangu_engine *e, const pangu_pack *md, void *stream);
 /* Current tile shapes: {march1, threads1, march2, threads2, march3,
  * threads3, tuned}. */
 int pangu_flux_config(const pangu_engine *e, int32_t out[7]);
-/* Sets the tile shapes {march1 (1), threads1, march2, threads2, march3,
- * threads3}: march 1, 2 or 4 with threads 64 or 128, or for x2 and x3 march
- * 0 (tiles of 32 x threads/32 faces, each cell reconstructed once) with
- * threads 128 or 256 (PANGU_EINVAL otherwise), e.g. to repeat a configuration
+/* Sets the tile shapes {march1, threads1, march2, threads2, march3,
+ * threads3}: march 1, 2 or 4 (x1: 1) with threads 64 or 128, or for x2 and x3
+ * march 0 (tiles of 32 x threads/32 faces, each cell reconstructed once) with
+ * threads 128 or 256, or march 8 with threads 128 (TMA-staged: x1 rows of 4 x
+ * 31 faces, x2/x3 tiles of 32 x 4 faces; the rows of the primitives must be
+ * whole 16-byte units), PANGU_EINVAL otherwise, e.g. to repeat a configuration
  * the autotuner chose elsewhere. */
 int pangu_set_flux_config(pangu_engine *e, const int32_t cfg[6]);
 
@@ -403,8 +413,12 @@ int pangu_generate(pangu_engine *e, int32_t job, const pangu_problem *problem,
 /* ---- serving: continuous batching over block pools --------------------- */
 /* No counterpart in the reference. A server owns one block pool per job
  * class (parameter set + block shape), each with its containers, dt arrays,
- * stream and captured RK2-cycle graph, allocated against an HBM budget when
- * the class is added. pangu_server_run admits every submitted job once its
+ * stream and captured RK2-cycle graph, charged against an HBM budget (the
+ * containers as allocated, the pool engine by the device memory its creation
+ * takes): when the class is added (pangu_server_add_class), or, for a class
+ * declared with pangu_server_declare_class, when the run admits the first job
+ * that needs it; such a class is released again whenever none of its jobs is
+ * running or has arrived and waits. pangu_server_run admits every submitted job once its
  * arrival time (seconds after the run starts) has passed and its class pool
  * has room (first fit in arrival order), steps the admitted jobs of each
  * class one RK2 cycle per tick of that class (classes tick independently on
@@ -418,14 +432,25 @@ typedef struct pangu_server_stats {
   double zone_cycles;        /* interior cells x cycles, summed over jobs    */
   double zone_cycles_per_s;  /* zone_cycles / wall_s                         */
   double p50_s, p99_s;       /* job latency (completion - arrival)           */
-  uint64_t hbm_bytes;        /* device memory held by the classes' arenas    */
+  uint64_t hbm_bytes;        /* device memory the classes hold after the run */
+  uint64_t hbm_peak_bytes;   /* the most they held at once during the run    */
+  int64_t memory_waits;      /* jobs that waited because their class's
+                                memory did not fit in the budget yet          */
 } pangu_server_stats;
 int pangu_server_create(uint64_t hbm_budget_bytes, pangu_server **out);
 int pangu_server_destroy(pangu_server *s);
-/* PANGU_ENOMEM when the class's arena does not fit in the remaining budget. */
+/* PANGU_ENOMEM when the class's memory does not fit in the remaining budget. */
 int pangu_server_add_class(pangu_server *s, const pangu_params *params,
                            const pangu_mesh *block, int32_t capacity_blocks,
                            int32_t max_jobs, double dt_factor, int32_t *class_out);
+/* A class whose memory is charged only when pangu_server_run admits its first
+ * job, and released while none of its jobs runs or waits: jobs of classes
+ * that do not fit in the budget together take turns. pangu_server_run returns
+ * PANGU_ENOMEM if an arrived job's class cannot fit even with nothing else
+ * running. */
+int pangu_server_declare_class(pangu_server *s, const pangu_params *params,
+                               const pangu_mesh *block, int32_t capacity_blocks,
+                               int32_t max_jobs, double dt_factor, int32_t *class_out);
 /* prim_host: the job's initial primitives, FP64 [block][var][k][j][i] over
  * every cell of each block (ghosts are filled at admission). Copied. */
 int pangu_server_submit(pangu_server *s, int32_t cls, const pangu_mesh *mesh,

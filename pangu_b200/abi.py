@@ -97,7 +97,8 @@ class ServerStats(C.Structure):
         ("jobs", C.c_int64), ("ticks", C.c_int64),
         ("wall_s", C.c_double), ("zone_cycles", C.c_double),
         ("zone_cycles_per_s", C.c_double), ("p50_s", C.c_double), ("p99_s", C.c_double),
-        ("hbm_bytes", C.c_uint64),
+        ("hbm_bytes", C.c_uint64), ("hbm_peak_bytes", C.c_uint64),
+        ("memory_waits", C.c_int64),
     ]
 
 

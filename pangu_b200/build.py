@@ -43,6 +43,18 @@ def sources():
     return out
 
 
+def source_hash() -> str:
+    """Fingerprint of the engine's sources (csrc/ and the C ABI header): the
+    build that a profile summary was captured on carries it, so measurements
+    of other sources are never reported against this build."""
+    import hashlib
+    h = hashlib.sha256()
+    for src in sorted(sources()):
+        with open(src, "rb") as f:
+            h.update(os.path.basename(src).encode() + b"\0" + f.read())
+    return h.hexdigest()[:16]
+
+
 def up_to_date() -> bool:
     if not os.path.exists(LIB):
         return False

@@ -47,6 +47,7 @@ int run_halo_unpack(pangu_engine *e, const pangu_pack *md, const double *buf, cu
 int run_job_start(pangu_engine *e, int job, const pangu_pack *base, const pangu_pack *one,
                   cudaStream_t s);
 int run_autotune(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
+bool flux_tma_ok(const pangu_engine *e);
 int run_generate(pangu_engine *e, int job, const pangu_problem &pb, const pangu_pack *base,
                  cudaStream_t s);
 }  // namespace pgkmx
@@ -94,6 +95,7 @@ int pangu_engine_destroy(pangu_engine *e) {
   cudaFree(e->d_fail_vals);
   cudaFree(e->d_dtmin);
   cudaFree(e->d_dt_ticket);
+  cudaFree(e->d_err);
   cudaFree(e->d_hsend);
   cudaFree(e->d_hrecv);
   delete e;
@@ -185,6 +187,7 @@ int pool_init(pangu_engine *e, int capacity, int max_jobs) {
   rc |= dalloc(&e->d_fail_vals, (size_t)e->fail_cap * d.NF);
   rc |= dalloc(&e->d_dtmin, 3 * (size_t)capacity);
   rc |= dalloc(&e->d_dt_ticket, 1);
+  rc |= dalloc(&e->d_err, 1);
   rc |= dalloc(&e->d_tmp_slots, capacity);
   rc |= dalloc(&e->d_genred, 3);
   // every ghost cell of a slot has at most one exchange source
@@ -209,6 +212,7 @@ int pool_init(pangu_engine *e, int capacity, int max_jobs) {
   ok &= cudaMemset(e->d_slot_job, 0, (size_t)capacity * sizeof(int)) == cudaSuccess;
   ok &= cudaMemset(e->d_bcf, 0xff, 6 * (size_t)capacity) == cudaSuccess;  // -1: no BC
   ok &= cudaMemset(e->d_dt_ticket, 0, sizeof(unsigned int)) == cudaSuccess;
+  ok &= cudaMemset(e->d_err, 0, sizeof(int)) == cudaSuccess;
   k_dt_init<<<grid_for(3 * capacity), kThreads>>>(3 * capacity, e->d_dtmin);
   ok &= cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(0) == cudaSuccess;
   if (!ok) return PANGU_ECUDA;
@@ -594,10 +598,13 @@ int pangu_flux_config(const pangu_engine *e, int32_t out[7]) {
 
 int pangu_set_flux_config(pangu_engine *e, const int32_t cfg[6]) {
   if (!e || !cfg) return PANGU_EINVAL;
+  const bool tma = RUN(flux_tma_ok, e);
   for (int d = 0; d < 3; ++d) {
     const int m = cfg[2 * d], t = cfg[2 * d + 1];
-    const bool march_ok = d == 0 ? m == 1 : (m == 0 || m == 1 || m == 2 || m == 4);
-    const bool threads_ok = m == 0 ? (t == 128 || t == 256) : (t == 64 || t == 128);
+    const bool march_ok = d == 0 ? (m == 1 || (m == kMarchTma && tma))
+                                 : (m == 0 || m == 1 || m == 2 || m == 4 || (m == kMarchTma && tma));
+    const bool threads_ok = m == 0 ? (t == 128 || t == 256)
+                                   : (m == kMarchTma ? t == 128 : (t == 64 || t == 128));
     if (!march_ok || !threads_ok) return PANGU_EINVAL;
   }
   for (int d = 0; d < 3; ++d) {
@@ -827,6 +834,15 @@ int pangu_counters(pangu_engine *e, uint64_t out[PANGU_NCOUNTERS]) {
 }
 
 long long pangu_launches(const pangu_engine *e) { return e ? e->launches : PANGU_EINVAL; }
+
+int pangu_device_error(const pangu_engine *e, int32_t *flag_out) {
+  if (!e || !flag_out) return PANGU_EINVAL;
+  int v = 0;
+  if (cudaMemcpy(&v, e->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return PANGU_ECUDA;
+  *flag_out = v;
+  return PANGU_OK;
+}
 
 int pangu_reset_counters(pangu_engine *e, void *stream) {
   if (!e) return PANGU_EINVAL;

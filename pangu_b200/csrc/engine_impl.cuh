@@ -67,6 +67,11 @@ struct Dims {
   const float *f1tab32, *f2tab32;
 };
 
+// Tile shape code of the flux kernels whose primitives are staged into
+// shared memory by TMA (x1 rows; x2/x3 tiles of 32 x 4 faces); the other
+// codes are march depths 1, 2, 4 and 0 for tiles loaded by the threads.
+constexpr int kMarchTma = 8;
+
 // A job: one mesh of equal meshblocks, placed in pool slots.
 struct PoolJob {
   bool live = false;
@@ -107,6 +112,7 @@ struct pangu_engine {
   long long *d_fix_list = nullptr;
   double *d_fail_vals = nullptr;
   long long fail_cap = 0;
+  int *d_err = nullptr;  // set by a kernel whose bounded wait gave up (0 otherwise)
   unsigned long long *d_dtmin = nullptr;  // [capacity][3]
   unsigned int *d_dt_ticket = nullptr;    // CTAs done in the current dt reduction
   long long launches = 0;  // kernels launched through this handle

@@ -6,6 +6,8 @@
 #error "define PGK_NS before including kernels.cuh"
 #endif
 
+#include <cuda.h>  // CUtensorMap (types only; the encoder comes from the runtime)
+#include <cudaTypedefs.h>
 #include <nvtx3/nvToolsExt.h>
 
 namespace PGK_NS {
@@ -1079,6 +1081,237 @@ __global__ void __launch_bounds__(32 * TF, TF == 4 ? flux_blocks(MT) : 2) k_flux
   flux_tile_body<MT, DIR, TF, OPT>(d, p, k0, k1, j0, j1, i0, i1, P, F, alfven);
 }
 
+// ---------------------------------------------------------------------------
+// Flux kernels whose primitives are staged into shared memory by TMA: one
+// cp.async.bulk.tensor load per CTA brings every component of the cells the
+// CTA's stencils reach from this GPU's memory, completing on an mbarrier; the
+// threads then reconstruct from shared memory (recon_cell reads the stencil
+// there) and evaluate their faces with face_flux / face_flux_split, so the
+// results are those of the other flux kernels bit for bit. No multicast: each
+// load reads this GPU's own memory and serves one CTA.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *tm, int c0, int c1,
+                                            int c2, int c3, unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<unsigned long long>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(c3),
+      "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Elements per 16 bytes: a copy's first column is rounded down to a multiple.
+constexpr int kTmaAlign = 16 / (int)sizeof(PT);
+// Bound on the mbarrier wait (polls of try_wait, each of which suspends for
+// a while itself): far beyond any copy's completion; past it the kernel
+// records an error and returns instead of waiting on.
+constexpr long long kTmaWaitPolls = 1ll << 26;
+
+// Waits for the CTA's copy; false (after recording the error) if the bound
+// ran out.
+__device__ __forceinline__ bool tma_wait(unsigned long long *bar, int *err) {
+  long long polls = 0;
+  while (!mbar_try_wait(bar, 0))
+    if (++polls == kTmaWaitPolls) {
+      if (threadIdx.x == 0) atomicExch(err, 1);
+      return false;
+    }
+  return true;
+}
+
+// x2 / x3 faces: tiles of 32 x TF faces. The copy holds the tile's 32 columns
+// (plus the few that align its start) and the TF + 5 cells along the face
+// direction that the TF faces' stencils reach; each thread reconstructs the
+// two cells of its face.
+constexpr int kTmaCols = 32 + kTmaAlign;
+
+template <int TF>
+inline size_t tma_tile_smem(int nf) {
+  // the staged primitives, whose space then holds the split faces' states
+  const size_t staged = (size_t)nf * (TF + 5) * kTmaCols * sizeof(PT);
+  const size_t split = split_faces(MKS) ? 3 * (size_t)TF * NPRIM * 32 * sizeof(double) : 0;
+  return std::max(staged, split);
+}
+
+template <int MT, int DIR, int TF, int OPT>
+__global__ void __launch_bounds__(32 * TF, flux_blocks(MT))
+    k_flux_tile_tma(const __grid_constant__ CUtensorMap tm, Dims d, pangu_params p, int k0,
+                    int k1, int j0, int j1, int i0, int i1, double *F, double *alfven,
+                    int *err) {
+  extern __shared__ __align__(128) unsigned char dsm[];
+  __shared__ __align__(8) unsigned long long bar;
+  pdl_grid_wait();
+  const int m0 = DIR == 2 ? j0 : k0, m1 = DIR == 2 ? j1 : k1;
+  const int a0 = DIR == 2 ? k0 : j0, a1 = DIR == 2 ? k1 : j1;
+  const int ni = i1 - i0 + 1, na = a1 - a0 + 1, nm = m1 - m0 + 1;
+  const int nti = (ni + 31) / 32, ntm = (nm + TF - 1) / TF;
+  long long ti, tmi, al;
+  long long r = div_fast(blockIdx.x, nti, ti);
+  r = div_fast(r, ntm, tmi);
+  const long long bb = div_fast(r, na, al);
+  if (bb >= d.NB) return;  // whole CTAs exit together
+  const int b = slot_of(d, (int)bb);
+  const int a = a0 + (int)al;
+  const int mt0 = m0 + (int)tmi * TF;
+  const int lane = threadIdx.x & 31, row = threadIdx.x >> 5;
+  const int x0 = i0 + (int)ti * 32;
+  const int xs = x0 & ~(kTmaAlign - 1);  // 16-byte aligned first column
+  const int off = x0 - xs;
+  constexpr int R = TF + 5;  // cells mt0 - 3 .. mt0 + TF + 1
+  PT *raw = reinterpret_cast<PT *>(dsm);
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_expect_tx(&bar, (unsigned)(d.NF * R * kTmaCols * sizeof(PT)));
+    if (DIR == 2)
+      tma_load_4d(raw, &tm, xs, mt0 - 3, a, b * d.NF, &bar);
+    else
+      tma_load_4d(raw, &tm, xs, a, mt0 - 3, b * d.NF, &bar);
+  }
+  if (!tma_wait(&bar, err)) return;
+  const int i = x0 + lane, f = mt0 + row;
+  const bool active = i <= i1 && f <= m1;
+  const bool use_mc = PGK_FLUX_MC(p);
+  FT PL[NPRIM], PR[NPRIM];
+#pragma unroll
+  for (int s = 0; s < NPRIM; ++s) {
+    PL[s] = 0;
+    PR[s] = 0;
+    if (active && d.pidx[s] >= 0) {
+      // cell f - 1 sits at tile row row + 2, cell f at row + 3
+      const PT *q = raw + ((size_t)d.pidx[s] * R + row + 2) * kTmaCols + lane + off;
+      FT lo, up;
+      recon_cell(use_mc, q, kTmaCols, PL[s], lo);
+      recon_cell(use_mc, q + kTmaCols, kTmaCols, up, PR[s]);
+    }
+  }
+  __syncthreads();  // the staged tile is read; its space is reused below
+  if (!active) return;
+  const int kk = DIR == 2 ? a : f, jj = DIR == 2 ? f : a;
+#if PGK_SPLIT_FACES
+  if (split_faces(MT)) {
+    double *sl = reinterpret_cast<double *>(dsm);
+    double *pl = sl + ((size_t)0 * TF + row) * NPRIM * 32 + lane;
+    double *pr = sl + ((size_t)1 * TF + row) * NPRIM * 32 + lane;
+    double *ul = sl + ((size_t)2 * TF + row) * NPRIM * 32 + lane;
+#pragma unroll
+    for (int s = 0; s < NPRIM; ++s) {
+      pl[s * 32] = PL[s];
+      pr[s * 32] = PR[s];
+    }
+    face_flux_split<MT, DIR, OPT>(d, p, b, kk, jj, i, pl, pr, ul, 32, F, alfven);
+    return;
+  }
+#endif
+  face_flux<MT, DIR, OPT>(d, p, b, kk, jj, i, PL, PR, F, alfven);
+}
+
+// x1 faces: a CTA of 4 warps takes 4 consecutive rows (j) of one k and one
+// segment of 31 faces; the copy holds the segment's 32 cells and 2 more on
+// each side (from a 16-byte aligned first column) of every component and row.
+// Lane l reconstructs cell i0 - 1 + 31 seg + l and hands its upper-face value
+// to lane l + 1, as k_flux_x1 does from global memory.
+constexpr int kTmaRowsX1 = 4;
+constexpr int kTmaColsX1 = (kFacesPerWarp + 5 + kTmaAlign - 1 + kTmaAlign - 1) / kTmaAlign *
+                           kTmaAlign;
+
+inline size_t tma_x1_smem(int nf) {
+  const size_t staged = (size_t)nf * kTmaRowsX1 * kTmaColsX1 * sizeof(PT);
+  const size_t split = split_faces(MKS) ? 3 * (size_t)NPRIM * 32 * kTmaRowsX1 * sizeof(double)
+                                        : 0;
+  return std::max(staged, split);
+}
+
+template <int MT, int OPT>
+__global__ void __launch_bounds__(32 * kTmaRowsX1, flux_blocks(MT))
+    k_flux_x1_tma(const __grid_constant__ CUtensorMap tm, Dims d, pangu_params p, int k0, int k1,
+                  int j0, int j1, int i0, int i1, double *F, double *alfven, int *err) {
+  extern __shared__ __align__(128) unsigned char dsm[];
+  __shared__ __align__(8) unsigned long long bar;
+  pdl_grid_wait();
+  const int nf = i1 - i0 + 1;
+  const int nseg = (nf + kFacesPerWarp - 1) / kFacesPerWarp;
+  const int nj = j1 - j0 + 1, njc = (nj + kTmaRowsX1 - 1) / kTmaRowsX1;
+  long long segl, jcl, kl;
+  long long r = div_fast(blockIdx.x, nseg, segl);
+  r = div_fast(r, njc, jcl);
+  const long long bb = div_fast(r, k1 - k0 + 1, kl);
+  if (bb >= d.NB) return;  // whole CTAs exit together
+  const int b = slot_of(d, (int)bb);
+  const int k = k0 + (int)kl, seg = (int)segl;
+  const int jr0 = j0 + (int)jcl * kTmaRowsX1;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int c0 = i0 - 1 + seg * kFacesPerWarp;  // the segment's first cell
+  const int xs = (c0 - 2) & ~(kTmaAlign - 1);
+  const int off = c0 - xs;  // column of cell c0 in the staged rows
+  PT *raw = reinterpret_cast<PT *>(dsm);
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_expect_tx(&bar, (unsigned)(d.NF * kTmaRowsX1 * kTmaColsX1 * sizeof(PT)));
+    tma_load_4d(raw, &tm, xs, jr0, k, b * d.NF, &bar);
+  }
+  if (!tma_wait(&bar, err)) return;
+  const int j = jr0 + w, c = c0 + lane;
+  const bool active = c <= i1 && j <= j1;  // cell c is needed by face c (and c + 1)
+  const bool use_mc = PGK_FLUX_MC(p);
+  FT up[NPRIM], lo[NPRIM];
+#pragma unroll
+  for (int s = 0; s < NPRIM; ++s) {
+    up[s] = 0;
+    lo[s] = 0;
+    if (d.pidx[s] >= 0 && active)
+      recon_cell(use_mc, raw + ((size_t)d.pidx[s] * kTmaRowsX1 + w) * kTmaColsX1 + off + lane, 1,
+                 up[s], lo[s]);
+  }
+#if PGK_SPLIT_FACES
+  if (split_faces(MT)) {
+    __syncthreads();  // the staged rows are read; their space is reused below
+    // [3][NPRIM][blockDim.x] as in k_flux_x1
+    double *fsm = reinterpret_cast<double *>(dsm);
+    const int ss = blockDim.x, t = threadIdx.x;
+#pragma unroll
+    for (int s = 0; s < NPRIM; ++s) {
+      fsm[s * ss + t] = up[s];
+      fsm[(NPRIM + s) * ss + t] = lo[s];
+    }
+    __syncwarp();
+    if (lane == 0 || !active) return;
+    face_flux_split<MT, 1, OPT>(d, p, b, k, j, c, fsm + t - 1, fsm + NPRIM * ss + t,
+                                fsm + 2 * NPRIM * ss + t, ss, F, alfven);
+    return;
+  }
+#endif
+  FT PL[NPRIM];
+#pragma unroll
+  for (int s = 0; s < NPRIM; ++s) PL[s] = __shfl_up_sync(0xffffffffu, up[s], 1);
+  if (lane == 0 || !active) return;
+  face_flux<MT, 1, OPT>(d, p, b, k, j, c, PL, lo, F, alfven);
+}
+
 template <int MT, int MARCH, int OPT>
 __global__ void __launch_bounds__(kFluxThreads, flux_blocks(MT)) k_flux_march2(Dims d, pangu_params p, int k0, int k1,
                                                           int j0, int j1, int i0, int i1,
@@ -1666,6 +1899,9 @@ __global__ void __launch_bounds__(kThreads) k_recovery_retry(Dims d, pangu_param
                                                              int *nfix, long long *fix) {
   pdl_grid_wait();
   const int n = *nretry;
+  // A few cells per stage run the isentropic schemes here, one thread each:
+  // their chains of pow calls would wait on L2 for every table load.
+  if ((long long)blockIdx.x * blockDim.x < n) pgm::prefetch_tables_l1();
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x) {
     const long long fc = retry[t];
@@ -2261,6 +2497,51 @@ int run_calc_cons(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
 
 // Launches the flux kernel of one direction with a given march depth
 // (x2/x3) and CTA size.
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library links the runtime only).
+inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }();
+  return fn;
+}
+
+// TMA-staged flux kernels need rows of whole 16-byte units (N1 * sizeof(PT)
+// a multiple of 16) and the tensor-map encoder.
+inline bool tma_ok(const pangu_engine *e) {
+  return ((size_t)e->d.N1 * sizeof(PT)) % 16 == 0 && e->d.NF <= 256 &&
+         tensor_map_encoder() != nullptr;
+}
+
+// Tensor map of md's primitives as a 4D array {i, j, k, slot * NF + var}
+// (i fastest) with the box of the TMA-staged flux kernels of direction dir:
+// x1, kTmaColsX1 x kTmaRowsX1 rows (j); x2 / x3, kTmaCols x (4 + 5) cells
+// running along j / k; every component.
+inline bool tma_tile_map(const pangu_engine *e, const pangu_pack *md, int dir, CUtensorMap *tm) {
+  const Dims &d = e->d;
+  auto enc = tensor_map_encoder();
+  if (!enc) return false;
+  const cuuint64_t dims[4] = {(cuuint64_t)d.N1, (cuuint64_t)d.N2, (cuuint64_t)d.N3,
+                              (cuuint64_t)e->capacity * d.NF};
+  const cuuint64_t strides[3] = {(cuuint64_t)d.N1 * sizeof(PT),
+                                 (cuuint64_t)d.N1 * d.N2 * sizeof(PT),
+                                 (cuuint64_t)d.N1 * d.N2 * d.N3 * sizeof(PT)};
+  const cuuint32_t box[4] = {(cuuint32_t)(dir == 1 ? kTmaColsX1 : kTmaCols),
+                             dir == 1 ? (cuuint32_t)kTmaRowsX1 : (dir == 2 ? 9u : 1u),
+                             dir == 3 ? 9u : 1u, (cuuint32_t)d.NF};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  return enc(tm, sizeof(PT) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+             4, (void *)prim_of(md), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <int MT, int OPT>
 void launch_flux_dir(const pangu_engine *e, const pangu_pack *md, int dir, int march, int threads,
                      cudaStream_t s) {
@@ -2276,6 +2557,17 @@ void launch_flux_dir(const pangu_engine *e, const pangu_pack *md, int dir, int m
   }
   double *F = dir == 1 ? md->flux1 : (dir == 2 ? md->flux2 : md->flux3);
   const PT *P = prim_of(md);
+  if (dir == 1 && march == kMarchTma) {
+    CUtensorMap tm;
+    if (!tma_tile_map(e, md, 1, &tm)) return;  // pangu_set_flux_config checked tma_ok
+    const int nseg = (i1 - i0 + 1 + kFacesPerWarp - 1) / kFacesPerWarp;
+    const long long nt = (long long)d.NB * (k1 - k0 + 1) *
+                         ((j1 - j0 + 1 + kTmaRowsX1 - 1) / kTmaRowsX1) * nseg;
+    launch_pdl_smem(k_flux_x1_tma<MT, OPT>, dim3((unsigned)nt), dim3(32 * kTmaRowsX1),
+                    tma_x1_smem(d.NF), s, tm, d, e->p, k0, k1, j0, j1, i0, i1, F, md->alfven,
+                    e->d_err);
+    return;
+  }
   if (dir == 1) {
     const int nseg = (i1 - i0 + 1 + kFacesPerWarp - 1) / kFacesPerWarp;
     const long long warps = (long long)d.NB * (k1 - k0 + 1) * (j1 - j0 + 1) * nseg;
@@ -2286,6 +2578,20 @@ void launch_flux_dir(const pangu_engine *e, const pangu_pack *md, int dir, int m
   }
   const int m = dir == 2 ? (j1 - j0 + 1) : (k1 - k0 + 1);
   const int na = dir == 2 ? (k1 - k0 + 1) : (j1 - j0 + 1);
+  if (march == kMarchTma) {  // TMA-staged tiles of 32 x 4 faces
+    CUtensorMap tm;
+    if (!tma_tile_map(e, md, dir, &tm)) return;  // pangu_set_flux_config checked tma_ok
+    const long long nt = (long long)d.NB * na * ((m + 3) / 4) * ((i1 - i0 + 1 + 31) / 32);
+    if (dir == 2)
+      launch_pdl_smem(k_flux_tile_tma<MT, 2, 4, OPT>, dim3((unsigned)nt), dim3(128),
+                      tma_tile_smem<4>(d.NF), s, tm, d, e->p, k0, k1, j0, j1, i0, i1, F,
+                      md->alfven, e->d_err);
+    else
+      launch_pdl_smem(k_flux_tile_tma<MT, 3, 4, OPT>, dim3((unsigned)nt), dim3(128),
+                      tma_tile_smem<4>(d.NF), s, tm, d, e->p, k0, k1, j0, j1, i0, i1, F,
+                      md->alfven, e->d_err);
+    return;
+  }
   if (march == 0) {  // tiles of 32 x (threads / 32) faces
     const long long nt = (long long)d.NB * na * ((m + threads / 32 - 1) / (threads / 32)) *
                          ((i1 - i0 + 1 + 31) / 32);
@@ -2359,6 +2665,8 @@ int run_fluxes(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
 // pack's own data (best of three launches after one untimed launch, CUDA
 // events on stream s) and keeps the fastest in e->tune. The candidates
 // compute every face identically, so the choice never changes results.
+bool flux_tma_ok(const pangu_engine *e) { return tma_ok(e); }
+
 int run_autotune(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
   if (e->d.NB == 0) return PANGU_OK;
   cudaEvent_t ev[2];
@@ -2369,21 +2677,24 @@ int run_autotune(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
   }
   int rc = PANGU_OK;
   // candidates {march, CTA size}; march 0 is the tiled kernel (tiles of 32 x
-  // CTA size / 32 faces)
-  const int cand[8][2] = {{1, 64}, {1, 128}, {2, 64}, {2, 128}, {4, 64}, {4, 128}, {0, 128},
-                          {0, 256}};
+  // CTA size / 32 faces), kMarchTma its TMA-staged form (where the rows allow)
+  const int cand[9][2] = {{1, 64}, {1, 128}, {2, 64}, {2, 128}, {4, 64}, {4, 128}, {0, 128},
+                          {0, 256}, {kMarchTma, 128}};
+  // x1: march 1 with CTAs of 64 or 128 threads, or the TMA-staged rows
+  const int x1cand[3][2] = {{1, 64}, {1, 128}, {kMarchTma, 128}};
   // Each candidate's time is the minimum over two interleaved rounds of five
   // launches after one warm-up launch, so that clock ramps and cache states
   // do not favour whichever candidate runs first. A candidate of x2 (x3) is
   // timed behind the chosen x1 (and x2) launches, as it runs in a stage, so
   // that it meets the caches those leave.
   for (int dir = 1; dir <= e->d.ndim && !rc; ++dir) {
-    const int nc = dir == 1 ? 2 : 8;
-    float t[8];
+    const int nc = dir == 1 ? (tma_ok(e) ? 3 : 2) : (tma_ok(e) ? 9 : 8);
+    float t[9];
     for (int ci = 0; ci < nc; ++ci) t[ci] = 1e30f;
     for (int round = 0; round < 2 && !rc; ++round)
       for (int ci = 0; ci < nc && !rc; ++ci) {
-        const int march = cand[ci][0], threads = cand[ci][1];
+        const int march = dir == 1 ? x1cand[ci][0] : cand[ci][0];
+        const int threads = dir == 1 ? x1cand[ci][1] : cand[ci][1];
         for (int rep = 0; rep < 6 && !rc; ++rep) {
           if (cudaEventRecord(ev[0], s) != cudaSuccess) rc = PANGU_ECUDA;
           for (int lower = 1; lower < dir && !rc; ++lower)
@@ -2401,8 +2712,8 @@ int run_autotune(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
     for (int ci = 0; ci < nc && !rc; ++ci)
       if (t[ci] < best) {
         best = t[ci];
-        e->tune.march[dir - 1] = cand[ci][0];
-        e->tune.threads[dir - 1] = cand[ci][1];
+        e->tune.march[dir - 1] = dir == 1 ? x1cand[ci][0] : cand[ci][0];
+        e->tune.threads[dir - 1] = dir == 1 ? x1cand[ci][1] : cand[ci][1];
       }
   }
   if (!rc) e->tune.tuned = 1;

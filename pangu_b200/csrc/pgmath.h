@@ -198,6 +198,23 @@ PGM_FN double exp_tab(int i) {
 #endif
 }
 
+#if defined(__CUDACC__)
+// Brings both tables into this SM's L1 (one 128-byte line per lane and
+// step). For kernels where a few threads run long chains of pow calls, each
+// of whose table loads would otherwise wait on L2 in turn.
+__device__ __forceinline__ void prefetch_tables_l1() {
+#if defined(__CUDA_ARCH__)
+  const int lane = threadIdx.x & 31;
+  const char *lt = reinterpret_cast<const char *>(kLogTabD);
+  const char *et = reinterpret_cast<const char *>(kExpTabD);
+  for (int o = lane * 128; o < (int)sizeof(kLogTabD); o += 32 * 128)
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(lt + o));
+  for (int o = lane * 128; o < (int)sizeof(kExpTabD); o += 32 * 128)
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(et + o));
+#endif
+}
+#endif
+
 // ln x as double-double for finite x > 0, relative error below 2^-80.
 PGM_FN dd log_fast(double x) {
   int e;

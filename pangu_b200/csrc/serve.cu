@@ -2,8 +2,13 @@
 //
 // A server holds one block pool (pangu_pool_create) per job class -- one
 // parameter set and block shape -- with its containers, dt arrays, CUDA
-// stream and captured RK2-cycle graph, all allocated at class creation
-// against the server's HBM budget. Submitted jobs wait until their arrival
+// stream and captured RK2-cycle graph, charged against the server's HBM
+// budget: at class creation (pangu_server_add_class), or, for a class
+// declared with pangu_server_declare_class, when the first job that needs it
+// is admitted -- a job of a class whose memory does not fit in what is left of
+// the budget waits until retiring jobs and released classes free enough --
+// and released again when none of the class's jobs is running or waiting.
+// Submitted jobs wait until their arrival
 // time; a job is admitted as soon as its class pool has a free job id and
 // enough free block slots (first fit in arrival order) and then runs one RK2
 // cycle per tick of its class together with every other admitted job of the
@@ -46,6 +51,10 @@ struct SClass {
   cudaGraphExec_t graph = nullptr;
   bool dirty = true, inflight = false, tuned = false;
   int running = 0;
+  bool lazy = false;       // allocated at admission, released when idle
+  bool allocated = false;  // engine, arena, stream and event exist
+  uint64_t bytes = 0;      // device memory charged to the budget while allocated
+  uint64_t need = 0;       // bytes an allocation of the class took (0: unknown)
 };
 
 struct SJob {
@@ -61,6 +70,7 @@ struct SJob {
   int job = -1;
   std::vector<int32_t> slots;
   double t_admit = 0, t_done = 0;
+  bool waited_for_memory = false;  // its class's memory did not fit at some point
   uint64_t counters[PANGU_NCOUNTERS] = {};
 };
 
@@ -71,7 +81,7 @@ double now_s(std::chrono::steady_clock::time_point t0) {
 }  // namespace
 
 struct pangu_server {
-  uint64_t budget = 0, used = 0;
+  uint64_t budget = 0, used = 0, peak = 0;
   std::vector<SClass> classes;
   std::vector<SJob> jobs;
   pangu_server_stats stats{};
@@ -80,23 +90,117 @@ struct pangu_server {
 namespace {
 
 template <class T>
-int salloc(pangu_server *s, Arena &a, T **p, size_t n) {
+int salloc(pangu_server *s, SClass &c, T **p, size_t n) {
   const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
   if (s->used + bytes > s->budget) return PANGU_ENOMEM;
   if (cudaMalloc((void **)p, bytes) != cudaSuccess) return PANGU_ENOMEM;
-  a.allocs.push_back(*p);
+  c.a.allocs.push_back(*p);
   s->used += bytes;
+  c.bytes += bytes;
   if (cudaMemset(*p, 0, bytes) != cudaSuccess) return PANGU_ECUDA;
   return PANGU_OK;
 }
 
-void free_class(SClass &c) {
+// Frees a class's device resources and returns its bytes to the budget; the
+// class keeps its parameters and can be allocated again.
+void release(pangu_server *s, SClass &c) {
   if (c.graph) cudaGraphExecDestroy(c.graph);
   if (c.e) pangu_engine_destroy(c.e);
   for (void *p : c.a.allocs) cudaFree(p);
   if (c.tick_done) cudaEventDestroy(c.tick_done);
   if (c.stream) cudaStreamDestroy(c.stream);
-  c = SClass{};
+  s->used -= std::min(s->used, c.bytes);
+  c.graph = nullptr;
+  c.e = nullptr;
+  c.a = Arena{};
+  c.tick_done = nullptr;
+  c.stream = nullptr;
+  c.bytes = 0;
+  c.allocated = false;
+  c.dirty = true;
+  c.inflight = false;
+  c.tuned = false;
+  c.running = 0;
+}
+
+// Creates a class's pool engine, containers, dt arrays, stream and event,
+// charging the budget: the containers as allocated, the engine by the device
+// memory its creation took (tables, block table, exchange map, lists).
+int allocate(pangu_server *s, SClass &c) {
+  size_t free0 = 0, free1 = 0, total = 0;
+  if (cudaMemGetInfo(&free0, &total) != cudaSuccess) return PANGU_ECUDA;
+  int rc = pangu_pool_create(&c.p, &c.block, c.capacity, c.max_jobs, &c.e);
+  if (rc) return rc;
+  if (cudaMemGetInfo(&free1, &total) != cudaSuccess) return PANGU_ECUDA;
+  const uint64_t eng = free0 > free1 ? free0 - free1 : 0;
+  if (s->used + eng > s->budget) {
+    pangu_engine_destroy(c.e);
+    c.e = nullptr;
+    return PANGU_ENOMEM;
+  }
+  s->used += eng;
+  c.bytes = eng;
+  const int act[3] = {c.block.nx1 > 1, c.block.nx2 > 1, c.block.nx3 > 1};
+  const size_t nv = (size_t)c.capacity * c.nf * c.ncell;
+  const size_t na = (size_t)c.capacity * 3 * c.ncell;
+  Arena &a = c.a;
+  double *alfven = nullptr, *efield = nullptr, *flag = nullptr;
+  rc = salloc(s, c, &alfven, na);
+  if (!rc) rc = salloc(s, c, &efield, na);
+  if (!rc) rc = salloc(s, c, &flag, (size_t)c.capacity * c.ncell);
+  pangu_pack *packs[2] = {&a.base, &a.one};
+  for (pangu_pack *pk : packs) {
+    if (rc) break;
+    if (c.prim_bytes == 4) {
+      float *pf = nullptr;
+      rc = salloc(s, c, &pf, nv);
+      pk->prim = reinterpret_cast<double *>(pf);
+    } else {
+      rc = salloc(s, c, &pk->prim, nv);
+    }
+    if (!rc) rc = salloc(s, c, &pk->cons, nv);
+    if (!rc) rc = salloc(s, c, &pk->flux1, nv);
+    if (!rc && act[1]) rc = salloc(s, c, &pk->flux2, nv);
+    if (!rc && act[2]) rc = salloc(s, c, &pk->flux3, nv);
+    pk->alfven = alfven;
+    pk->efield = efield;
+    pk->flag = flag;
+  }
+  if (!rc) rc = salloc(s, c, &a.dt, c.max_jobs);
+  if (!rc) rc = salloc(s, c, &a.dt_est, c.max_jobs);
+  if (!rc && cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess)
+    rc = PANGU_ECUDA;
+  if (!rc && cudaEventCreateWithFlags(&c.tick_done, cudaEventDisableTiming) != cudaSuccess)
+    rc = PANGU_ECUDA;
+  if (rc) {
+    release(s, c);
+    return rc;
+  }
+  c.allocated = true;
+  c.need = c.bytes;
+  s->peak = std::max(s->peak, s->used);
+  return PANGU_OK;
+}
+
+int init_class(SClass &c, const pangu_params *params, const pangu_mesh *block,
+               int32_t capacity_blocks, int32_t max_jobs, double dt_factor) {
+  c.p = *params;
+  c.block = *block;
+  c.capacity = capacity_blocks;
+  c.max_jobs = max_jobs;
+  c.dt_factor = dt_factor;
+  c.nf = pangu_num_fields(params);
+  if (c.nf <= 0) return PANGU_EINVAL;
+  c.prim_bytes = params->precision == PANGU_PRECISION_MIXED ? 4 : 8;
+  const int act[3] = {block->nx1 > 1, block->nx2 > 1, block->nx3 > 1};
+  const int nx[3] = {block->nx1, block->nx2, block->nx3};
+  c.ncell = 1;
+  c.interior = 1;
+  for (int d = 0; d < 3; ++d) {
+    c.ncell *= nx[d] + 2 * block->ng * act[d];
+    c.interior *= nx[d];
+  }
+  return PANGU_OK;
 }
 
 // Captures one RK2 cycle of the class pool (both stages and the dt policy).
@@ -223,7 +327,7 @@ int pangu_server_destroy(pangu_server *s) {
   if (!s) return PANGU_EINVAL;
   for (SClass &c : s->classes)
     if (c.stream) cudaStreamSynchronize(c.stream);
-  for (SClass &c : s->classes) free_class(c);
+  for (SClass &c : s->classes) release(s, c);
   delete s;
   return PANGU_OK;
 }
@@ -234,59 +338,23 @@ int pangu_server_add_class(pangu_server *s, const pangu_params *params, const pa
   if (!s || !params || !block || !class_out || capacity_blocks < 1 || max_jobs < 1)
     return PANGU_EINVAL;
   SClass c;
-  c.p = *params;
-  c.block = *block;
-  c.capacity = capacity_blocks;
-  c.max_jobs = max_jobs;
-  c.dt_factor = dt_factor;
-  c.nf = pangu_num_fields(params);
-  c.prim_bytes = params->precision == PANGU_PRECISION_MIXED ? 4 : 8;
-  const int act[3] = {block->nx1 > 1, block->nx2 > 1, block->nx3 > 1};
-  const int nx[3] = {block->nx1, block->nx2, block->nx3};
-  c.ncell = 1;
-  c.interior = 1;
-  for (int d = 0; d < 3; ++d) {
-    c.ncell *= nx[d] + 2 * block->ng * act[d];
-    c.interior *= nx[d];
-  }
-  const uint64_t used0 = s->used;
-  int rc = pangu_pool_create(params, block, capacity_blocks, max_jobs, &c.e);
-  const size_t nv = (size_t)capacity_blocks * c.nf * c.ncell;
-  const size_t na = (size_t)capacity_blocks * 3 * c.ncell;
-  Arena &a = c.a;
-  double *alfven = nullptr, *efield = nullptr, *flag = nullptr;
-  if (!rc) rc = salloc(s, a, &alfven, na);
-  if (!rc) rc = salloc(s, a, &efield, na);
-  if (!rc) rc = salloc(s, a, &flag, (size_t)capacity_blocks * c.ncell);
-  pangu_pack *packs[2] = {&a.base, &a.one};
-  for (pangu_pack *pk : packs) {
-    if (rc) break;
-    if (c.prim_bytes == 4) {
-      float *pf = nullptr;
-      rc = salloc(s, a, &pf, nv);
-      pk->prim = reinterpret_cast<double *>(pf);
-    } else {
-      rc = salloc(s, a, &pk->prim, nv);
-    }
-    if (!rc) rc = salloc(s, a, &pk->cons, nv);
-    if (!rc) rc = salloc(s, a, &pk->flux1, nv);
-    if (!rc && act[1]) rc = salloc(s, a, &pk->flux2, nv);
-    if (!rc && act[2]) rc = salloc(s, a, &pk->flux3, nv);
-    pk->alfven = alfven;
-    pk->efield = efield;
-    pk->flag = flag;
-  }
-  if (!rc) rc = salloc(s, a, &a.dt, max_jobs);
-  if (!rc) rc = salloc(s, a, &a.dt_est, max_jobs);
-  if (!rc && cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess)
-    rc = PANGU_ECUDA;
-  if (!rc && cudaEventCreateWithFlags(&c.tick_done, cudaEventDisableTiming) != cudaSuccess)
-    rc = PANGU_ECUDA;
-  if (rc) {
-    free_class(c);
-    s->used = used0;
-    return rc;
-  }
+  int rc = init_class(c, params, block, capacity_blocks, max_jobs, dt_factor);
+  if (!rc) rc = allocate(s, c);
+  if (rc) return rc;
+  *class_out = (int32_t)s->classes.size();
+  s->classes.push_back(c);
+  return PANGU_OK;
+}
+
+int pangu_server_declare_class(pangu_server *s, const pangu_params *params,
+                               const pangu_mesh *block, int32_t capacity_blocks,
+                               int32_t max_jobs, double dt_factor, int32_t *class_out) {
+  if (!s || !params || !block || !class_out || capacity_blocks < 1 || max_jobs < 1)
+    return PANGU_EINVAL;
+  SClass c;
+  const int rc = init_class(c, params, block, capacity_blocks, max_jobs, dt_factor);
+  if (rc) return rc;
+  c.lazy = true;
   *class_out = (int32_t)s->classes.size();
   s->classes.push_back(c);
   return PANGU_OK;
@@ -361,7 +429,7 @@ int pangu_server_run(pangu_server *s) {
   // the cycle is credited to its running jobs, finished jobs are copied out
   // and detached, arrived jobs admitted, and the next cycle launched.
   while (done < s->jobs.size()) {
-    bool busy = false;
+    bool busy = false, starved = false, released = false;
     for (int ci = 0; ci < (int)s->classes.size(); ++ci) {
       SClass &c = s->classes[ci];
       if (c.inflight) {
@@ -393,6 +461,7 @@ int pangu_server_run(pangu_server *s) {
         }
       }
       const double t = now_s(t0);
+      bool waiting = false;
       for (int q : order) {  // first fit in arrival order
         SJob &j = s->jobs[q];
         if (j.cls != ci || j.state != 0) continue;
@@ -403,13 +472,33 @@ int pangu_server_run(pangu_server *s) {
           continue;
         }
         if (j.arrival > t) continue;
+        waiting = true;
+        if (!c.allocated) {
+          // the class's memory is charged at its first admission; a class
+          // that does not fit yet waits for retiring work to free the budget
+          rc = c.need && s->used + c.need > s->budget ? PANGU_ENOMEM : allocate(s, c);
+          if (rc == PANGU_ENOMEM) {
+            j.waited_for_memory = true;
+            starved = true;
+            break;
+          }
+          if (rc) return rc;
+        }
         rc = admit(c, j);
         if (rc == PANGU_EFULL) continue;
         if (rc) return rc;
         j.state = 1;
         j.t_admit = now_s(t0);
       }
-      if (!c.running) continue;
+      if (!c.running) {
+        // an idle lazily allocated class with no arrived job waiting gives its
+        // memory back
+        if (c.lazy && c.allocated && !c.inflight && !waiting) {
+          release(s, c);
+          released = true;
+        }
+        continue;
+      }
       if (!c.tuned) {  // flux tile shapes, tuned once on the class's first jobs
         if ((rc = pangu_autotune(c.e, &c.a.base, c.stream))) return rc;
         c.tuned = true;
@@ -420,6 +509,11 @@ int pangu_server_run(pangu_server *s) {
         return PANGU_ECUDA;
       c.inflight = true;
       busy = true;
+    }
+    if (!busy && starved && !released) {
+      // nothing runs, so nothing will free memory: an arrived job's class does
+      // not fit in the budget even with every idle class released
+      return PANGU_ENOMEM;
     }
     if (!busy && done < s->jobs.size()) {
       // nothing on the device: sleep until the next arrival
@@ -436,6 +530,12 @@ int pangu_server_run(pangu_server *s) {
     }
   }
   st.wall_s = now_s(t0);
+  // lazily allocated classes give their memory back once the run is over
+  for (SClass &c : s->classes)
+    if (c.lazy && c.allocated) {
+      if (cudaStreamSynchronize(c.stream) != cudaSuccess) return PANGU_ECUDA;
+      release(s, c);
+    }
   std::vector<double> lat;
   for (const SJob &j : s->jobs)
     if (j.state == 2) lat.push_back(j.t_done - j.arrival);
@@ -451,8 +551,10 @@ int pangu_server_run(pangu_server *s) {
     st.p99_s = pct(0.99);
   }
   st.jobs = (int64_t)lat.size();
+  for (const SJob &j : s->jobs) st.memory_waits += j.waited_for_memory;
   st.zone_cycles_per_s = st.wall_s > 0 ? st.zone_cycles / st.wall_s : 0;
   st.hbm_bytes = s->used;
+  st.hbm_peak_bytes = s->peak;
   return PANGU_OK;
 }
 

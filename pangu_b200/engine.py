@@ -71,6 +71,7 @@ def lib():
     L.pangu_reset_counters.argtypes = [_P, _P]
     L.pangu_launches.argtypes = [_P]
     L.pangu_launches.restype = C.c_longlong
+    L.pangu_device_error.argtypes = [_P, C.POINTER(C.c_int32)]
     L.pangu_pool_create.argtypes = [C.POINTER(abi.Params), C.POINTER(abi.Mesh), C.c_int32,
                                     C.c_int32, C.POINTER(_P)]
     L.pangu_job_attach.argtypes = [_P, C.POINTER(abi.Mesh), C.c_double, C.c_double,
@@ -90,6 +91,7 @@ def lib():
     L.pangu_server_destroy.argtypes = [_P]
     L.pangu_server_add_class.argtypes = [_P, C.POINTER(abi.Params), C.POINTER(abi.Mesh), C.c_int32,
                                          C.c_int32, C.c_double, C.POINTER(C.c_int32)]
+    L.pangu_server_declare_class.argtypes = L.pangu_server_add_class.argtypes
     L.pangu_server_submit.argtypes = [_P, C.c_int32, C.POINTER(abi.Mesh), C.c_double, C.c_double,
                                       C.c_double, C.c_int64, C.c_double, C.c_void_p,
                                       C.POINTER(C.c_int32)]
@@ -296,6 +298,13 @@ class Engine:
     def launches(self) -> int:
         return int(self.L.pangu_launches(self.h))
 
+    def device_error(self) -> bool:
+        """True if a kernel of this engine gave up a bounded wait (its results
+        are then incomplete)."""
+        out = C.c_int32()
+        _check(self.L.pangu_device_error(self.h, C.byref(out)), "pangu_device_error")
+        return bool(out.value)
+
     def reset_counters(self):
         _check(self.L.pangu_reset_counters(self.h, self.stream()), "pangu_reset_counters")
 
@@ -312,13 +321,13 @@ class Engine:
         out = (C.c_int32 * 7)()
         _check(self.L.pangu_flux_config(self.h, out), "pangu_flux_config")
         v = list(out)
-        return {"x1_threads": v[1], "x2_march": v[2], "x2_threads": v[3],
+        return {"x1_march": v[0], "x1_threads": v[1], "x2_march": v[2], "x2_threads": v[3],
                 "x3_march": v[4], "x3_threads": v[5], "tuned": bool(v[6])}
 
     def set_flux_config(self, x1_threads=128, x2_march=2, x2_threads=128, x3_march=2,
-                        x3_threads=128, **_):
+                        x3_threads=128, x1_march=1, **_):
         """Sets the flux tile shapes (the keys of flux_config())."""
-        cfg = (C.c_int32 * 6)(1, x1_threads, x2_march, x2_threads, x3_march, x3_threads)
+        cfg = (C.c_int32 * 6)(x1_march, x1_threads, x2_march, x2_threads, x3_march, x3_threads)
         _check(self.L.pangu_set_flux_config(self.h, cfg), "pangu_set_flux_config")
 
     # ---- block pool --------------------------------------------------------
@@ -708,16 +717,22 @@ class Server:
         except Exception:
             pass
 
-    def add_class(self, template: ParameterInput, capacity_blocks: int, max_jobs: int) -> int:
+    def add_class(self, template: ParameterInput, capacity_blocks: int, max_jobs: int,
+                  lazy: bool = False) -> int:
+        """A job class (the template's parameters and block shape) with a pool
+        of `capacity_blocks` block slots for up to `max_jobs` jobs. Its device
+        memory is charged against the budget now, or with lazy=True when its
+        first job is admitted (and released again while it has nothing to
+        run)."""
         params = params_struct(process_packages(template))
         params.precision = engine_precision(template)
         block = mesh_struct(template)
         block.nbx1 = block.nbx2 = block.nbx3 = 1
         factor = template.get_or_add_real("parthenon/time", "dt_factor", 2.0)
         out = C.c_int32()
-        _check(self.L.pangu_server_add_class(self.h, C.byref(params), C.byref(block),
-                                             int(capacity_blocks), int(max_jobs), factor,
-                                             C.byref(out)), "pangu_server_add_class")
+        fn = "pangu_server_declare_class" if lazy else "pangu_server_add_class"
+        _check(getattr(self.L, fn)(self.h, C.byref(params), C.byref(block), int(capacity_blocks),
+                                   int(max_jobs), factor, C.byref(out)), fn)
         nf = self.L.pangu_num_fields(C.byref(params))
         act = [block.nx1 > 1, block.nx2 > 1, block.nx3 > 1]
         n = [block.nx1, block.nx2, block.nx3]

@@ -2,13 +2,14 @@
 
     python -m pangu_b200.run [--workload torus2d|ot|torus3d|batch48]
                              [--precision fp64|mixed] [--cycles N]
-                             [--graph-cycles G] [--tiles X1,M2,T2,M3,T3]
+                             [--graph-cycles G] [--tiles [M1,]T1,M2,T2,M3,T3]
 
 First ``--cycles`` cycles are launched from the host (every stage kernel once
 per stage, in a fixed order), then ``--graph-cycles`` cycles are captured once
 as a CUDA graph and replayed. ``--tiles`` pins the flux kernels' tile shapes
-(x1 threads, x2 march, x2 threads, x3 march, x3 threads; march 0 = a
-shared-memory tile) instead of the engine's defaults; nothing is autotuned, so
+(x1 threads, x2 march, x2 threads, x3 march, x3 threads; or x1 march
+first, six values; march 0 = a tile loaded by the threads, 8 = primitives
+staged by TMA) instead of the engine's defaults; nothing is autotuned, so
 the sequence of launches depends only on the arguments. That makes the run a
 fixed target for a profiler: the n-th launch of a kernel is always the same
 stage of the same cycle. ``--profile-cycle K`` brackets host cycle K (from 0)
@@ -28,9 +29,12 @@ from . import workloads
 
 def _set_tiles(engine, tiles):
     if tiles:
-        x1, m2, t2, m3, t3 = (int(v) for v in tiles.split(","))
-        engine.set_flux_config(x1_threads=x1, x2_march=m2, x2_threads=t2, x3_march=m3,
-                               x3_threads=t3)
+        v = [int(x) for x in tiles.split(",")]
+        if len(v) == 5:  # x1 march 1
+            v = [1] + v
+        m1, t1, m2, t2, m3, t3 = v
+        engine.set_flux_config(x1_march=m1, x1_threads=t1, x2_march=m2, x2_threads=t2,
+                               x3_march=m3, x3_threads=t3)
 
 
 def run(workload="torus2d", precision="fp64", cycles=40, graph_cycles=0, tiles=None,
@@ -104,7 +108,7 @@ def main():
     ap.add_argument("--cycles", type=int, default=40)
     ap.add_argument("--graph-cycles", type=int, default=0)
     ap.add_argument("--tiles", default=None,
-                    help="x1_threads,x2_march,x2_threads,x3_march,x3_threads")
+                    help="[x1_march,]x1_threads,x2_march,x2_threads,x3_march,x3_threads")
     ap.add_argument("--profile-cycle", type=int, default=None,
                     help="host cycle bracketed by cudaProfilerStart/Stop")
     args = ap.parse_args()

@@ -1,18 +1,32 @@
 """Parity at the benchmark sizes: the engine against the CPU oracle on the
-full workloads that bench.py measures (512x256 torus, 256^2 Orszag-Tang,
-256x128x128 torus in 16 blocks of 64^3), whole RK2 cycles with the dynamic dt
-policy. FP64 is bit-identical: primitives, conserved variables and flags
-over every cell, dt and every counter. The mixed form at full size stays
-within its tolerances (density 1e-5) after the same cycles."""
+full workloads that bench.py measures, whole RK2 cycles with the dynamic dt
+policy.
+
+* FP64, ten RK2 cycles of the 512x256 torus, the 256^2 Orszag-Tang vortex
+  and the 256x128x128 torus in 16 blocks of 64^3: primitives, conserved
+  variables and flags over every cell, dt and every counter equal the
+  oracle's bit for bit after the first and after the tenth cycle; the
+  accuracy targets (relative L1 per conserved field <= 1e-12 after one
+  cycle, <= 1e-9 after ten) are asserted as statements of their own.
+* The 48-torus batch (uneven grids of 128x64 blocks, 512x256 included) in one
+  block pool, two cycles: each job's primitives, dt and counters equal the
+  oracle run of that job alone.
+* The mixed form on the 3D torus for fifty cycles, and on the 2D torus and
+  Orszag-Tang for ten: per-field relative L1 against the FP64 engine within
+  the stated tolerances (density 1e-5, energy/velocity/field 1e-3, entropies
+  1e-2).
+"""
 import os
 
 import numpy as np
 import pytest
 
+from parity_util import rel_l1
+
 pytestmark = pytest.mark.gpu
 
 
-def _oracle_run(pin, prim0, cycles):
+def _oracle(pin, prim0):
     import pyoracle as po
     from pangu_b200 import params as prm
     po.set_threads(os.cpu_count() or 1)
@@ -24,45 +38,80 @@ def _oracle_run(pin, prim0, cycles):
     O.apply_boundary_conditions(base)
     one.prim[...] = base.prim
     one.cons[...] = base.cons
-    dt = pin.get_or_add_real("parthenon/time", "dt_init", 1e-5)
-    factor = pin.get_or_add_real("parthenon/time", "dt_factor", 2.0)
     O.reset_counters()
-    for _ in range(cycles):
-        dt = min(factor * dt, O.step(base, one, dt))
-    return O, base, dt
+    return O, base, one
 
 
-def _engine_run(pin, prim0, cycles):
+def _interior(geo, a):
+    s = geo.interior()
+    return a[:, :, s[0], s[1], s[2]]
+
+
+@pytest.mark.parametrize("workload", ["torus2d", "ot", "torus3d"])
+def test_fullsize_fp64_ten_cycles_bit_identical(workload):
     import torch
+
+    from pangu_b200 import workloads
     from pangu_b200.engine import Simulation
+    pin = workloads.job_input(workload, "fp64")
+    _, _, geo, prim0 = workloads.initial_state(pin)
     sim = Simulation(pin)
     sim.set_primitives(prim0)
     sim.engine.reset_counters()
-    for _ in range(cycles):
+    O, hbase, hone = _oracle(pin, prim0)
+    dt = pin.get_or_add_real("parthenon/time", "dt_init", 1e-5)
+    factor = pin.get_or_add_real("parthenon/time", "dt_factor", 2.0)
+    for cycle in range(1, 11):
         sim.step()
+        dt = min(factor * dt, O.step(hbase, hone, dt))
+        if cycle not in (1, 10):
+            continue
+        torch.cuda.synchronize()
+        for name in ("prim", "cons", "flag"):
+            np.testing.assert_array_equal(getattr(sim.base, name).cpu().numpy(),
+                                          getattr(hbase, name), err_msg=f"{name} cycle {cycle}")
+        assert sim.dt.item() == dt
+        np.testing.assert_array_equal(sim.engine.counters(), O.counters())
+        l1 = rel_l1(_interior(geo, sim.base.cons.cpu().numpy()), _interior(geo, hbase.cons))
+        assert np.all(l1 <= (1e-12 if cycle == 1 else 1e-9)), (cycle, l1)
+
+
+def test_batch48_pool_each_job_equals_oracle_alone():
+    import torch
+
+    from pangu_b200 import workloads
+    from pangu_b200.engine import Pool
+    pins, states = workloads.batch_jobs("fp64", states=True)
+    nblocks = [st.shape[0] for st in states]
+    pool = Pool(pins[0], sum(nblocks), len(pins))
+    jobs = [pool.attach(pin, st) for pin, st in zip(pins, states)]
+    pool.engine.reset_counters()
+    cycles = 2
+    for _ in range(cycles):
+        pool.step()
     torch.cuda.synchronize()
-    return sim
+    grids = set()
+    for job, pin, st in zip(jobs, pins, states):
+        O, hbase, hone = _oracle(pin, st)
+        dt = pin.get_or_add_real("parthenon/time", "dt_init", 1e-5)
+        factor = pin.get_or_add_real("parthenon/time", "dt_factor", 2.0)
+        for _ in range(cycles):
+            dt = min(factor * dt, O.step(hbase, hone, dt))
+        np.testing.assert_array_equal(pool.primitives(job), hbase.prim, err_msg=f"job {job}")
+        assert pool.dt[job].item() == dt, job
+        np.testing.assert_array_equal(pool.engine.job_counters(job), O.counters())
+        grids.add((pin.get_or_add_integer("parthenon/mesh", "nx1", 1),
+                   pin.get_or_add_integer("parthenon/mesh", "nx2", 1)))
+    assert (512, 256) in grids and len(jobs) == 48
 
 
-@pytest.mark.parametrize("workload,cycles", [("torus2d", 3), ("ot", 3), ("torus3d", 1)])
-def test_fullsize_fp64_bit_identical(workload, cycles):
+@pytest.mark.parametrize("workload,cycles", [("torus3d", 50), ("torus2d", 10), ("ot", 10)])
+def test_fullsize_mixed_within_tolerance(workload, cycles):
     import bench
-    pin = bench.job_input(workload, "fp64")
-    _, _, _, prim0 = bench.initial_state(pin)
-    sim = _engine_run(pin, prim0, cycles)
-    O, hbase, dt = _oracle_run(pin, prim0, cycles)
-    for name in ("prim", "cons", "flag"):
-        np.testing.assert_array_equal(getattr(sim.base, name).cpu().numpy(),
-                                      getattr(hbase, name), err_msg=name)
-    assert sim.dt.item() == dt
-    np.testing.assert_array_equal(sim.engine.counters(), O.counters())
-
-
-@pytest.mark.parametrize("workload", ["torus2d", "ot"])
-def test_fullsize_mixed_within_tolerance(workload):
-    import bench
-    pin = bench.job_input(workload, "fp64")
-    _, _, geo, prim0 = bench.initial_state(pin)
-    err = bench.error_vs_fp64(pin, prim0, geo, 10)["rel_l1"]
-    assert err["density"] <= 1e-5, err
-    assert all(v <= 1e-2 for v in err.values()), err
+    from pangu_b200 import workloads
+    pin = workloads.job_input(workload, "fp64")
+    _, _, geo, prim0 = workloads.initial_state(pin)
+    err = bench.error_vs_fp64(pin, prim0, geo, cycles)["rel_l1"]
+    for name, v in err.items():
+        limit = 1e-2 if "entropy" in name else (1e-5 if name == "density" else 1e-3)
+        assert v <= limit, (name, v, err)

@@ -103,3 +103,54 @@ def test_server_cancellation():
     np.testing.assert_array_equal(got, ref)
     np.testing.assert_array_equal(cnt, ref_cnt)
     assert srv.stats()["jobs"] == 1
+
+
+def test_server_lazy_classes_take_turns_under_budget():
+    """Classes declared lazily are charged at their first admission and
+    released when idle: with a budget that holds either class's memory but not
+    both, the second class's job waits until the first class's job finishes
+    and its memory is released; every result equals the job run alone."""
+    from pangu_b200.engine import Server
+    a_job = _job("torus", nx1=128, nx2=64, bx=(32, 16, 1), seed=5)  # 16 blocks
+    b_job = _job("ot", n=128, nblock=32)                             # 16 blocks
+
+    def peak_alone(job):
+        srv = Server(8 << 30)
+        c = srv.add_class(job[0], 16, 1, lazy=True)
+        srv.submit(c, *job, 2, 0.0)
+        srv.run()
+        st = srv.stats()
+        assert st["hbm_bytes"] == 0 and st["memory_waits"] == 0  # released after the run
+        return st["hbm_peak_bytes"]
+
+    pa, pb = peak_alone(a_job), peak_alone(b_job)
+    # room for either class (the engine's share is measured from the device's
+    # free memory, which moves in whole pages), not for both
+    budget = max(pa, pb) + max(4 << 20, min(pa, pb) // 3)
+    assert budget < pa + pb, (pa, pb)
+    srv = Server(budget)
+    ca = srv.add_class(a_job[0], 16, 1, lazy=True)
+    cb = srv.add_class(b_job[0], 16, 1, lazy=True)
+    ta = srv.submit(ca, *a_job, 4, 0.0)
+    tb = srv.submit(cb, *b_job, 3, 0.0)
+    srv.run()
+    st = srv.stats()
+    assert st["jobs"] == 2 and st["memory_waits"] == 1
+    assert st["hbm_peak_bytes"] <= budget and st["hbm_bytes"] == 0
+    (ga, times_a, cnt_a), (gb, times_b, cnt_b) = srv.result(ta), srv.result(tb)
+    first, second = (times_a, times_b) if times_a[1] <= times_b[1] else (times_b, times_a)
+    assert second[1] >= first[2]  # admitted only after the other class finished
+    for got, cnt, (pin, prim), n in ((ga, cnt_a, a_job, 4), (gb, cnt_b, b_job, 3)):
+        ref, ref_cnt = _alone(pin, prim, n)
+        np.testing.assert_array_equal(got, ref)
+        np.testing.assert_array_equal(cnt, ref_cnt)
+
+
+def test_server_lazy_class_too_big_reports_enomem():
+    from pangu_b200.engine import EngineError, Server
+    job = _job("torus", nx1=64, nx2=32, bx=(32, 16, 1), seed=6)
+    srv = Server(1 << 20)  # 1 MiB: the class never fits
+    c = srv.add_class(job[0], 4, 1, lazy=True)
+    srv.submit(c, *job, 2, 0.0)
+    with pytest.raises(EngineError):
+        srv.run()
