@@ -123,113 +123,142 @@ def error_vs_fp64(pin, prim0, geo, cycles):
 # ---------------------------------------------------------------------------
 # clocks sampled during the timed region
 # ---------------------------------------------------------------------------
+# The NVML sampling loop of ClockSampler, run as a separate process (a thread
+# of this interpreter is starved while the main thread sits in a blocking CUDA
+# call that holds the interpreter). Writes "monotonic time, SM MHz, max SM
+# MHz, power W, clock-event reason bits" lines until it is terminated.
+_NVML_SAMPLER = r"""
+import sys, time
+import pynvml as nv
+nv.nvmlInit()
+want = tuple(int(a) for a in sys.argv[1:4])
+h = None
+for n in range(nv.nvmlDeviceGetCount()):
+    c = nv.nvmlDeviceGetHandleByIndex(n)
+    pci = nv.nvmlDeviceGetPciInfo(c)
+    if (pci.domain, pci.bus, pci.device) == want:
+        h = c
+if h is None:
+    sys.exit(3)
+smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+while True:
+    t = time.monotonic()
+    sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+    pw = nv.nvmlDeviceGetPowerUsage(h) / 1e3
+    rb = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+    sys.stdout.write("%.6f,%d,%d,%.1f,%d\n" % (t, sm, smax, pw, rb))
+    sys.stdout.flush()
+    time.sleep(0.0005)
+"""
+
+
 class ClockSampler:
-    """SM clock, power and clock-event reasons of the benchmarked GPU, sampled
-    about every millisecond by a thread reading NVML while the timed region
-    runs (nvidia-smi's own sampling period, 100 ms, is longer than a short
-    timed region). Falls back to nvidia-smi when NVML cannot be opened."""
+    """SM clock, power and clock-event reasons of the benchmarked GPU during
+    the timed region: a separate process reads NVML about every millisecond
+    (NVML's device is the one with the CUDA device's PCI domain, bus and
+    device numbers: NVML enumerates every GPU of the machine, CUDA only the
+    visible ones), and the samples stamped inside the region are kept.
+    Falls back to nvidia-smi (100 ms period) when NVML cannot be opened."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
     REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40),
                ("sw_thermal_slowdown", 0x20), ("sw_power_cap", 0x4))
 
-    def __init__(self, gpu_index, period_s=0.001):
+    def __init__(self, gpu_index):
         self.gpu = gpu_index
-        self.period = period_s
-        self.rows = []   # (sm_mhz, max_mhz, power_w, reason bits)
         self.proc = None
         self.path = None
-        self.thread = None
+        self.nvml = False
+        self.t0 = self.t1 = None
 
-    def _handle(self, nv):
-        """The NVML device of CUDA device `gpu`: the one with its PCI domain,
-        bus and device numbers (NVML enumerates every GPU of the machine,
-        CUDA only the visible ones)."""
-        import torch
-        props = torch.cuda.get_device_properties(self.gpu)
-        want = (props.pci_domain_id, props.pci_bus_id, props.pci_device_id)
-        for n in range(nv.nvmlDeviceGetCount()):
-            h = nv.nvmlDeviceGetHandleByIndex(n)
-            pci = nv.nvmlDeviceGetPciInfo(h)
-            if (pci.domain, pci.bus, pci.device) == want:
-                return h
-        raise RuntimeError("no NVML device with the CUDA device's PCI address")
-
-    def _sample(self, nv, h, stop):
-        smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
-        while not stop.is_set():
-            try:
-                self.rows.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), smax,
-                                  nv.nvmlDeviceGetPowerUsage(h) / 1e3,
-                                  nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
-            except Exception:
-                break
-            stop.wait(self.period)
-
-    def __enter__(self):
-        import threading
-        try:
-            import pynvml as nv
-            nv.nvmlInit()
-            h = self._handle(nv)
-            self._stop = threading.Event()
-            self.thread = threading.Thread(target=self._sample, args=(nv, h, self._stop),
-                                           daemon=True)
-            self.thread.start()
-            return self
-        except Exception:
-            self.thread = None
+    def _start(self, cmd):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
+        self.out = open(self.path, "w")
+        self.proc = subprocess.Popen(cmd, stdout=self.out, stderr=subprocess.DEVNULL)
+
+    def _stop(self):
+        if self.proc is None:
+            return
+        self.proc.terminate()
         try:
-            self.out = open(self.path, "w")
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100", "-i", str(self.gpu)], stdout=self.out, stderr=subprocess.DEVNULL)
-        except (OSError, FileNotFoundError):
-            self.proc = None
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.close()
+        self.proc = None
+
+    def __enter__(self):
+        import torch
+        props = torch.cuda.get_device_properties(self.gpu)
+        pci = (props.pci_domain_id, props.pci_bus_id, props.pci_device_id)
+        try:
+            self._start([sys.executable, "-c", _NVML_SAMPLER, *map(str, pci)])
+            # wait for the first sample (or the sampler's exit)
+            deadline = time.monotonic() + 20.0
+            while time.monotonic() < deadline and self.proc.poll() is None and \
+                    os.path.getsize(self.path) == 0:
+                time.sleep(0.01)
+            self.nvml = os.path.getsize(self.path) > 0
+        except OSError:
+            self.nvml = False
+        if not self.nvml:
+            self._stop()
+            try:
+                self._start(["nvidia-smi", f"--query-gpu={self.FIELDS}",
+                             "--format=csv,noheader,nounits", "-lms", "100",
+                             "-i", str(self.gpu)])
+            except (OSError, FileNotFoundError):
+                self.proc = None
+        self.t0 = time.monotonic()
         return self
 
     def __exit__(self, *exc):
-        if self.thread is not None:
-            self._stop.set()
-            self.thread.join(timeout=5)
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-            self.out.close()
+        self.t1 = time.monotonic()
+        self._stop()
 
     def summary(self):
-        rows = list(self.rows)
-        src = "nvml, ~1 ms period, during the timed region"
+        rows = []
+        src = "nvml in a separate process, ~1 ms period, samples stamped inside the timed region"
         if self.path and os.path.exists(self.path):
-            src = "nvidia-smi, 100 ms period, during the timed region"
-            bits = [b for _, b in self.REASONS]
             with open(self.path) as f:
-                for line in f:
+                lines = f.read().splitlines()
+            os.unlink(self.path)
+            if self.nvml:
+                for line in lines:
+                    parts = line.split(",")
+                    if len(parts) != 5:
+                        continue
+                    t = float(parts[0])
+                    if self.t0 <= t <= self.t1:
+                        rows.append((float(parts[1]), float(parts[2]), float(parts[3]),
+                                     int(parts[4])))
+            else:
+                src = "nvidia-smi, 100 ms period, during the timed region"
+                bits = [b for _, b in self.REASONS]
+                for line in lines:
                     parts = [p.strip() for p in line.split(",")]
                     if len(parts) == 9 and parts[1].replace(".", "", 1).isdigit():
                         rb = sum(b for b, v in zip(bits, parts[5:9]) if v == "Active")
                         rows.append((float(parts[1]), float(parts[2]), None, rb))
-            os.unlink(self.path)
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         reasons = sorted({n for r in rows for n, b in self.REASONS if r[3] & b})
         pw = [r[2] for r in rows if r[2] is not None]
-        return {"sm_mhz": statistics.median(r[0] for r in rows),
-                "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
-                "samples": len(rows), "power_w_max": round(max(pw), 1) if pw else None,
-                "source": src}
+        out = {"sm_mhz": statistics.median(r[0] for r in rows),
+               "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+               "samples": len(rows), "power_w_max": round(max(pw), 1) if pw else None,
+               "source": src}
+        if self.t0 is not None and self.t1 is not None:
+            out["window_ms"] = round(1e3 * (self.t1 - self.t0), 1)
+        return out
 
 
 def wait_event(ev):
-    """Waits for a recorded CUDA event by polling it with short sleeps, so the
-    clock-sampling thread runs while the device works (a blocking synchronize
-    holds the interpreter)."""
+    """Waits for a recorded CUDA event by polling it with short sleeps (the
+    host returns as soon as the device is done, and the sampler's window
+    closes with the timed region)."""
     while not ev.query():
         time.sleep(0.0002)
 
@@ -661,24 +690,91 @@ def _oracle_job(pin, prim0, threads):
     return O, base, one
 
 
+class ReferenceJob:
+    """One job stepped by the REFERENCE's own stage tasks (pangu/src compiled
+    here over the Parthenon stand-in, timing build: OpenMP over par_for, the C
+    library's pow, -O3), in the order of ideal_grmhd.cc:62-110, with the
+    restatement's versions of the parts Parthenon does (update, ghost
+    exchange, boundary conditions). Used where that library exists (it is
+    built from the reference's sources and travels with the repository);
+    otherwise the restatement alone (oracle.cc) is timed."""
+
+    KIND = "reference"
+    WHAT = ("the reference's stage tasks (pangu/src over a Parthenon stand-in, OpenMP) with "
+            "the restatement's update, exchange and boundaries")
+
+    def __init__(self, pin, prim0, threads):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as po
+        self.O, self.base, self.one = _oracle_job(pin, prim0, threads)
+        packages = prm.process_packages(pin)
+        self.params = prm.params_struct(packages)
+        self.R = po.RefTasks(self.params, prm.mesh_struct(pin), timing=True)
+
+    def step(self, dt):
+        O, R, p = self.O, self.R, self.params
+        est = None
+        for st, beta in ((1, 0.5), (2, 1.0)):
+            c0, c1 = (self.base, self.one) if st == 1 else (self.one, self.base)
+            R.run("fix_primitive", c0)
+            R.run("calculate_conservative", c0)
+            R.run("calculate_fluxes", c0)
+            if p.enable_B:
+                R.run("constrained_transport", c0)
+            O.flux_divergence_update(self.base, c0, c1, beta * dt)
+            O.exchange_ghosts(c1)
+            R.run("add_geometric_source", c1, beta * dt)
+            R.run("recovery", c1)
+            if p.enable_heating:
+                R.run("apply_electron_heating", c1)
+            if p.recovery == 0:
+                R.run("fix_recovery", c1)
+            O.apply_boundary_conditions(c1)
+            if st == 2:
+                est = R.run("estimate_dt", c1)
+        return est
+
+
+class PortJob:
+    """One job stepped by the CPU restatement (oracle.cc, OpenMP)."""
+
+    KIND = "port"
+    WHAT = "oracle/oracle.cc, OpenMP"
+
+    def __init__(self, pin, prim0, threads):
+        self.O, self.base, self.one = _oracle_job(pin, prim0, threads)
+
+    def step(self, dt):
+        return self.O.step(self.base, self.one, dt)
+
+
+def cpu_job(pin, prim0, threads):
+    """The reference's own tasks where their library exists, else the port."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    if po.reftasks_omp() is not None:
+        return ReferenceJob(pin, prim0, threads)
+    return PortJob(pin, prim0, threads)
+
+
 def cpu_baseline(pin, prim0, budget_s=15.0, max_steps=None):
     threads = os.cpu_count() or 1
-    O, base, one = _oracle_job(pin, prim0, threads)
+    job = cpu_job(pin, prim0, threads)
     dt = pin.get_or_add_real("parthenon/time", "dt_init", 1e-5)
     factor = pin.get_or_add_real("parthenon/time", "dt_factor", 2.0)
     steps = 0
     t0 = time.perf_counter()
     while True:
-        est = O.step(base, one, dt)
+        est = job.step(dt)
         dt = min(factor * dt, est)
         steps += 1
         el = time.perf_counter() - t0
         if el >= budget_s or (max_steps and steps >= max_steps):
             break
     value = interior_cells(pin) * steps / el
-    return {"value": round(value, 1), "unit": METRIC, "cores": threads, "kind": "port",
+    return {"value": round(value, 1), "unit": METRIC, "cores": threads, "kind": job.KIND,
             "sample": f"{steps} RK2 steps of the same job from its initial state "
-                      f"({el:.1f} s, oracle/oracle.cc, OpenMP, FP64)"}
+                      f"({el:.1f} s, {job.WHAT}, FP64)"}
 
 
 # ---------------------------------------------------------------------------
@@ -876,10 +972,11 @@ def run_reference(args):
     for pin in pins:
         pin.set("b200", "precision", "fp64")
         prim0 = initial_state(pin)[3]
-        O, base, one = _oracle_job(pin, prim0, threads)
+        job = cpu_job(pin, prim0, threads)
         dt = pin.get_or_add_real("parthenon/time", "dt_init", 1e-5)
         factor = pin.get_or_add_real("parthenon/time", "dt_factor", 2.0)
-        runs.append([O, base, one, dt, factor, interior_cells(pin)])
+        runs.append([job, dt, factor, interior_cells(pin)])
+    kind, what = runs[0][0].KIND, runs[0][0].WHAT
     budget = args.ref_budget
     # W untimed warm-up steps, round robin over the jobs like the timed ones
     # (bounded by the same time budget)
@@ -887,21 +984,21 @@ def run_reference(args):
     t0 = time.perf_counter()
     while warm < args.warmup and time.perf_counter() - t0 < budget:
         r = runs[warm % len(runs)]
-        r[3] = min(r[4] * r[3], r[0].step(r[1], r[2], r[3]))
+        r[1] = min(r[2] * r[1], r[0].step(r[1]))
         warm += 1
     steps, cells = 0, 0
     t0 = time.perf_counter()
     while steps < args.steps:
         r = runs[steps % len(runs)]
-        r[3] = min(r[4] * r[3], r[0].step(r[1], r[2], r[3]))
-        cells += r[5]
+        r[1] = min(r[2] * r[1], r[0].step(r[1]))
+        cells += r[3]
         steps += 1
         if time.perf_counter() - t0 >= budget:
             break
     el = time.perf_counter() - t0
     value = cells / el
     sample = (f"{steps} of {args.steps} RK2 steps, round robin over {len(runs)} job(s) of the "
-              f"workload ({el:.1f} s of CPU time budget {budget:.0f} s, FP64)")
+              f"workload ({el:.1f} s of CPU time budget {budget:.0f} s, {what}, FP64)")
     line = {"metric": METRIC, "value": round(value, 1), "unit": METRIC, "n_gpus": 0,
             "steps": steps, "warmup": warm,
             "ms_per_step": round(1e3 * el / steps, 3), "higher_is_better": True,
@@ -909,7 +1006,7 @@ def run_reference(args):
             "data": "synthetic (seeded initial conditions)",
             "config": config(args.workload, args.precision), "impl": "reference",
             "cpu_baseline": {"value": round(value, 1), "unit": METRIC, "cores": threads,
-                             "kind": "port", "sample": sample},
+                             "kind": kind, "sample": sample},
             "e2e": {"value": round(value, 1), "unit": METRIC, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

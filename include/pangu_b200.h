@@ -19,7 +19,9 @@
  * PANGU_OK (0) or a negative PANGU_E* code. Field arrays are caller-owned device memory laid
  * out like a Parthenon MeshBlockPack with Kokkos LayoutRight:
  *   [block][variable][k][j][i]  (i fastest), over the "entire" index domain
- *   (interior plus ng ghost cells on each side of every active direction).
+ *   (interior plus ng ghost cells on each side of every active direction),
+ * or, array by array, one allocation per (block, component) reached through
+ * a pointer table (pangu_pack), as Parthenon keeps its variables.
  * The engine keeps no pointer to them past the call.
  *
  * Variable order inside prim/cons is the order of
@@ -146,6 +148,34 @@ typedef struct pangu_pack {
   double *alfven;  /* [NB][3][N3][N2][N1] */
   double *efield;  /* [NB][3][N3][N2][N1] */
   double *flag;    /* [NB][N3][N2][N1]; chainer only (may be NULL otherwise) */
+  /* Per-(block, component) layout, the form of a Parthenon pack of
+   * per-block, per-variable views (md->PackVariables, laxf.cc:37-53): a
+   * non-NULL table replaces the contiguous layout of its array above (whose
+   * pointer may then be NULL). Entry b * NC + c of a table is the device
+   * address of component c of block b, an [N3][N2][N1] array with i fastest;
+   * NC = NF for prim, cons and the fluxes, 3 for alfven and efield, 1 for
+   * flag. Each table is a device array of NB * NC addresses (NB: the engine's
+   * blocks, or the pool's capacity), each of an array of N3 * N2 * N1
+   * elements, that must stay valid while the call's work runs (and for the
+   * replays of a CUDA graph that captured it); the engine cannot check either
+   * on the host. Packs with tables run separately compiled instances of the
+   * kernels, so the contiguous layout pays nothing for them; FP64 results are
+   * bit-identical to the contiguous layout's, mixed-precision ones agree to
+   * rounding (that form is compiled with FMA contraction, whose choices may
+   * differ between the two instances). The
+   * per-task and stage entry points accept tables; pangu_job_start,
+   * pangu_generate, the block pool and the serving loop take the contiguous
+   * layout only (PANGU_EINVAL otherwise), and the TMA-staged flux kernels are
+   * replaced by their thread-loaded forms for primitives given by a table.
+   * A zero-initialised pack has no tables. */
+  double *const *prim_vars;
+  double *const *cons_vars;
+  double *const *flux1_vars;
+  double *const *flux2_vars;
+  double *const *flux3_vars;
+  double *const *alfven_vars;
+  double *const *efield_vars;
+  double *const *flag_vars;
 } pangu_pack;
 
 /* Hit counters of the floors and fixers (not present in the reference, which

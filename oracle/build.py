@@ -6,6 +6,11 @@
   where they lie, through the stand-in headers of ``oracle/refshim``. Only
   when the reference sources are present (this container); the built file
   travels with the repository snapshot like any other built library.
+* ``oracle/_ref/libpangu_reftasks_omp.so`` -- the same tasks built for timing
+  (the CPU baseline and ``bench.py --impl reference``): the reference's own
+  math functions (the C library's pow), -O3 with the compiler's default
+  contraction, and the stand-in's par_for/par_reduce spread over the host
+  threads with OpenMP, as Kokkos' OpenMP backend would run them.
 * ``oracle/_ref/libpangu_reftasks.so`` -- the reference's own stage tasks
   (REF_TASK_SOURCES below, compiled from where they lie) over the host-only
   Parthenon stand-in of ``oracle/refshim/parthenon/package.hpp``, with the
@@ -31,6 +36,7 @@ REFERENCE_SRC = os.environ.get("PANGU_REFERENCE_SRC", "/root/reference/pangu/src
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 REFCELL_SO = os.path.join(HERE, "_ref", "libpangu_refcell.so")
 REFTASKS_SO = os.path.join(HERE, "_ref", "libpangu_reftasks.so")
+REFTASKS_OMP_SO = os.path.join(HERE, "_ref", "libpangu_reftasks_omp.so")
 
 # The reference's stage-task sources (paths under pangu/src).
 REF_TASK_SOURCES = (
@@ -95,8 +101,27 @@ def build_reftasks(force: bool = False) -> str | None:
     return REFTASKS_SO
 
 
+def build_reftasks_omp(force: bool = False) -> str | None:
+    if not os.path.isdir(REFERENCE_SRC):
+        return REFTASKS_OMP_SO if os.path.exists(REFTASKS_OMP_SO) else None
+    shim = os.path.join(HERE, "refshim")
+    src = [os.path.join(HERE, "ref_tasks.cc"), os.path.join(shim, "parthenon", "package.hpp"),
+           os.path.join(shim, "Kokkos_Core.hpp")]
+    ref = [os.path.join(REFERENCE_SRC, f) for f in REF_TASK_SOURCES]
+    if not force and _newer(REFTASKS_OMP_SO, src + ref):
+        return REFTASKS_OMP_SO
+    os.makedirs(os.path.dirname(REFTASKS_OMP_SO), exist_ok=True)
+    cmd = ["g++", "-O3", "-std=c++17", "-shared", "-fPIC", "-fopenmp", "-DPANGU_REFSHIM_OMP",
+           "-I", shim, "-I", os.path.join(ROOT, "pangu_b200", "csrc"),
+           "-I", os.path.join(ROOT, "include"), "-I", REFERENCE_SRC, src[0], *ref,
+           "-o", REFTASKS_OMP_SO]
+    subprocess.check_call(cmd)
+    return REFTASKS_OMP_SO
+
+
 if __name__ == "__main__":
     force = "--force" in sys.argv
     print(build_oracle(force))
     print(build_refcell(force))
     print(build_reftasks(force))
+    print(build_reftasks_omp(force))

@@ -112,11 +112,32 @@ def reftasks():
     return _reftasks
 
 
-class RefTasks:
-    """The reference's task functions on host containers (HostContainer)."""
+_reftasks_omp = None
 
-    def __init__(self, params: abi.Params, mesh: abi.Mesh):
-        self.L = reftasks()
+
+def reftasks_omp():
+    """The timing build of the reference's stage tasks (the C library's pow,
+    -O3, par_for over the host threads with OpenMP), or None where it was
+    neither built nor travelled with the repository."""
+    global _reftasks_omp
+    if _reftasks_omp is None:
+        path = _build.build_reftasks_omp()
+        if path is None or not os.path.exists(path):
+            return None
+        L = C.CDLL(path)
+        L.ref_task.restype = C.c_int
+        L.ref_task.argtypes = [C.POINTER(abi.Params), C.POINTER(abi.Mesh), C.POINTER(abi.Pack),
+                               C.c_int, C.c_double, _D]
+        _reftasks_omp = L
+    return _reftasks_omp
+
+
+class RefTasks:
+    """The reference's task functions on host containers (HostContainer);
+    timing=True takes the OpenMP timing build."""
+
+    def __init__(self, params: abi.Params, mesh: abi.Mesh, timing: bool = False):
+        self.L = reftasks_omp() if timing else reftasks()
         if self.L is None:
             raise RuntimeError("the reference's task library is not built")
         self.params, self.mesh = params, mesh

@@ -11,13 +11,18 @@
 //  * a MeshData is a set of equal meshblocks; variables are addressed per
 //    (block, component) through a table of base pointers of [N3][N2][N1]
 //    arrays (i fastest), as Parthenon's packs of per-variable views are;
+//    MeshBlockData::Get(name) gives one block's variable (its components
+//    contiguous, as a Parthenon variable's are) and its face fluxes;
 //  * IndexDomain::entire spans every cell, IndexDomain::interior the cells
 //    without the ng ghost layers of each active direction;
 //  * uniform Cartesian coordinates: Xc<d>(idx) = x0_d + (idx + 1/2) dx_d and
 //    Xf<d, f>(k, j, i) = x0_d + idx dx_d on the face f == d (the cell centre
 //    along the other directions), x0_d = block xmin - ng dx_d;
 //  * par_for runs its index ranges as serial nested loops in argument order;
-//    par_reduce with Kokkos::Min starts from the largest finite Real.
+//    par_reduce with Kokkos::Min starts from the largest finite Real. Built
+//    with PANGU_REFSHIM_OMP and OpenMP (the timing build of the reference's
+//    tasks only), both spread their index ranges over the host threads, as
+//    Kokkos' OpenMP backend does; the fixtures use the serial form.
 #ifndef PANGU_ORACLE_REFSHIM_PARTHENON_PACKAGE_HPP
 #define PANGU_ORACLE_REFSHIM_PARTHENON_PACKAGE_HPP
 
@@ -239,6 +244,9 @@ class MeshBlock {
   template <class F>
   void par_for(const char *, int b0, int b1, int k0, int k1, int j0, int j1, int i0, int i1,
                const F &f) const {
+#if defined(PANGU_REFSHIM_OMP) && defined(_OPENMP)
+#pragma omp parallel for collapse(4) schedule(static)
+#endif
     for (int b = b0; b <= b1; ++b)
       for (int k = k0; k <= k1; ++k)
         for (int j = j0; j <= j1; ++j)
@@ -246,6 +254,9 @@ class MeshBlock {
   }
   template <class F>
   void par_for(const char *, int k0, int k1, int j0, int j1, int i0, int i1, const F &f) const {
+#if defined(PANGU_REFSHIM_OMP) && defined(_OPENMP)
+#pragma omp parallel for collapse(3) schedule(static)
+#endif
     for (int k = k0; k <= k1; ++k)
       for (int j = j0; j <= j1; ++j)
         for (int i = i0; i <= i1; ++i) f(k, j, i);
@@ -254,11 +265,28 @@ class MeshBlock {
   void par_reduce(const char *, int k0, int k1, int j0, int j1, int i0, int i1, const F &f,
                   Kokkos::Min<Real> red) const {
     Real acc = std::numeric_limits<Real>::max();
+#if defined(PANGU_REFSHIM_OMP) && defined(_OPENMP)
+#pragma omp parallel for collapse(3) schedule(static) reduction(min : acc)
+#endif
     for (int k = k0; k <= k1; ++k)
       for (int j = j0; j <= j1; ++j)
         for (int i = i0; i <= i1; ++i) f(k, j, i, acc);
     red.result = acc;
   }
+};
+
+// One variable of one block, as MeshBlockData::Get returns it: the
+// device-side data of its components (contiguous, [comp][N3][N2][N1]) and of
+// its face fluxes, flux[X1DIR..X3DIR].
+struct ArrayRef {
+  Real *p = nullptr;
+  Real *data() const { return p; }
+};
+struct VariableRef {
+  ArrayRef data;
+  ArrayRef flux[4];
+  int ncomp = 1;
+  int NumComponents() const { return ncomp; }
 };
 
 template <class T>
@@ -267,6 +295,15 @@ class MeshBlockData {
   MeshBlockData(std::shared_ptr<MeshBlock> pmb, std::shared_ptr<const VarTable> vt, int b)
       : pmb_(std::move(pmb)), vt_(std::move(vt)), b_(b) {}
   std::shared_ptr<MeshBlock> GetBlockPointer() const { return pmb_; }
+  VariableRef Get(const std::string &name) const {
+    const VarTable::Var &v = vt_->vars.at(name);
+    VariableRef r;
+    r.ncomp = v.ncomp;
+    r.data.p = v.data[(size_t)b_ * v.ncomp];
+    for (int d = 0; d < 3; ++d)
+      if (!v.flux[d].empty()) r.flux[d + 1].p = v.flux[d][(size_t)b_ * v.ncomp];
+    return r;
+  }
   VariablePack<T> PackVariables(const std::vector<std::string> &names, PackIndexMap &idx) {
     return VariablePack<T>(make_pack(vt_, names, &idx, false), b_);
   }

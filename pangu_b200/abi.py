@@ -89,6 +89,10 @@ class Pack(C.Structure):
         ("prim", C.c_void_p), ("cons", C.c_void_p),
         ("flux1", C.c_void_p), ("flux2", C.c_void_p), ("flux3", C.c_void_p),
         ("alfven", C.c_void_p), ("efield", C.c_void_p), ("flag", C.c_void_p),
+        # per-(block, component) pointer tables (device arrays), NULL: contiguous
+        ("prim_vars", C.c_void_p), ("cons_vars", C.c_void_p),
+        ("flux1_vars", C.c_void_p), ("flux2_vars", C.c_void_p), ("flux3_vars", C.c_void_p),
+        ("alfven_vars", C.c_void_p), ("efield_vars", C.c_void_p), ("flag_vars", C.c_void_p),
     ]
 
 

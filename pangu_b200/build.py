@@ -31,7 +31,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "--f
 # Translation units of the mixed-precision form: FMA contraction and the fast
 # FP32 division, square root and math functions (2.6 % per cycle on the 2D
 # torus, 6.6 % on the 3D one; the errors against FP64 do not change).
-MIXED_SOURCES = ("engine_mixed.cu",)
+MIXED_SOURCES = ("engine_mixed.cu", "engine_mixed_tables.cu")
 
 
 def sources():

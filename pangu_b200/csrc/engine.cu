@@ -16,45 +16,62 @@
 using namespace pgd;
 using namespace pgk64;
 
-// The mixed-precision instantiation of the launch helpers (engine_mixed.cu).
-namespace pgkmx {
-int run_fix_primitive(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
-int run_calc_cons(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
-int run_fluxes(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
-int run_ct(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
-int run_update(pangu_engine *e, const pangu_pack *mi, const pangu_pack *m0, const pangu_pack *m1,
-               double beta, const double *dt, cudaStream_t s);
-int run_exchange(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
-int run_source(pangu_engine *e, const pangu_pack *md, double beta, const double *dt,
-               cudaStream_t s);
-int run_recovery(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
-int run_heating(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
-int run_fix_recovery(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
-int run_bcs(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
-int run_estimate_dt(pangu_engine *e, const pangu_pack *md, double *dt_out, cudaStream_t s);
-int run_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
-              double beta, const double *dt, double *dt_est, cudaStream_t s);
-int run_stage_begin(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
-                    double beta, const double *dt, double *send, cudaStream_t s);
-int run_stage_update(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
-                     double beta, const double *dt, cudaStream_t s);
-int run_stage_middle(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
-                     double beta, const double *dt, cudaStream_t s);
-int run_stage_end(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
-                  const double *recv, double *dt_est, cudaStream_t s);
-int run_halo_pack(pangu_engine *e, const pangu_pack *md, double *buf, cudaStream_t s);
-int run_halo_unpack(pangu_engine *e, const pangu_pack *md, const double *buf, cudaStream_t s);
-int run_job_start(pangu_engine *e, int job, const pangu_pack *base, const pangu_pack *one,
-                  cudaStream_t s);
-int run_autotune(pangu_engine *e, const pangu_pack *md, cudaStream_t s);
-bool flux_tma_ok(const pangu_engine *e);
-int run_generate(pangu_engine *e, int job, const pangu_problem &pb, const pangu_pack *base,
+// The launch helpers of the other instantiations of kernels.cuh: mixed
+// precision (engine_mixed.cu) and the pointer-table forms of both precisions
+// (engine_tables.cu, engine_mixed_tables.cu).
+#define PGK_RUN_DECLS                                                                              \
+int run_fix_primitive(pangu_engine *e, const pangu_pack *md, cudaStream_t s);                      \
+int run_calc_cons(pangu_engine *e, const pangu_pack *md, cudaStream_t s);                          \
+int run_fluxes(pangu_engine *e, const pangu_pack *md, cudaStream_t s);                             \
+int run_ct(pangu_engine *e, const pangu_pack *md, cudaStream_t s);                                 \
+int run_update(pangu_engine *e, const pangu_pack *mi, const pangu_pack *m0, const pangu_pack *m1,  \
+               double beta, const double *dt, cudaStream_t s);                                     \
+int run_exchange(pangu_engine *e, const pangu_pack *md, cudaStream_t s);                           \
+int run_source(pangu_engine *e, const pangu_pack *md, double beta, const double *dt,               \
+               cudaStream_t s);                                                                    \
+int run_recovery(pangu_engine *e, const pangu_pack *md, cudaStream_t s);                           \
+int run_heating(pangu_engine *e, const pangu_pack *md, cudaStream_t s);                            \
+int run_fix_recovery(pangu_engine *e, const pangu_pack *md, cudaStream_t s);                       \
+int run_bcs(pangu_engine *e, const pangu_pack *md, cudaStream_t s);                                \
+int run_estimate_dt(pangu_engine *e, const pangu_pack *md, double *dt_out, cudaStream_t s);        \
+int run_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,           \
+              double beta, const double *dt, double *dt_est, cudaStream_t s);                      \
+int run_stage_begin(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,     \
+                    double beta, const double *dt, double *send, cudaStream_t s);                  \
+int run_stage_update(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,    \
+                     double beta, const double *dt, cudaStream_t s);                               \
+int run_stage_middle(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,    \
+                     double beta, const double *dt, cudaStream_t s);                               \
+int run_stage_end(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,       \
+                  const double *recv, double *dt_est, cudaStream_t s);                             \
+int run_halo_pack(pangu_engine *e, const pangu_pack *md, double *buf, cudaStream_t s);             \
+int run_halo_unpack(pangu_engine *e, const pangu_pack *md, const double *buf, cudaStream_t s);     \
+int run_job_start(pangu_engine *e, int job, const pangu_pack *base, const pangu_pack *one,         \
+                  cudaStream_t s);                                                                 \
+int run_autotune(pangu_engine *e, const pangu_pack *md, cudaStream_t s);                           \
+bool flux_tma_ok(const pangu_engine *e);                                                           \
+int run_generate(pangu_engine *e, int job, const pangu_problem &pb, const pangu_pack *base,        \
                  cudaStream_t s);
-}  // namespace pgkmx
 
-// Launch helper of the engine's precision.
+namespace pgkmx {
+PGK_RUN_DECLS
+}  // namespace pgkmx
+namespace pgk64t {
+PGK_RUN_DECLS
+}  // namespace pgk64t
+namespace pgkmxt {
+PGK_RUN_DECLS
+}  // namespace pgkmxt
+
+// Launch helper of the engine's precision, for packs in the contiguous layout.
 #define RUN(fn, ...)                                                               \
   (e->p.precision == PANGU_PRECISION_MIXED ? pgkmx::fn(__VA_ARGS__) : pgk64::fn(__VA_ARGS__))
+// Launch helper of the engine's precision and of the packs' layout: tab is
+// true when a pack of the call gives an array through a pointer table.
+#define RUNT(tab, fn, ...)                                                                 \
+  (e->p.precision == PANGU_PRECISION_MIXED                                                 \
+       ? ((tab) ? pgkmxt::fn(__VA_ARGS__) : pgkmx::fn(__VA_ARGS__))                        \
+       : ((tab) ? pgk64t::fn(__VA_ARGS__) : pgk64::fn(__VA_ARGS__)))
 
 
 // ===========================================================================
@@ -482,8 +499,8 @@ int pangu_job_attach(pangu_engine *e, const pangu_mesh *mesh, double a, double h
 
 int pangu_job_start(pangu_engine *e, int32_t job, const pangu_pack *base, const pangu_pack *one,
                     void *stream) {
-  if (!pack_ok(e, base) || !pack_ok(e, one) || job < 0 || job >= e->max_jobs ||
-      !e->jobs[job].live)
+  if (!pack_ok(e, base) || !pack_ok(e, one) || !contiguous(base) || !contiguous(one) ||
+      job < 0 || job >= e->max_jobs || !e->jobs[job].live)
     return PANGU_EINVAL;
   return RUN(run_job_start, e, job, base, one, S(stream));
 }
@@ -513,70 +530,71 @@ int pangu_active_blocks(const pangu_engine *e) { return e ? e->d.NB : PANGU_EINV
 
 int pangu_fix_primitive(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
-  return RUN(run_fix_primitive, e, md, S(stream));
+  return RUNT(!contiguous(md), run_fix_primitive, e, md, S(stream));
 }
 int pangu_calculate_conservative(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
-  return RUN(run_calc_cons, e, md, S(stream));
+  return RUNT(!contiguous(md), run_calc_cons, e, md, S(stream));
 }
 int pangu_calculate_fluxes(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
-  return RUN(run_fluxes, e, md, S(stream));
+  return RUNT(!contiguous(md), run_fluxes, e, md, S(stream));
 }
 int pangu_constrained_transport(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
   if (!e->p.enable_B) return PANGU_EINVAL;
-  return RUN(run_ct, e, md, S(stream));
+  return RUNT(!contiguous(md), run_ct, e, md, S(stream));
 }
 int pangu_flux_divergence_update(pangu_engine *e, const pangu_pack *mc_init, const pangu_pack *mc0,
                                  const pangu_pack *mc1, double beta, const double *dt,
                                  void *stream) {
   if (!pack_ok(e, mc_init) || !pack_ok(e, mc0) || !pack_ok(e, mc1) || !dt) return PANGU_EINVAL;
   if (e->d.NB == 0) return PANGU_OK;
-  return RUN(run_update, e, mc_init, mc0, mc1, beta, dt, S(stream));
+  return RUNT(!contiguous(mc_init) || !contiguous(mc0) || !contiguous(mc1), run_update,
+              e, mc_init, mc0, mc1, beta, dt, S(stream));
 }
 int pangu_exchange_ghosts(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
-  return RUN(run_exchange, e, md, S(stream));
+  return RUNT(!contiguous(md), run_exchange, e, md, S(stream));
 }
 int pangu_add_geometric_source(pangu_engine *e, const pangu_pack *md, double beta, const double *dt,
                                void *stream) {
   GUARD(e, md);
   if (!dt) return PANGU_EINVAL;
-  return RUN(run_source, e, md, beta, dt, S(stream));
+  return RUNT(!contiguous(md), run_source, e, md, beta, dt, S(stream));
 }
 int pangu_recovery(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
-  return RUN(run_recovery, e, md, S(stream));
+  return RUNT(!contiguous(md), run_recovery, e, md, S(stream));
 }
 int pangu_apply_electron_heating(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
-  return RUN(run_heating, e, md, S(stream));
+  return RUNT(!contiguous(md), run_heating, e, md, S(stream));
 }
 int pangu_fix_recovery(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
   if (e->p.recovery != PANGU_RECOVERY_CHAINER) return PANGU_EINVAL;
-  return RUN(run_fix_recovery, e, md, S(stream));
+  return RUNT(!contiguous(md), run_fix_recovery, e, md, S(stream));
 }
 int pangu_apply_boundary_conditions(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
-  return RUN(run_bcs, e, md, S(stream));
+  return RUNT(!contiguous(md), run_bcs, e, md, S(stream));
 }
 int pangu_estimate_dt(pangu_engine *e, const pangu_pack *md, double *dt_out, void *stream) {
   GUARD(e, md);
   if (!dt_out) return PANGU_EINVAL;
-  return RUN(run_estimate_dt, e, md, dt_out, S(stream));
+  return RUNT(!contiguous(md), run_estimate_dt, e, md, dt_out, S(stream));
 }
 
 int pangu_autotune(pangu_engine *e, const pangu_pack *md, void *stream) {
   GUARD(e, md);
-  return RUN(run_autotune, e, md, S(stream));
+  return RUNT(!contiguous(md), run_autotune, e, md, S(stream));
 }
 
 int pangu_generate(pangu_engine *e, int32_t job, const pangu_problem *problem,
                    const pangu_pack *base, void *stream) {
-  if (!pack_ok(e, base) || !problem || job < 0 || job >= e->max_jobs || !e->jobs[job].live ||
-      problem->kind < 0 || problem->kind > 2)
+  if (!pack_ok(e, base) || !contiguous(base) || !problem || job < 0 || job >= e->max_jobs ||
+      !e->jobs[job].live || problem->kind < 0 || problem->kind > 2)
     return PANGU_EINVAL;
   if (problem->kind == PANGU_PROBLEM_FM_TORUS &&
       !(problem->kappa > 0 && problem->beta > 0 && problem->rmax > problem->rin))
@@ -621,7 +639,8 @@ int pangu_stage(pangu_engine *e, int stage, const pangu_pack *base, const pangu_
     return PANGU_EINVAL;
   if (halo_sends(e) || halo_recvs(e)) return PANGU_EINVAL;  // a shard: the three-part calls
   if (e->d.NB == 0) return PANGU_OK;
-  return RUN(run_stage, e, stage, base, one, beta, dt, dt_est, S(stream));
+  return RUNT(!contiguous(base) || !contiguous(one), run_stage,
+              e, stage, base, one, beta, dt, dt_est, S(stream));
 }
 
 // ---------------------------------------------------------------------------
@@ -694,12 +713,12 @@ int pangu_halo_counts(const pangu_engine *e, int64_t *send_counts, int64_t *recv
 
 int pangu_halo_pack(pangu_engine *e, const pangu_pack *md, double *send, void *stream) {
   if (!pack_ok(e, md) || (halo_sends(e) && !send)) return PANGU_EINVAL;
-  return RUN(run_halo_pack, e, md, send, S(stream));
+  return RUNT(!contiguous(md), run_halo_pack, e, md, send, S(stream));
 }
 
 int pangu_halo_unpack(pangu_engine *e, const pangu_pack *md, const double *recv, void *stream) {
   if (!pack_ok(e, md) || (halo_recvs(e) && !recv)) return PANGU_EINVAL;
-  return RUN(run_halo_unpack, e, md, recv, S(stream));
+  return RUNT(!contiguous(md), run_halo_unpack, e, md, recv, S(stream));
 }
 
 int pangu_stage_begin(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
@@ -708,7 +727,8 @@ int pangu_stage_begin(pangu_engine *e, int stage, const pangu_pack *base, const 
       (halo_sends(e) && !send))
     return PANGU_EINVAL;
   if (e->d.NB == 0) return PANGU_OK;
-  return RUN(run_stage_begin, e, stage, base, one, beta, dt, send, S(stream));
+  return RUNT(!contiguous(base) || !contiguous(one), run_stage_begin,
+              e, stage, base, one, beta, dt, send, S(stream));
 }
 
 int pangu_stage_update(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
@@ -716,7 +736,8 @@ int pangu_stage_update(pangu_engine *e, int stage, const pangu_pack *base, const
   if (!pack_ok(e, base) || !pack_ok(e, one) || !dt || (stage != 1 && stage != 2))
     return PANGU_EINVAL;
   if (e->d.NB == 0) return PANGU_OK;
-  return RUN(run_stage_update, e, stage, base, one, beta, dt, S(stream));
+  return RUNT(!contiguous(base) || !contiguous(one), run_stage_update,
+              e, stage, base, one, beta, dt, S(stream));
 }
 
 int pangu_stage_middle(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
@@ -724,7 +745,8 @@ int pangu_stage_middle(pangu_engine *e, int stage, const pangu_pack *base, const
   if (!pack_ok(e, base) || !pack_ok(e, one) || !dt || (stage != 1 && stage != 2))
     return PANGU_EINVAL;
   if (e->d.NB == 0) return PANGU_OK;
-  return RUN(run_stage_middle, e, stage, base, one, beta, dt, S(stream));
+  return RUNT(!contiguous(base) || !contiguous(one), run_stage_middle,
+              e, stage, base, one, beta, dt, S(stream));
 }
 
 int pangu_stage_end(pangu_engine *e, int stage, const pangu_pack *base, const pangu_pack *one,
@@ -733,7 +755,8 @@ int pangu_stage_end(pangu_engine *e, int stage, const pangu_pack *base, const pa
       (halo_recvs(e) && !recv))
     return PANGU_EINVAL;
   if (e->d.NB == 0) return PANGU_OK;
-  return RUN(run_stage_end, e, stage, base, one, recv, dt_est, S(stream));
+  return RUNT(!contiguous(base) || !contiguous(one), run_stage_end,
+              e, stage, base, one, recv, dt_est, S(stream));
 }
 
 // ---------------------------------------------------------------------------

@@ -65,6 +65,15 @@ struct Dims {
   // Mixed form only: the x1- and x2-face tables rounded once to FP32 (the
   // FP32 face fluxes read these); null otherwise.
   const float *f1tab32, *f2tab32;
+  // Layout of the launch's arrays: when the pack they come from gives
+  // per-(block, component) pointer tables (pangu_pack *_vars), the table of
+  // each role; null for the contiguous layout [slot][component][N3][N2][N1].
+  // Roles: prim; cons written (or read) by the task; cons read as the RK
+  // starting state; the launch's flux array; the three flux arrays; alfven;
+  // efield; flag.
+  void *const *tP;
+  double *const *tU, *const *tUi, *const *tF, *const *tF1, *const *tF2, *const *tF3;
+  double *const *tA, *const *tE, *const *tG;
 };
 
 // Tile shape code of the flux kernels whose primitives are staged into
@@ -85,7 +94,7 @@ struct PoolJob {
 struct pangu_engine {
   pangu_params p;
   pangu_mesh m;  // block shape (nx, ng); for a single-mesh engine the whole mesh
-  Dims d;        // d.NB = active blocks; d.slot = d_active
+  Dims d{};      // d.NB = active blocks; d.slot = d_active
   int capacity = 0, max_jobs = 0;
   std::vector<PoolJob> jobs;
   std::vector<char> slot_used;

@@ -1,9 +1,16 @@
-// kernels.cuh -- the engine's kernels and launch helpers, compiled twice:
-// engine.cu instantiates them in namespace pgk64 (FP64 throughout, built
-// with --fmad=false for bit-exact parity) and engine_mixed.cu in namespace
-// pgkmx (mixed precision). The includer defines PGK_NS and PGK_MIXED.
+// kernels.cuh -- the engine's kernels and launch helpers, compiled four
+// times: engine.cu instantiates them in namespace pgk64 (FP64 throughout,
+// built with --fmad=false for bit-exact parity) and engine_mixed.cu in
+// namespace pgkmx (mixed precision), both for packs in the contiguous layout;
+// engine_tables.cu (pgk64t) and engine_mixed_tables.cu (pgkmxt) are the same
+// kernels for packs that give arrays through per-(block, component) pointer
+// tables. The includer defines PGK_NS, PGK_MIXED and (for the table forms)
+// PGK_TABLES; the table test then costs the contiguous kernels nothing.
 #ifndef PGK_NS
 #error "define PGK_NS before including kernels.cuh"
+#endif
+#ifndef PGK_TABLES
+#define PGK_TABLES 0
 #endif
 
 #include <cuda.h>  // CUtensorMap (types only; the encoder comes from the runtime)
@@ -77,20 +84,69 @@ __device__ __forceinline__ double dx_of(const Dims &d, int b, int dir) {
   return d.bdx ? __ldg(d.bdx + 3 * b + dir) : d.dx[dir];
 }
 
-__device__ __forceinline__ long long vidx(const Dims &d, int b, int v, int k, int j, int i) {
-  return (((long long)b * d.NF + v) * d.N3 + k) * (long long)d.N2 * d.N1 + (long long)j * d.N1 + i;
-}
 __device__ __forceinline__ long long cidx(const Dims &d, int b, int k, int j, int i) {
   return ((long long)b * d.N3 + k) * (long long)d.N2 * d.N1 + (long long)j * d.N1 + i;
 }
-__device__ __forceinline__ long long aidx(const Dims &d, int b, int c, int k, int j, int i) {
-  return (((long long)b * 3 + c) * d.N3 + k) * (long long)d.N2 * d.N1 + (long long)j * d.N1 + i;
+
+// Offset of cell (k, j, i) inside one component's [N3][N2][N1] array.
+__device__ __forceinline__ long long coff(const Dims &d, int k, int j, int i) {
+  return ((long long)k * d.N2 + j) * d.N1 + i;
+}
+// Base of component v of slot b of an array with nc components per slot: in
+// the table forms the pack's table entry when it gives one, else (and always
+// in the contiguous forms) the contiguous layout.
+template <class T, class Tab>
+__device__ __forceinline__ T *comp(const Dims &d, T *base, Tab *const *tab, int nc, int b, int v) {
+#if PGK_TABLES
+  if (tab) {
+    const unsigned long long a =
+        __ldg(reinterpret_cast<const unsigned long long *>(tab) + (long long)b * nc + v);
+    return reinterpret_cast<T *>(a);
+  }
+#else
+  (void)tab;
+#endif
+  return base + ((long long)b * nc + v) * d.ncell;
+}
+// The roles of Dims' tables: primitives, the task's conserved variables,
+// the RK starting state's, the launch's flux array, the three flux arrays,
+// alfven, efield and flag.
+template <class T> __device__ __forceinline__ T *a_prim(const Dims &d, T *P, int b, int v) {
+  return comp(d, P, d.tP, d.NF, b, v);
+}
+template <class T> __device__ __forceinline__ T *a_cons(const Dims &d, T *U, int b, int v) {
+  return comp(d, U, d.tU, d.NF, b, v);
+}
+template <class T> __device__ __forceinline__ T *a_cons0(const Dims &d, T *U, int b, int v) {
+  return comp(d, U, d.tUi, d.NF, b, v);
+}
+template <class T> __device__ __forceinline__ T *a_flux(const Dims &d, T *F, int b, int v) {
+  return comp(d, F, d.tF, d.NF, b, v);
+}
+template <class T> __device__ __forceinline__ T *a_flux1(const Dims &d, T *F, int b, int v) {
+  return comp(d, F, d.tF1, d.NF, b, v);
+}
+template <class T> __device__ __forceinline__ T *a_flux2(const Dims &d, T *F, int b, int v) {
+  return comp(d, F, d.tF2, d.NF, b, v);
+}
+template <class T> __device__ __forceinline__ T *a_flux3(const Dims &d, T *F, int b, int v) {
+  return comp(d, F, d.tF3, d.NF, b, v);
+}
+template <class T> __device__ __forceinline__ T *a_alfven(const Dims &d, T *A, int b, int c) {
+  return comp(d, A, d.tA, 3, b, c);
+}
+template <class T> __device__ __forceinline__ T *a_efield(const Dims &d, T *E, int b, int c) {
+  return comp(d, E, d.tE, 3, b, c);
+}
+template <class T> __device__ __forceinline__ T *a_flag(const Dims &d, T *G, int b) {
+  return comp(d, G, d.tG, 1, b, 0);
 }
 
 __device__ __forceinline__ void load_prim(const Dims &d, const PT *P, int b, int k, int j,
                                           int i, double out[NPRIM]) {
+  const long long o = coff(d, k, j, i);
 #pragma unroll
-  for (int s = 0; s < NPRIM; ++s) out[s] = d.pidx[s] >= 0 ? P[vidx(d, b, d.pidx[s], k, j, i)] : 0.0;
+  for (int s = 0; s < NPRIM; ++s) out[s] = d.pidx[s] >= 0 ? a_prim(d, P, b, d.pidx[s])[o] : 0.0;
 }
 
 // Cell-centre coordinate (origin + (idx + 1/2) dx, rounded step by step).
@@ -393,7 +449,7 @@ inline unsigned grid_for(long long n) {
 // FixPrimitive (primitive_fixer.cc:15-169), entire domain.
 // ---------------------------------------------------------------------------
 template <int MT>
-// With U non-null the kernel also computes the conserved variables of the
+// With with_cons set the kernel also computes the conserved variables of the
 // interior cells from the primitives it has just stored, which is what
 // CalculateConservative (the next task of the stage) would read back
 // (with_b = 0: conserved B left as is, see k_calc_cons).
@@ -401,7 +457,8 @@ template <int MT>
 // set to 0 here so that the stage needs no memset.
 __global__ void __launch_bounds__(kThreads, 4) k_fix_primitive(Dims d, pangu_params p, PT *P,
                                                             unsigned long long *cnt, double *U,
-                                                            int with_b, int *zero0, int *zero1) {
+                                                            int with_cons, int with_b, int *zero0,
+                                                            int *zero1) {
   pdl_grid_wait();
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -414,9 +471,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_fix_primitive(Dims d, pangu_par
   const double gam = p.adiabatic_index;
   constexpr double small = 1.0e-20;
   const double sigma_max_safe = kmax(p.sigma_max, small);
-  const long long q = vidx(d, b, 0, k, j, i);
-  const long long vs = d.ncell;
-  const double rho_before = kmax(P[q], small);
+  const long long o = coff(d, k, j, i);
+  const double rho_before = kmax(a_prim(d, P, b, 0)[o], small);
   double r = 1.0;
   double rho_floor, eng_floor;
   if (MT == MKS) {
@@ -484,17 +540,17 @@ __global__ void __launch_bounds__(kThreads, 4) k_fix_primitive(Dims d, pangu_par
     ent = (gam - 1.0) * e_excise * PGK_POW(p.dexcise, -gam);
     if (p.enable_heating) kel = e_excise;
   }
-  P[q] = pr;
-  P[q + vs] = pu;
-  P[q + 2 * vs] = u1;
-  P[q + 3 * vs] = u2;
-  P[q + 4 * vs] = u3;
-  P[q + d.pidx[ENT] * vs] = ent;
-  if (p.enable_heating) P[q + d.pidx[KEL] * vs] = kel;
+  a_prim(d, P, b, 0)[o] = pr;
+  a_prim(d, P, b, 1)[o] = pu;
+  a_prim(d, P, b, 2)[o] = u1;
+  a_prim(d, P, b, 3)[o] = u2;
+  a_prim(d, P, b, 4)[o] = u3;
+  a_prim(d, P, b, d.pidx[ENT])[o] = ent;
+  if (p.enable_heating) a_prim(d, P, b, d.pidx[KEL])[o] = kel;
   count(cnt, job_of(d, b), PANGU_CNT_RHO_FLOOR, hit_r);
   count(cnt, job_of(d, b), PANGU_CNT_ENG_FLOOR, hit_u);
   count(cnt, job_of(d, b), PANGU_CNT_LORENTZ_CAP, cap);
-  if (U && k >= d.ks && k <= d.ke && j >= d.js && j <= d.je && i >= d.is && i <= d.ie) {
+  if (with_cons && k >= d.ks && k <= d.ke && j >= d.js && j <= d.je && i >= d.is && i <= d.ie) {
     // the stored values, as a reload would see them
     double pf[NPRIM];
 #pragma unroll
@@ -512,7 +568,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_fix_primitive(Dims d, pangu_par
     flux_from_state(gam, pf, sf, g.sg, 0, f);
 #pragma unroll
     for (int v = 0; v < NPRIM; ++v)
-      if (d.pidx[v] >= 0 && (with_b || v < BX1 || v > BX3)) U[q + d.pidx[v] * vs] = f[v];
+      if (d.pidx[v] >= 0 && (with_b || v < BX1 || v > BX3)) a_cons(d, U, b, d.pidx[v])[o] = f[v];
   }
 }
 
@@ -540,7 +596,8 @@ __global__ void __launch_bounds__(kThreads) k_calc_cons(Dims d, pangu_params p, 
   flux_from_state(p.adiabatic_index, pc, s, g.sg, 0, f);
 #pragma unroll
   for (int v = 0; v < NPRIM; ++v)
-    if (d.pidx[v] >= 0 && (with_b || v < BX1 || v > BX3)) U[vidx(d, b, d.pidx[v], k, j, i)] = f[v];
+    if (d.pidx[v] >= 0 && (with_b || v < BX1 || v > BX3))
+      a_cons(d, U, b, d.pidx[v])[coff(d, k, j, i)] = f[v];
 }
 
 // ---------------------------------------------------------------------------
@@ -638,7 +695,7 @@ template <int MT, int DIR, int OPT>
 __device__ __forceinline__ void face_flux(const Dims &d, const pangu_params &p, int b, int k, int j,
                                           int i, const FT PL[NPRIM], const FT PR[NPRIM],
                                           double *F, double *alfven) {
-  const long long fo = vidx(d, b, 0, k, j, i);
+  const long long fo = coff(d, k, j, i);
   GeoT<FT> g;
   int ok;
   if ((MT == MKS || MT == BL) && DIR != 3) {
@@ -659,10 +716,10 @@ __device__ __forceinline__ void face_flux(const Dims &d, const pangu_params &p, 
     if (ok) geo_cast<MT>(g64, g);
   }
   if (!ok) {
-    alfven[aidx(d, b, DIR - 1, k, j, i)] = 0.0;
+    a_alfven(d, alfven, b, DIR - 1)[fo] = 0.0;
 #pragma unroll
     for (int s = 0; s < NPRIM; ++s)
-      if (d.pidx[s] >= 0) F[fo + d.pidx[s] * d.ncell] = 0.0;
+      if (d.pidx[s] >= 0) a_flux(d, F, b, d.pidx[s])[fo] = 0.0;
     return;
   }
   const FT gam = (FT)p.adiabatic_index;
@@ -676,7 +733,7 @@ __device__ __forceinline__ void face_flux(const Dims &d, const pangu_params &p, 
   const FT cmax = fabs(tmax(tmax(FT(0), vmaxL), vmaxR));
   const FT cmin = fabs(tmax(tmax(FT(0), -vminL), -vminR));
   const FT cms = tmax(cmax, cmin);
-  alfven[aidx(d, b, DIR - 1, k, j, i)] = cms;
+  a_alfven(d, alfven, b, DIR - 1)[fo] = cms;
   const bool hll = PGK_FLUX_HLL(p);
   const FT ihll = FT(1) / (cmax + cmin + FT(1e-20));
 #define PGD_FACE_COMPONENT(C)                                                         \
@@ -685,7 +742,7 @@ __device__ __forceinline__ void face_flux(const Dims &d, const pangu_params &p, 
     const FT fr = flux_component_t<C>(gam, PR, sR, sg, DIR);                          \
     const FT ul = flux_component_t<C>(gam, PL, sL, sg, 0);                            \
     const FT ur = flux_component_t<C>(gam, PR, sR, sg, 0);                            \
-    F[fo + d.pidx[C] * d.ncell] =                                                     \
+    a_flux(d, F, b, d.pidx[C])[fo] =                                                     \
         hll ? (cmax * fl + cmin * fr - cmax * cmin * (ur - ul)) * ihll                 \
             : FT(0.5) * (fl + fr - cms * (ur - ul));                                   \
   }
@@ -709,14 +766,14 @@ __device__ __forceinline__ void face_flux(const Dims &d, const pangu_params &p, 
                                           int i, const double PL[NPRIM], const double PR[NPRIM],
                                           double *F, double *alfven) {
   Geo g;
-  const long long fo = vidx(d, b, 0, k, j, i);
+  const long long fo = coff(d, k, j, i);
   if (!face_metric<MT>(d, p, DIR, b, k, j, i, g)) {
     // Singular code metric (theta = 0 exactly on a polar face): zero flux,
     // zero speed (the reference reads an unwritten inverse here).
-    alfven[aidx(d, b, DIR - 1, k, j, i)] = 0.0;
+    a_alfven(d, alfven, b, DIR - 1)[fo] = 0.0;
 #pragma unroll
     for (int s = 0; s < NPRIM; ++s)
-      if (d.pidx[s] >= 0) F[fo + d.pidx[s] * d.ncell] = 0.0;
+      if (d.pidx[s] >= 0) a_flux(d, F, b, d.pidx[s])[fo] = 0.0;
     return;
   }
   const double gam = p.adiabatic_index;
@@ -730,7 +787,7 @@ __device__ __forceinline__ void face_flux(const Dims &d, const pangu_params &p, 
   const double cmax = fabs(kmax(kmax(0., vmaxL), vmaxR));
   const double cmin = fabs(kmax(kmax(0., -vminL), -vminR));
   const double cms = kmax(cmax, cmin);
-  alfven[aidx(d, b, DIR - 1, k, j, i)] = cms;
+  a_alfven(d, alfven, b, DIR - 1)[fo] = cms;
   const bool hll = PGK_FLUX_HLL(p);
 #define PGD_FACE_COMPONENT(C)                                                         \
   if (d.pidx[C] >= 0) {                                                               \
@@ -738,7 +795,7 @@ __device__ __forceinline__ void face_flux(const Dims &d, const pangu_params &p, 
     const double fr = flux_component<C>(gam, PR, sR, sg, DIR);                        \
     const double ul = flux_component<C>(gam, PL, sL, sg, 0);                          \
     const double ur = flux_component<C>(gam, PR, sR, sg, 0);                          \
-    F[fo + d.pidx[C] * d.ncell] =                                                     \
+    a_flux(d, F, b, d.pidx[C])[fo] =                                                     \
         hll ? (cmax * fl + cmin * fr - cmax * cmin * (ur - ul)) / (cmax + cmin + 1e-20) \
             : 0.5 * (fl + fr - cms * (ur - ul));                                      \
   }
@@ -766,12 +823,12 @@ __device__ __forceinline__ void face_flux_split(const Dims &d, const pangu_param
                                                 int j, int i, double *sl, const double *sr,
                                                 double *su, int ss, double *F, double *alfven) {
   Geo g;
-  const long long fo = vidx(d, b, 0, k, j, i);
+  const long long fo = coff(d, k, j, i);
   if (!face_metric<MT>(d, p, DIR, b, k, j, i, g)) {
-    alfven[aidx(d, b, DIR - 1, k, j, i)] = 0.0;
+    a_alfven(d, alfven, b, DIR - 1)[fo] = 0.0;
 #pragma unroll
     for (int s = 0; s < NPRIM; ++s)
-      if (d.pidx[s] >= 0) F[fo + d.pidx[s] * d.ncell] = 0.0;
+      if (d.pidx[s] >= 0) a_flux(d, F, b, d.pidx[s])[fo] = 0.0;
     return;
   }
   const double gam = p.adiabatic_index;
@@ -813,7 +870,7 @@ __device__ __forceinline__ void face_flux_split(const Dims &d, const pangu_param
   const double cmax = fabs(kmax(kmax(0., vmaxL), vmaxR));
   const double cmin = fabs(kmax(kmax(0., -vminL), -vminR));
   const double cms = kmax(cmax, cmin);
-  alfven[aidx(d, b, DIR - 1, k, j, i)] = cms;
+  a_alfven(d, alfven, b, DIR - 1)[fo] = cms;
   const bool hll = PGK_FLUX_HLL(p);
 #define PGD_RIGHT_COMPONENT(C)                                                        \
   if (d.pidx[C] >= 0) {                                                               \
@@ -821,7 +878,7 @@ __device__ __forceinline__ void face_flux_split(const Dims &d, const pangu_param
     const double fr = flux_component<C>(gam, P, st, sg, DIR);                         \
     const double ul = su[C * ss];                                                     \
     const double ur = flux_component<C>(gam, P, st, sg, 0);                           \
-    F[fo + d.pidx[C] * d.ncell] =                                                     \
+    a_flux(d, F, b, d.pidx[C])[fo] =                                                     \
         hll ? (cmax * fl + cmin * fr - cmax * cmin * (ur - ul)) / (cmax + cmin + 1e-20) \
             : 0.5 * (fl + fr - cms * (ur - ul));                                      \
   }
@@ -890,7 +947,7 @@ __global__ void __launch_bounds__(kFluxThreads, flux_blocks(MT)) k_flux_x1(Dims 
     for (int s = 0; s < NPRIM; ++s) {
       FT up = 0, lo = 0;
       if (d.pidx[s] >= 0 && active)
-        recon_cell(use_mc, P + vidx(d, b, d.pidx[s], k, j, c), 1, up, lo);
+        recon_cell(use_mc, a_prim(d, P, b, d.pidx[s]) + coff(d, k, j, c), 1, up, lo);
       fsm[s * ss + t] = up;
       fsm[(NPRIM + s) * ss + t] = lo;
     }
@@ -906,7 +963,7 @@ __global__ void __launch_bounds__(kFluxThreads, flux_blocks(MT)) k_flux_x1(Dims 
   for (int s = 0; s < NPRIM; ++s) {
     FT up = 0, lo = 0;
     if (d.pidx[s] >= 0 && active)
-      recon_cell(use_mc, P + vidx(d, b, d.pidx[s], k, j, c), 1, up, lo);
+      recon_cell(use_mc, a_prim(d, P, b, d.pidx[s]) + coff(d, k, j, c), 1, up, lo);
     PL[s] = __shfl_up_sync(0xffffffffu, up, 1);
     PR[s] = lo;
   }
@@ -957,7 +1014,7 @@ __device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_param
       for (int s = 0; s < NPRIM; ++s) {
         FT up = 0, lo;
         if (d.pidx[s] >= 0)
-          recon_cell(use_mc, P + vidx(d, b, d.pidx[s], kk, jj, i), stride, up, lo);
+          recon_cell(use_mc, a_prim(d, P, b, d.pidx[s]) + coff(d, kk, jj, i), stride, up, lo);
         carry[s * ss] = up;
       }
     }
@@ -967,7 +1024,7 @@ __device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_param
       for (int s = 0; s < NPRIM; ++s) {
         FT up = 0, lo = 0;
         if (d.pidx[s] >= 0)
-          recon_cell(use_mc, P + vidx(d, b, d.pidx[s], kk, jj, i), stride, up, lo);
+          recon_cell(use_mc, a_prim(d, P, b, d.pidx[s]) + coff(d, kk, jj, i), stride, up, lo);
         next[s * ss] = up;
         lower[s * ss] = lo;
       }
@@ -986,7 +1043,7 @@ __device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_param
 #pragma unroll
     for (int s = 0; s < NPRIM; ++s) {
       FT up = 0, lo;
-      if (d.pidx[s] >= 0) recon_cell(use_mc, P + vidx(d, b, d.pidx[s], kk, jj, i), stride, up, lo);
+      if (d.pidx[s] >= 0) recon_cell(use_mc, a_prim(d, P, b, d.pidx[s]) + coff(d, kk, jj, i), stride, up, lo);
       carry[s] = up;
     }
   }
@@ -998,7 +1055,7 @@ __device__ __forceinline__ void flux_march_body(const Dims &d, const pangu_param
       up[s] = 0.0;
       PR[s] = 0.0;
       if (d.pidx[s] >= 0)
-        recon_cell(use_mc, P + vidx(d, b, d.pidx[s], kk, jj, i), stride, up[s], PR[s]);
+        recon_cell(use_mc, a_prim(d, P, b, d.pidx[s]) + coff(d, kk, jj, i), stride, up[s], PR[s]);
     }
     face_flux<MT, DIR, OPT>(d, p, b, kk, jj, i, carry, PR, F, alfven);
 #pragma unroll
@@ -1041,7 +1098,7 @@ __device__ __forceinline__ void flux_tile_body(const Dims &d, const pangu_params
 #pragma unroll
       for (int s = 0; s < NPRIM; ++s) {
         FT up = 0, lo = 0;
-        if (d.pidx[s] >= 0) recon_cell(use_mc, P + vidx(d, b, d.pidx[s], kk, jj, i), stride, up, lo);
+        if (d.pidx[s] >= 0) recon_cell(use_mc, a_prim(d, P, b, d.pidx[s]) + coff(d, kk, jj, i), stride, up, lo);
         sup[cr][s][lane] = up;
         slo[cr][s][lane] = lo;
       }
@@ -1340,23 +1397,23 @@ __global__ void __launch_bounds__(kThreads) k_ct_emf(Dims d, const double *F1, c
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, d.ks, d.ke + o3, d.js, d.je + o2, d.is, d.ie + o1, b, k, j, i)) return;
   b = slot_of(d, b);
-  const long long sj = d.N1, sk = (long long)d.N1 * d.N2;
+  const long long sj = d.N1, sk = (long long)d.N1 * d.N2, o = coff(d, k, j, i);
   double e1 = 0.0, e2 = 0.0, e3 = 0.0;
   if (o2 && o3) {
-    const long long a = vidx(d, b, BX3, k, j, i), c = vidx(d, b, BX2, k, j, i);
-    e1 = 0.25 * ((F2[a] + F2[a - sk]) - (F3[c] + F3[c - sj]));
+    const double *a = a_flux2(d, F2, b, BX3) + o, *c = a_flux3(d, F3, b, BX2) + o;
+    e1 = 0.25 * ((a[0] + a[-sk]) - (c[0] + c[-sj]));
   }
   if (o3 && o1) {
-    const long long a = vidx(d, b, BX1, k, j, i), c = vidx(d, b, BX3, k, j, i);
-    e2 = 0.25 * ((F3[a] + F3[a - 1]) - (F1[c] + F1[c - sk]));
+    const double *a = a_flux3(d, F3, b, BX1) + o, *c = a_flux1(d, F1, b, BX3) + o;
+    e2 = 0.25 * ((a[0] + a[-1]) - (c[0] + c[-sk]));
   }
   if (o1 && o2) {
-    const long long a = vidx(d, b, BX2, k, j, i), c = vidx(d, b, BX1, k, j, i);
-    e3 = 0.25 * ((F1[a] + F1[a - sj]) - (F2[c] + F2[c - 1]));
+    const double *a = a_flux1(d, F1, b, BX2) + o, *c = a_flux2(d, F2, b, BX1) + o;
+    e3 = 0.25 * ((a[0] + a[-sj]) - (c[0] + c[-1]));
   }
-  E[aidx(d, b, 0, k, j, i)] = e1;
-  E[aidx(d, b, 1, k, j, i)] = e2;
-  E[aidx(d, b, 2, k, j, i)] = e3;
+  a_efield(d, E, b, 0)[o] = e1;
+  a_efield(d, E, b, 1)[o] = e2;
+  a_efield(d, E, b, 2)[o] = e3;
 }
 
 // Face-B overwrite (constrained_transport.cc:78-127) of every direction in
@@ -1372,27 +1429,23 @@ __global__ void __launch_bounds__(kThreads) k_ct_faces(Dims d, double *F1, doubl
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, d.ks, d.ke + o3, d.js, d.je + o2, d.is, d.ie + o1, b, k, j, i)) return;
   b = slot_of(d, b);
-  const long long sj = d.N1, sk = (long long)d.N1 * d.N2;
-  const long long e0 = aidx(d, b, 0, k, j, i), e1 = aidx(d, b, 1, k, j, i),
-                  e2 = aidx(d, b, 2, k, j, i);
+  const long long sj = d.N1, sk = (long long)d.N1 * d.N2, o = coff(d, k, j, i);
+  const double *Ea = a_efield(d, E, b, 0) + o, *Eb = a_efield(d, E, b, 1) + o, *Ec = a_efield(d, E, b, 2) + o;
   const bool in_i = i <= d.ie, in_j = j <= d.je, in_k = k <= d.ke;
   if (in_j && in_k) {
-    double *F = F1;
-    if (o1) F[vidx(d, b, BX1, k, j, i)] = 0;
-    if (E2) F[vidx(d, b, BX3, k, j, i)] = -0.5 * (E[e1] + E[e1 + sk]);
-    if (E3) F[vidx(d, b, BX2, k, j, i)] = 0.5 * (E[e2] + E[e2 + sj]);
+    if (o1) a_flux1(d, F1, b, BX1)[o] = 0;
+    if (E2) a_flux1(d, F1, b, BX3)[o] = -0.5 * (Eb[0] + Eb[sk]);
+    if (E3) a_flux1(d, F1, b, BX2)[o] = 0.5 * (Ec[0] + Ec[sj]);
   }
   if (d.ndim >= 2 && in_i && in_k) {
-    double *F = F2;
-    if (E1) F[vidx(d, b, BX3, k, j, i)] = 0.5 * (E[e0] + E[e0 + sk]);
-    if (o2) F[vidx(d, b, BX2, k, j, i)] = 0.;
-    if (E3) F[vidx(d, b, BX1, k, j, i)] = -0.5 * (E[e2] + E[e2 + 1]);
+    if (E1) a_flux2(d, F2, b, BX3)[o] = 0.5 * (Ea[0] + Ea[sk]);
+    if (o2) a_flux2(d, F2, b, BX2)[o] = 0.;
+    if (E3) a_flux2(d, F2, b, BX1)[o] = -0.5 * (Ec[0] + Ec[1]);
   }
   if (d.ndim == 3 && in_i && in_j) {
-    double *F = F3;
-    if (E1) F[vidx(d, b, BX2, k, j, i)] = -0.5 * (E[e0] + E[e0 + sj]);
-    if (E2) F[vidx(d, b, BX1, k, j, i)] = 0.5 * (E[e1] + E[e1 + 1]);
-    if (o3) F[vidx(d, b, BX3, k, j, i)] = 0;
+    if (E1) a_flux3(d, F3, b, BX2)[o] = -0.5 * (Ea[0] + Ea[sj]);
+    if (E2) a_flux3(d, F3, b, BX1)[o] = 0.5 * (Eb[0] + Eb[1]);
+    if (o3) a_flux3(d, F3, b, BX3)[o] = 0;
   }
 }
 
@@ -1410,19 +1463,24 @@ __global__ void __launch_bounds__(kThreads) k_flux_div_update(Dims d, const doub
   // b here runs over (active block, variable) pairs
   const int v = b % d.NF;
   b = slot_of(d, b / d.NF);
-  const long long q = vidx(d, b, v, k, j, i);
+  const long long q = coff(d, k, j, i);
   const double dx0 = dx_of(d, b, 0), dx1 = dx_of(d, b, 1), dx2 = dx_of(d, b, 2);
   const double A1 = MUL(dx1, dx2), A2 = MUL(dx0, dx2), A3 = MUL(dx0, dx1);
   const double V = MUL(MUL(dx0, dx1), dx2);
-  double du = SUB(MUL(A1, F1[q + 1]), MUL(A1, F1[q]));
-  if (d.ndim >= 2) du = ADD(du, SUB(MUL(A2, F2[q + d.N1]), MUL(A2, F2[q])));
+  const double *f1 = a_flux1(d, F1, b, v) + q;
+  double du = SUB(MUL(A1, f1[1]), MUL(A1, f1[0]));
+  if (d.ndim >= 2) {
+    const double *f2 = a_flux2(d, F2, b, v) + q;
+    du = ADD(du, SUB(MUL(A2, f2[d.N1]), MUL(A2, f2[0])));
+  }
   if (d.ndim == 3) {
     const long long sk = (long long)d.N1 * d.N2;
-    du = ADD(du, SUB(MUL(A3, F3[q + sk]), MUL(A3, F3[q])));
+    const double *f3 = a_flux3(d, F3, b, v) + q;
+    du = ADD(du, SUB(MUL(A3, f3[sk]), MUL(A3, f3[0])));
   }
   const double dudt = DIV(-du, V);
   const double bdt = MUL(beta, dt[job_of(d, b)]);
-  Uout[q] = ADD(Uinit[q], MUL(bdt, dudt));
+  a_cons(d, Uout, b, v)[q] = ADD(a_cons0(d, Uinit, b, v)[q], MUL(bdt, dudt));
 }
 
 // ---------------------------------------------------------------------------
@@ -1438,10 +1496,8 @@ __global__ void __launch_bounds__(kThreads) k_exchange(Dims d, long long n, cons
   long long db, dof, sb, sof;
   split_cell(dc, d.ncell, db, dof);
   split_cell(sc, d.ncell, sb, sof);
-  const long long dp = db * d.NF * d.ncell + dof;
-  const long long sp = sb * d.NF * d.ncell + sof;
-  for (int v = 0; v < d.NF; ++v) P[dp + v * d.ncell] = P[sp + v * d.ncell];
-  if (flag) flag[dc] = flag[sc];
+  for (int v = 0; v < d.NF; ++v) a_prim(d, P, (int)db, v)[dof] = a_prim(d, P, (int)sb, v)[sof];
+  if (flag || d.tG) a_flag(d, flag, (int)db)[dof] = a_flag(d, flag, (int)sb)[sof];
 }
 
 // Halo messages of a sharded mesh: the cells of the exchange whose other end
@@ -1457,10 +1513,9 @@ __global__ void __launch_bounds__(kThreads) k_halo_pack(Dims d, long long n, con
   const long long c = cells[t];
   long long b, off;
   split_cell(c, d.ncell, b, off);
-  const long long q = b * d.NF * d.ncell + off;
   double *o = buf + t * (d.NF + 1);
-  for (int v = 0; v < d.NF; ++v) o[v] = (double)P[q + v * d.ncell];
-  o[d.NF] = flag ? flag[c] : 0.0;
+  for (int v = 0; v < d.NF; ++v) o[v] = (double)a_prim(d, P, (int)b, v)[off];
+  o[d.NF] = (flag || d.tG) ? a_flag(d, flag, (int)b)[off] : 0.0;
 }
 
 __global__ void __launch_bounds__(kThreads) k_halo_unpack(Dims d, long long n,
@@ -1472,10 +1527,9 @@ __global__ void __launch_bounds__(kThreads) k_halo_unpack(Dims d, long long n,
   const long long c = cells[t];
   long long b, off;
   split_cell(c, d.ncell, b, off);
-  const long long q = b * d.NF * d.ncell + off;
   const double *o = buf + t * (d.NF + 1);
-  for (int v = 0; v < d.NF; ++v) P[q + v * d.ncell] = (PT)o[v];
-  if (flag) flag[c] = o[d.NF];
+  for (int v = 0; v < d.NF; ++v) a_prim(d, P, (int)b, v)[off] = (PT)o[v];
+  if (flag || d.tG) a_flag(d, flag, (int)b)[off] = o[d.NF];
 }
 
 // ---------------------------------------------------------------------------
@@ -1484,10 +1538,9 @@ __global__ void __launch_bounds__(kThreads) k_halo_unpack(Dims d, long long n,
 // step like the metric itself.
 // ---------------------------------------------------------------------------
 template <int MT>
-__device__ __forceinline__ void christoffel(const Dims &d, const pangu_params &p, int b, int k,
-                                            int j, int i, const Geo &g, double conn[4][4][4]) {
+__device__ __forceinline__ void metric_derivs(const Dims &d, const pangu_params &p, int b, int k,
+                                              int j, int i, double dg[4][4][4]) {
   constexpr double twod = 2.0 * 1.0e-5;
-  double dg[4][4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -1514,6 +1567,12 @@ __device__ __forceinline__ void christoffel(const Dims &d, const pangu_params &p
 #pragma unroll
       for (int c = 0; c < 4; ++c) dg[dir][r][c] = DIV(SUB(gp[r][c], gm[r][c]), twod);
   }
+}
+
+// Gamma^a_jk = g^al (d_j g_lk + d_k g_lj - d_l g_jk) / 2 in the order of
+// christoffel.h:120-146, with every term.
+__device__ __forceinline__ void connection(const double dg[4][4][4], const Geo &g,
+                                           double conn[4][4][4]) {
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -1528,6 +1587,14 @@ __device__ __forceinline__ void christoffel(const Dims &d, const pangu_params &p
         }
         conn[a][jj][kk] = v;
       }
+}
+
+template <int MT>
+__device__ __forceinline__ void christoffel(const Dims &d, const pangu_params &p, int b, int k,
+                                            int j, int i, const Geo &g, double conn[4][4][4]) {
+  double dg[4][4][4];
+  metric_derivs<MT>(d, p, b, k, j, i, dg);
+  connection(dg, g, conn);
 }
 
 // Geometric source of one interior cell: U += (T^r_c Gamma^c_{dir r})
@@ -1545,10 +1612,10 @@ __device__ __forceinline__ void source_cell(const Dims &d, const pangu_params &p
     // primitives and the tabulated FP64 metric rounded once; the increment is
     // accumulated into the FP64 conserved variables.
     constexpr TabLayout L = tab_layout(MT);
-    const long long vs = d.ncell, q0 = vidx(d, b, 0, k, j, i);
+    const long long q0 = coff(d, k, j, i);
     FT pf[NPRIM];
 #pragma unroll
-    for (int v = 0; v < NPRIM; ++v) pf[v] = d.pidx[v] >= 0 ? P[q0 + d.pidx[v] * vs] : FT(0);
+    for (int v = 0; v < NPRIM; ++v) pf[v] = d.pidx[v] >= 0 ? a_prim(d, P, b, d.pidx[v])[q0] : FT(0);
     GeoT<FT> gf;
     geo_cast<MT>(g, gf);
     StateT<FT> sf;
@@ -1573,7 +1640,7 @@ __device__ __forceinline__ void source_cell(const Dims &d, const pangu_params &p
             con += T * (FT)__ldg(cn + L.conn[c][dir][r] * plane);
           }
       const int v = dir == 0 ? d.pidx[ENY] : d.pidx[UX1] + dir - 1;
-      U[q0 + v * vs] += (double)con * sg * bdt;
+      a_cons(d, U, b, v)[q0] += (double)con * sg * bdt;
     }
     return;
   }
@@ -1600,8 +1667,7 @@ __device__ __forceinline__ void source_cell(const Dims &d, const pangu_params &p
         for (int c = 0; c < 4; ++c)
           if (L.conn[c][dir][r] >= 0) con += T[r][c] * __ldg(cn + L.conn[c][dir][r] * plane);
       const int v = dir == 0 ? d.pidx[ENY] : d.pidx[UX1] + dir - 1;
-      const long long q = vidx(d, b, v, k, j, i);
-      U[q] += con * sg * bdt;
+      a_cons(d, U, b, v)[coff(d, k, j, i)] += con * sg * bdt;
     }
   } else {
     double conn[4][4][4];
@@ -1614,8 +1680,7 @@ __device__ __forceinline__ void source_cell(const Dims &d, const pangu_params &p
 #pragma unroll
         for (int c = 0; c < 4; ++c) con += T[r][c] * conn[c][dir][r];
       const int v = dir == 0 ? d.pidx[ENY] : d.pidx[UX1] + dir - 1;
-      const long long q = vidx(d, b, v, k, j, i);
-      U[q] += con * sg * bdt;
+      a_cons(d, U, b, v)[coff(d, k, j, i)] += con * sg * bdt;
     }
   }
 }
@@ -1734,30 +1799,30 @@ template <int MT>
 __device__ __forceinline__ void heat_cell(const Dims &d, const pangu_params &p, PT *P,
                                           const double *U, int b, int k, int j, int i,
                                           const Geo &g) {
-  const long long q = vidx(d, b, 0, k, j, i);
-  const long long vs = d.ncell;
-  const double cr = U[q];
+  const long long q = coff(d, k, j, i);
+  const double cr = a_cons(d, U, b, 0)[q];
   const HeatParams hp = {p.model, p.adiabatic_index, p.gamma_p, p.gamma_e, p.fel_constant,
                          p.ratio_min, p.ratio_max, p.limit_kel, p.suppress_highb_heat,
                          p.enforce_positive_dissipation};
 #if PGK_MIXED
   FT pc[NPRIM];
 #pragma unroll
-  for (int v = 0; v < NPRIM; ++v) pc[v] = d.pidx[v] >= 0 ? P[q + d.pidx[v] * vs] : FT(0);
+  for (int v = 0; v < NPRIM; ++v) pc[v] = d.pidx[v] >= 0 ? a_prim(d, P, b, d.pidx[v])[q] : FT(0);
   GeoT<FT> gf;
   geo_cast<MT>(g, gf);
   StateT<FT> s;
   calc_state_t<MT>(pc, gf, s);
-  P[q + d.pidx[KEL] * vs] = heating_apply_t<FT>(hp, pc[RHO], pc[ENY], s.bsq,
-                                                (FT)(U[q + d.pidx[ENT] * vs] / cr), pc[ENT],
-                                                (FT)(U[q + d.pidx[KEL] * vs] / cr));
+  a_prim(d, P, b, d.pidx[KEL])[q] =
+      heating_apply_t<FT>(hp, pc[RHO], pc[ENY], s.bsq, (FT)(a_cons(d, U, b, d.pidx[ENT])[q] / cr),
+                          pc[ENT], (FT)(a_cons(d, U, b, d.pidx[KEL])[q] / cr));
 #else
   double pc[NPRIM];
   load_prim(d, P, b, k, j, i, pc);
   State s;
   calc_state<MT>(pc, g, s);
-  P[q + d.pidx[KEL] * vs] = heating_apply(hp, pc[RHO], pc[ENY], s.bsq, U[q + d.pidx[ENT] * vs] / cr,
-                                          pc[ENT], U[q + d.pidx[KEL] * vs] / cr);
+  a_prim(d, P, b, d.pidx[KEL])[q] =
+      heating_apply(hp, pc[RHO], pc[ENY], s.bsq, a_cons(d, U, b, d.pidx[ENT])[q] / cr, pc[ENT],
+                    a_cons(d, U, b, d.pidx[KEL])[q] / cr);
 #endif
 }
 
@@ -1798,20 +1863,19 @@ __device__ __forceinline__ void c2p_inputs(const Dims &d, const pangu_params &p,
                                            const double *U, int b, int k, int j, int i,
                                            const Geo &g, double UH[9], double PH[9],
                                            bool write_b) {
-  const long long q = vidx(d, b, 0, k, j, i);
-  const long long vs = d.ncell;
+  const long long q = coff(d, k, j, i);
   double C[9];
 #pragma unroll
   for (int s = 0; s < 9; ++s) {
-    C[s] = d.pidx[s] >= 0 ? U[q + d.pidx[s] * vs] : 0.0;
-    PH[s] = d.pidx[s] >= 0 ? P[q + d.pidx[s] * vs] : 0.0;
+    C[s] = d.pidx[s] >= 0 ? a_cons(d, U, b, d.pidx[s])[q] : 0.0;
+    PH[s] = d.pidx[s] >= 0 ? a_prim(d, P, b, d.pidx[s])[q] : 0.0;
   }
   const double isg = 1.0 / g.sg;
   const double aisg = g.alpha * isg;
   if (p.enable_B && write_b) {
-    P[q + d.pidx[BX1] * vs] = C[BX1] * isg;
-    P[q + d.pidx[BX2] * vs] = C[BX2] * isg;
-    P[q + d.pidx[BX3] * vs] = C[BX3] * isg;
+    a_prim(d, P, b, d.pidx[BX1])[q] = C[BX1] * isg;
+    a_prim(d, P, b, d.pidx[BX2])[q] = C[BX2] * isg;
+    a_prim(d, P, b, d.pidx[BX3])[q] = C[BX3] * isg;
   }
   UH[RHO] = aisg * C[RHO];
   UH[ENY] = aisg * (C[ENY] - C[RHO]);
@@ -1826,13 +1890,12 @@ __device__ __forceinline__ void c2p_inputs(const Dims &d, const pangu_params &p,
 
 __device__ __forceinline__ void c2p_write(const Dims &d, PT *P, int b, int k, int j, int i,
                                           const double PH[9]) {
-  const long long q = vidx(d, b, 0, k, j, i);
-  const long long vs = d.ncell;
-  P[q] = PH[RHO];
-  P[q + vs] = PH[ENY];
-  P[q + 2 * vs] = PH[UX1];
-  P[q + 3 * vs] = PH[UX2];
-  P[q + 4 * vs] = PH[UX3];
+  const long long q = coff(d, k, j, i);
+  a_prim(d, P, b, 0)[q] = PH[RHO];
+  a_prim(d, P, b, 1)[q] = PH[ENY];
+  a_prim(d, P, b, 2)[q] = PH[UX1];
+  a_prim(d, P, b, 3)[q] = PH[UX2];
+  a_prim(d, P, b, 4)[q] = PH[UX3];
 }
 
 // Recovery, first pass: Kastaun (robuster), or Scheme2D of the chain. Cells
@@ -1861,7 +1924,7 @@ __global__ void __launch_bounds__(kRecoveryThreads, 7) k_recovery(Dims d, pangu_
     const bool exc = sqrt(0.5 * (rad2 - a2 + sqrt(sa))) < p.r_excise;
     count(cnt, job_of(d, b), PANGU_CNT_EXCISED, exc);
     if (exc) {
-      if (!robuster) flag[fc] = 0;
+      if (!robuster) a_flag(d, flag, b)[fc - (long long)b * d.ncell] = 0;
       return;
     }
   }
@@ -1880,7 +1943,7 @@ __global__ void __launch_bounds__(kRecoveryThreads, 7) k_recovery(Dims d, pangu_
     const bool ok = invert_2d<MT>(UH, PH, gam, g, hs) == 0;
     count(cnt, job_of(d, b), PANGU_CNT_C2P_2D, ok);
     append(nretry, retry, !ok, fc);
-    flag[fc] = ok ? 1.0 : 0.0;
+    a_flag(d, flag, b)[fc - (long long)b * d.ncell] = ok ? 1.0 : 0.0;
     if (!ok) return;
   }
   c2p_write(d, P, b, k, j, i, PH);
@@ -1924,7 +1987,7 @@ __global__ void __launch_bounds__(kThreads) k_recovery_retry(Dims d, pangu_param
       count(cnt, job_of(d, b), PANGU_CNT_C2P_1D, ok);
       count(cnt, job_of(d, b), PANGU_CNT_C2P_FAIL, !ok);
     }
-    flag[fc] = ok ? 1.0 : 0.0;
+    a_flag(d, flag, b)[fc - (long long)b * d.ncell] = ok ? 1.0 : 0.0;
     c2p_write(d, P, b, k, j, i, PH);
     if (fix) append(nfix, fix, !ok, fc);
   }
@@ -1942,7 +2005,7 @@ __global__ void __launch_bounds__(kThreads) k_fixrec_scan(Dims d, pangu_params p
   if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
   b = slot_of(d, b);
   const long long fc = cidx(d, b, k, j, i);
-  if (flag[fc] != 0) return;
+  if (a_flag(d, flag, b)[coff(d, k, j, i)] != 0) return;
   if (p.metric_type == PANGU_METRIC_CKS) {
     const double x = xc(d, b, 0, i), y = xc(d, b, 1, j), z = xc(d, b, 2, k);
     const double a2 = p.a * p.a;
@@ -1967,11 +2030,12 @@ __global__ void __launch_bounds__(kThreads) k_fixrec_compute(Dims d, const int *
     const long long b = fc / d.ncell;
     const long long c = fc - b * d.ncell;
     const long long sj = (long long)off2 * d.N1;
-    auto fl = [&](long long o) { return (int)flag[fc + o]; };
+    const double *fb = a_flag(d, flag, (int)b) + c;
+    auto fl = [&](long long o) { return (int)fb[o]; };
     const int pf1 = fl(sj - 1), pf2 = fl(sj), pf3 = fl(sj + 1), pf4 = fl(1);
     const int pf5 = fl(-sj + 1), pf6 = fl(-sj), pf7 = fl(-sj - 1), pf8 = fl(-1);
     for (int v = 0; v < d.NF; ++v) {
-      const PT *q = P + (b * d.NF + v) * d.ncell + c;
+      const PT *q = a_prim(d, P, (int)b, v) + c;
       double val;
       if (pf2 && pf4 && pf6 && pf8)
         val = 0.25 * (q[sj] + q[-sj] + q[-1] + q[1]);
@@ -1997,9 +2061,9 @@ __global__ void __launch_bounds__(kThreads) k_fixrec_write(Dims d, const int *co
     const long long fc = list[t];
     const long long b = fc / d.ncell;
     const long long c = fc - b * d.ncell;
-    for (int v = 0; v < d.NF; ++v) P[(b * d.NF + v) * d.ncell + c] = vals[t * d.NF + v];
-    for (int v = 2; v < 5; ++v) P[(b * d.NF + v) * d.ncell + c] = 0.;
-    flag[fc] = 1;
+    for (int v = 0; v < d.NF; ++v) a_prim(d, P, (int)b, v)[c] = vals[t * d.NF + v];
+    for (int v = 2; v < 5; ++v) a_prim(d, P, (int)b, v)[c] = 0.;
+    a_flag(d, flag, (int)b)[c] = 1;
     count(cnt, job_of(d, (int)b), PANGU_CNT_FIXRECOVERY, true);
   }
 }
@@ -2045,20 +2109,20 @@ __global__ void __launch_bounds__(kThreads) k_bcs(Dims d, int enable_B, PT *P,
     }
   }
   if (!ghost) return;
-  const long long dc = cidx(d, b, idx[2], idx[1], idx[0]);
-  const long long sc = cidx(d, b, src[2], src[1], src[0]);
-  const long long base = (long long)b * (d.NF - 1) * d.ncell;
+  const long long dc = coff(d, idx[2], idx[1], idx[0]);
+  const long long sc = coff(d, src[2], src[1], src[0]);
   for (int v = 0; v < d.NF; ++v) {
-    double val = P[base + sc + v * d.ncell];
+    PT *pv = a_prim(d, P, b, v);
+    double val = pv[sc];
 #pragma unroll
     for (int dir = 0; dir < 3; ++dir) {
       const bool vel = v == d.pidx[UX1] + dir;
       const bool mag = enable_B && v == d.pidx[BX1] + dir;
       if (flip[dir] && (vel || mag)) val = -val;
     }
-    P[base + dc + v * d.ncell] = val;
+    pv[dc] = val;
   }
-  if (flag) flag[dc] = flag[sc];
+  if (flag || d.tG) a_flag(d, flag, b)[dc] = a_flag(d, flag, b)[sc];
 }
 
 // ---------------------------------------------------------------------------
@@ -2105,7 +2169,7 @@ __device__ __forceinline__ void dt_reduce_cta(const Dims &d, double cfl, const d
 #pragma unroll
     for (int dir = 0; dir < 3; ++dir) {
       if (!act[dir]) continue;
-      const double dt = cdx[dir] / alfven[aidx(d, b, dir, k, j, i)];
+      const double dt = cdx[dir] / a_alfven(d, alfven, b, dir)[coff(d, k, j, i)];
       if (dt == dt) {
         const unsigned long long key = dt_key(dt);
         m[dir] = key < m[dir] ? key : m[dir];
@@ -2321,10 +2385,10 @@ __global__ void __launch_bounds__(kThreads) k_gen_cells(Dims d, pangu_params p, 
     }
   }
   pr[KEL] = p.fel_0 * pr[ENT];
-  const long long q = vidx(d, b, 0, k, j, i);
+  const long long q = coff(d, k, j, i);
 #pragma unroll
   for (int v = 0; v < NPRIM; ++v)
-    if (d.pidx[v] >= 0) P[q + d.pidx[v] * d.ncell] = (PT)pr[v];
+    if (d.pidx[v] >= 0) a_prim(d, P, b, d.pidx[v])[q] = (PT)pr[v];
 }
 
 // Torus: density and energy divided by the maximum density (all cells).
@@ -2336,9 +2400,10 @@ __global__ void __launch_bounds__(kThreads) k_gen_normalize(Dims d, PT *P,
   if (!box_index(t, d.NB, 0, d.N3 - 1, 0, d.N2 - 1, 0, d.N1 - 1, bb, k, j, i)) return;
   const int b = slot_of(d, bb);
   const double rhomax = __longlong_as_double((long long)red[0]);
-  const long long q = vidx(d, b, 0, k, j, i);
-  P[q] = (PT)((double)P[q] / rhomax);
-  P[q + d.ncell] = (PT)((double)P[q + d.ncell] / rhomax);
+  const long long q = coff(d, k, j, i);
+  PT *p0 = a_prim(d, P, b, 0), *p1 = a_prim(d, P, b, 1);
+  p0[q] = (PT)((double)p0[q] / rhomax);
+  p1[q] = (PT)((double)p1[q] / rhomax);
 }
 
 // Torus field (interior cells): A_phi = max(<rho> - cut, 0) at cell corners,
@@ -2351,8 +2416,9 @@ __global__ void __launch_bounds__(kThreads) k_gen_bfield(Dims d, pangu_params p,
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, bb, k, j, i)) return;
   const int b = slot_of(d, bb);
-  const long long q = vidx(d, b, 0, k, j, i);
-  auto rho = [&](int jj, int ii) -> double { return P[q + (long long)(jj - j) * d.N1 + (ii - i)]; };
+  const long long q = coff(d, k, j, i);
+  const PT *p0 = a_prim(d, P, b, 0);
+  auto rho = [&](int jj, int ii) -> double { return p0[q + (long long)(jj - j) * d.N1 + (ii - i)]; };
   auto corner = [&](int jj, int ii) -> double {
     const double avg = 0.25 * (((rho(jj, ii) + rho(jj, ii - 1)) + rho(jj - 1, ii)) + rho(jj - 1, ii - 1));
     const double v = avg - ga.cut;
@@ -2364,8 +2430,8 @@ __global__ void __launch_bounds__(kThreads) k_gen_bfield(Dims d, pangu_params p,
   cell_metric<MT>(d, p, b, k, j, i, g);
   const double b1 = -(((a00 - a01) + a10) - a11) / ((2.0 * dx_of(d, b, 1)) * g.sg);
   const double b2 = (((a00 + a01) - a10) - a11) / ((2.0 * dx_of(d, b, 0)) * g.sg);
-  P[q + d.pidx[BX1] * d.ncell] = (PT)b1;
-  P[q + d.pidx[BX2] * d.ncell] = (PT)b2;
+  a_prim(d, P, b, d.pidx[BX1])[q] = (PT)b1;
+  a_prim(d, P, b, d.pidx[BX2])[q] = (PT)b2;
   double pc[NPRIM];
   load_prim(d, P, b, k, j, i, pc);
   State st;
@@ -2386,10 +2452,10 @@ __global__ void __launch_bounds__(kThreads) k_gen_scale(Dims d, double gam, doub
   const double bsq_max = __longlong_as_double((long long)red[2]);
   const double beta_min = 2.0 * (gam - 1.0) * (umax / rhomax) / (bsq_max + 1.0e-30);
   const double norm = sqrt(beta_min / beta);
-  const long long q = vidx(d, b, 0, k, j, i);
+  const long long q = coff(d, k, j, i);
   for (int v = BX1; v <= BX3; ++v) {
-    const long long o = q + d.pidx[v] * d.ncell;
-    P[o] = (PT)((double)P[o] * norm);
+    PT *pv = a_prim(d, P, b, d.pidx[v]);
+    pv[q] = (PT)((double)pv[q] * norm);
   }
 }
 
@@ -2456,23 +2522,52 @@ inline unsigned grid_flux(long long n, int threads) {
   return (unsigned)std::max<long long>(1, (n + threads - 1) / threads);
 }
 
+// Every array a stage task may touch is given, as a contiguous array or by
+// its per-(block, component) table.
 bool pack_ok(const pangu_engine *e, const pangu_pack *md) {
-  if (!e || !md || !md->prim || !md->cons || !md->flux1 || !md->alfven || !md->efield) return false;
-  if (e->d.ndim >= 2 && !md->flux2) return false;
-  if (e->d.ndim == 3 && !md->flux3) return false;
-  if (e->p.recovery == PANGU_RECOVERY_CHAINER && !md->flag) return false;
+  if (!e || !md) return false;
+  auto has = [](const void *a, const void *tab) { return a || tab; };
+  if (!has(md->prim, md->prim_vars) || !has(md->cons, md->cons_vars) ||
+      !has(md->flux1, md->flux1_vars) || !has(md->alfven, md->alfven_vars) ||
+      !has(md->efield, md->efield_vars))
+    return false;
+  if (e->d.ndim >= 2 && !has(md->flux2, md->flux2_vars)) return false;
+  if (e->d.ndim == 3 && !has(md->flux3, md->flux3_vars)) return false;
+  if (e->p.recovery == PANGU_RECOVERY_CHAINER && !has(md->flag, md->flag_vars)) return false;
   return true;
+}
+
+// True when no array of md goes through a per-(block, component) table.
+inline bool contiguous(const pangu_pack *md) {
+  return !md->prim_vars && !md->cons_vars && !md->flux1_vars && !md->flux2_vars &&
+         !md->flux3_vars && !md->alfven_vars && !md->efield_vars && !md->flag_vars;
+}
+
+// The engine's Dims with the layout tables of md's arrays (null tables: the
+// contiguous layout).
+inline Dims bind(const pangu_engine *e, const pangu_pack *md) {
+  Dims d = e->d;
+  d.tP = reinterpret_cast<void *const *>(md->prim_vars);
+  d.tU = d.tUi = md->cons_vars;
+  d.tF = nullptr;
+  d.tF1 = md->flux1_vars;
+  d.tF2 = md->flux2_vars;
+  d.tF3 = md->flux3_vars;
+  d.tA = md->alfven_vars;
+  d.tE = md->efield_vars;
+  d.tG = md->flag_vars;
+  return d;
 }
 
 // FixPrimitive; with_cons also computes the interior conserved variables
 // (CalculateConservative) in the same pass (the stage path).
 int run_fix_primitive(pangu_engine *e, const pangu_pack *md, bool with_cons, cudaStream_t s) {
-  const Dims &d = e->d;
+  const Dims d = bind(e, md);
   const long long n = (long long)d.NB * d.ncell;
   // on the stage path (with_cons) the C2P retry and FixRecovery list counters
   // are zeroed here for Recovery
   DISPATCH_MT(e->p.metric_type, k_fix_primitive, grid_for(n), s, d, e->p, prim_of(md), e->d_cnt,
-              with_cons ? md->cons : nullptr, PGK_MIXED ? 0 : 1,
+              md->cons, with_cons ? 1 : 0, PGK_MIXED ? 0 : 1,
               with_cons ? e->d_fail_count : nullptr, with_cons ? e->d_fix_count : nullptr);
   ++e->launches;
   return check_launch();
@@ -2492,11 +2587,9 @@ int run_calc_cons(pangu_engine *e, const Dims &d, const pangu_pack *md, bool wit
 }
 
 int run_calc_cons(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
-  return run_calc_cons(e, e->d, md, !PGK_MIXED, s);
+  return run_calc_cons(e, bind(e, md), md, !PGK_MIXED, s);
 }
 
-// Launches the flux kernel of one direction with a given march depth
-// (x2/x3) and CTA size.
 // cuTensorMapEncodeTiled through the runtime's driver entry point (the
 // library links the runtime only).
 inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -2542,10 +2635,16 @@ inline bool tma_tile_map(const pangu_engine *e, const pangu_pack *md, int dir, C
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Launches the flux kernel of one direction with a given march depth
+// (x2/x3) and CTA size. The TMA-staged kernels read the contiguous layout; a
+// pack whose primitives come through a table runs the thread-loaded form of
+// the same tile shape instead.
 template <int MT, int OPT>
 void launch_flux_dir(const pangu_engine *e, const pangu_pack *md, int dir, int march, int threads,
                      cudaStream_t s) {
-  const Dims &d = e->d;
+  Dims d = bind(e, md);
+  d.tF = dir == 1 ? md->flux1_vars : (dir == 2 ? md->flux2_vars : md->flux3_vars);
+  if (march == kMarchTma && md->prim_vars) march = dir == 1 ? 1 : 0;
   const bool hll = e->p.riemann_solver == PANGU_RIEMANN_HLL;
   int k0 = d.ks - d.o3, k1 = d.ke + d.o3, j0 = d.js - d.o2, j1 = d.je + d.o2;
   int i0 = d.is - d.o1, i1 = d.ie + d.o1;
@@ -2724,7 +2823,7 @@ int run_autotune(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
 
 
 int run_ct(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
-  const Dims &d = e->d;
+  const Dims d = bind(e, md);
   const int o1 = d.N1 > 1, o2 = d.N2 > 1, o3 = d.N3 > 1;
   launch_pdl(k_ct_emf, dim3(grid_for(box_count(d.NB, d.ks, d.ke + o3, d.js, d.je + o2, d.is,
                                                 d.ie + o1))),
@@ -2739,7 +2838,9 @@ int run_ct(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
 
 int run_update(pangu_engine *e, const pangu_pack *mi, const pangu_pack *m0, const pangu_pack *m1,
                double beta, const double *dt, cudaStream_t s) {
-  const Dims &d = e->d;
+  Dims d = bind(e, m0);  // the fluxes of mc0
+  d.tU = m1->cons_vars;  // written: mc1's conserved variables
+  d.tUi = mi->cons_vars;  // read: the starting state's
   const long long n = box_count(d.NB * d.NF, d.ks, d.ke, d.js, d.je, d.is, d.ie);
   launch_pdl(k_flux_div_update, dim3(grid_for(n)), dim3(kThreads), s, d, m0->flux1, m0->flux2,
              m0->flux3, mi->cons, m1->cons, beta, dt);
@@ -2750,7 +2851,7 @@ int run_update(pangu_engine *e, const pangu_pack *mi, const pangu_pack *m0, cons
 int run_exchange_range(pangu_engine *e, const pangu_pack *md, long long off, long long n,
                        cudaStream_t s) {
   if (n == 0) return PANGU_OK;
-  launch_pdl(k_exchange, dim3(grid_for(n)), dim3(kThreads), s, e->d, n, e->d_xdst + off,
+  launch_pdl(k_exchange, dim3(grid_for(n)), dim3(kThreads), s, bind(e, md), n, e->d_xdst + off,
              e->d_xsrc + off, prim_of(md), md->flag);
   ++e->launches;
   return check_launch();
@@ -2763,7 +2864,7 @@ int run_exchange(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
 int run_halo_pack(pangu_engine *e, const pangu_pack *md, double *buf, cudaStream_t s) {
   const long long n = e->hsend_off.empty() ? 0 : e->hsend_off.back();
   if (n == 0) return PANGU_OK;
-  launch_pdl(k_halo_pack, dim3(grid_for(n)), dim3(kThreads), s, e->d, n, e->d_hsend, prim_of(md),
+  launch_pdl(k_halo_pack, dim3(grid_for(n)), dim3(kThreads), s, bind(e, md), n, e->d_hsend, prim_of(md),
              md->flag, buf);
   ++e->launches;
   return check_launch();
@@ -2772,7 +2873,7 @@ int run_halo_pack(pangu_engine *e, const pangu_pack *md, double *buf, cudaStream
 int run_halo_unpack(pangu_engine *e, const pangu_pack *md, const double *buf, cudaStream_t s) {
   const long long n = e->hrecv_off.empty() ? 0 : e->hrecv_off.back();
   if (n == 0) return PANGU_OK;
-  launch_pdl(k_halo_unpack, dim3(grid_for(n)), dim3(kThreads), s, e->d, n, e->d_hrecv, prim_of(md),
+  launch_pdl(k_halo_unpack, dim3(grid_for(n)), dim3(kThreads), s, bind(e, md), n, e->d_hrecv, prim_of(md),
              md->flag, buf);
   ++e->launches;
   return check_launch();
@@ -2780,7 +2881,7 @@ int run_halo_unpack(pangu_engine *e, const pangu_pack *md, const double *buf, cu
 
 int run_source(pangu_engine *e, const pangu_pack *md, double beta, const double *dt,
                cudaStream_t s) {
-  const Dims &d = e->d;
+  const Dims d = bind(e, md);
   if (e->p.metric_type == PANGU_METRIC_MINKOWSKI) return PANGU_OK;  // zero connection
   const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
   DISPATCH_MT(e->p.metric_type, k_source, grid_for(n), s, d, e->p, prim_of(md), md->cons, beta, dt);
@@ -2793,7 +2894,7 @@ int run_source(pangu_engine *e, const pangu_pack *md, double beta, const double 
 // list_fix: the stage path, whose FixPrimitive launch has zeroed both list
 // counters; otherwise the retry counter is zeroed here.
 int run_recovery(pangu_engine *e, const pangu_pack *md, bool list_fix, cudaStream_t s) {
-  const Dims &d = e->d;
+  const Dims d = bind(e, md);
   const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
   if (!list_fix && cudaMemsetAsync(e->d_fail_count, 0, sizeof(int), s) != cudaSuccess)
     return PANGU_ECUDA;
@@ -2817,7 +2918,7 @@ int run_recovery(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
 }
 
 int run_heating(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
-  const Dims &d = e->d;
+  const Dims d = bind(e, md);
   if (!e->p.enable_heating) return PANGU_OK;
   const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
   DISPATCH_MT(e->p.metric_type, k_heating, grid_for(n), s, d, e->p, prim_of(md), md->cons);
@@ -2829,7 +2930,7 @@ int run_heating(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
 // (the stage path); otherwise a scan of the flags finds them. Both lists hold
 // the same cells (in a different order, which the two-phase fix ignores).
 int run_fix_recovery(pangu_engine *e, const pangu_pack *md, bool listed, cudaStream_t s) {
-  const Dims &d = e->d;
+  const Dims d = bind(e, md);
   int *count = e->d_fix_count;
   long long *list = e->d_fix_list;
   if (!listed) {
@@ -2861,11 +2962,11 @@ int run_bcs(pangu_engine *e, const Dims &d, bool any_bc, const pangu_pack *md, c
 }
 
 int run_bcs(pangu_engine *e, const pangu_pack *md, cudaStream_t s) {
-  return run_bcs(e, e->d, e->any_bc, md, s);
+  return run_bcs(e, bind(e, md), e->any_bc, md, s);
 }
 
 int run_estimate_dt(pangu_engine *e, const pangu_pack *md, double *dt_out, cudaStream_t s) {
-  const Dims &d = e->d;
+  const Dims d = bind(e, md);
   const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
   const unsigned gx = (unsigned)std::min<long long>((n / std::max(1, d.NB) + kThreads - 1) / kThreads, 592);
   // d_dtmin holds the key of DBL_MAX and d_dt_ticket 0 between calls (set at pool_init)

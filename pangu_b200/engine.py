@@ -163,6 +163,97 @@ class DeviceContainer:
         return C.byref(self._pack)
 
 
+class TableContainer:
+    """A stage container laid out as Parthenon keeps its variables: one device
+    allocation per block and variable, addressed through the pack's
+    per-(block, component) pointer tables (pangu_pack.*_vars).
+
+    ``prim_groups`` / ``cons_groups`` split the NF components into variables
+    (component counts, e.g. (1, 1, 3, 3, 1) for density, energy,
+    weighted_velocity, magnetic_field, entropy; default: one allocation per
+    component); the face fluxes follow ``cons_groups``; alfven and efield are
+    one 3-component variable, flag one scalar. ``contiguous`` names fields
+    kept in the contiguous [NB][NC][N3][N2][N1] layout instead (a pack may mix
+    both). ``shared`` takes alfven, efield and flag from another container
+    (Metadata::OneCopy)."""
+
+    FIELDS = DeviceContainer.FIELDS
+
+    def __init__(self, nb, nf, shape, device, prim_groups=None, cons_groups=None, shared=None,
+                 contiguous=(), mixed=False):
+        torch = _torch()
+        self.nb, self.nf, self.shape, self.device = nb, nf, tuple(shape), device
+        self.ncell = int(np.prod(shape))
+        pdt = torch.float32 if mixed else torch.float64
+        groups = {"prim": tuple(prim_groups or (1,) * nf), "alfven": (3,), "efield": (3,),
+                  "flag": (1,)}
+        for f in ("cons", "flux1", "flux2", "flux3"):
+            groups[f] = tuple(cons_groups or (1,) * nf)
+        # a table must hold NB * NC entries: the kernels index it by (slot, component)
+        for f in ("prim", "cons"):
+            if sum(groups[f]) != nf or min(groups[f]) < 1:
+                raise ValueError(f"{f} variables {groups[f]} do not cover the {nf} components")
+        self.arrays, self.tables, self.dense = {}, {}, {}
+        self._pack = abi.Pack()
+        for f in self.FIELDS:
+            if shared is not None and f in ("alfven", "efield", "flag"):
+                self.arrays[f] = shared.arrays.get(f)
+                self.dense[f] = shared.dense.get(f)
+                self.tables[f] = shared.tables.get(f)
+            else:
+                nc = sum(groups[f])
+                dtype = pdt if f == "prim" else torch.float64
+                if f in contiguous:
+                    shp = (nb, *shape) if f == "flag" else (nb, nc, *shape)
+                    self.dense[f] = torch.zeros(shp, dtype=dtype, device=device)
+                    self.arrays[f] = None
+                    self.tables[f] = None
+                else:
+                    self.dense[f] = None
+                    self.arrays[f] = [[torch.zeros((g, *shape), dtype=dtype, device=device)
+                                       for g in groups[f]] for _ in range(nb)]
+                    ptrs = []
+                    for b in range(nb):
+                        for t in self.arrays[f][b]:
+                            ptrs += [t.data_ptr() + c * self.ncell * t.element_size()
+                                     for c in range(t.shape[0])]
+                    self.tables[f] = torch.tensor(ptrs, dtype=torch.int64, device=device)
+            if self.dense[f] is not None:
+                setattr(self._pack, f, self.dense[f].data_ptr())
+            if self.tables[f] is not None:
+                setattr(self._pack, f + "_vars", self.tables[f].data_ptr())
+
+    @property
+    def pack(self):
+        return C.byref(self._pack)
+
+    def gather(self, f):
+        """Field f as one [NB][NC][N3][N2][N1] ([NB][N3][N2][N1] for flag) tensor."""
+        torch = _torch()
+        if self.dense[f] is not None:
+            return self.dense[f].clone()
+        out = torch.stack([torch.cat(blk, dim=0) for blk in self.arrays[f]])
+        return out[:, 0] if f == "flag" else out
+
+    def scatter(self, f, src):
+        """Writes field f from a tensor of the gather() shape."""
+        if self.dense[f] is not None:
+            self.dense[f].copy_(src)
+            return
+        src = src.reshape(self.nb, -1, *self.shape)
+        for b in range(self.nb):
+            c = 0
+            for t in self.arrays[f][b]:
+                t.copy_(src[b, c:c + t.shape[0]])
+                c += t.shape[0]
+
+    def load(self, other):
+        """Copies every field of a container (DeviceContainer or TableContainer)."""
+        for f in self.FIELDS:
+            self.scatter(f, other.gather(f) if isinstance(other, TableContainer)
+                         else getattr(other, f))
+
+
 class Engine:
     """An engine handle for one parameter set and mesh."""
 

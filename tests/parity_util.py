@@ -31,10 +31,12 @@ CASES = {
 
 
 class Case:
-    def __init__(self, name):
+    def __init__(self, name, extra=None):
+        """extra: more (block, key) -> value settings of the input, applied
+        after the case's own (e.g. mesh extents)."""
         problem, kw, over = CASES[name]
         pin, gen = problems.make_problem(problem, **kw)
-        for (blk, key), v in over.items():
+        for (blk, key), v in {**over, **(extra or {})}.items():
             pin.set(blk, key, v)
         self.name = name
         self.pin = pin
