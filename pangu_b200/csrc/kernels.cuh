@@ -1898,18 +1898,26 @@ __device__ __forceinline__ void c2p_write(const Dims &d, PT *P, int b, int k, in
   a_prim(d, P, b, 4)[q] = PH[UX3];
 }
 
-// Recovery, first pass: Kastaun (robuster), or Scheme2D of the chain. Cells
-// where Scheme2D fails are appended to `retry` (their primitives are left
-// untouched) and finished by k_recovery_retry, so the long 1Dvsq/1D Newton
-// loops of a few cells do not hold whole warps of converged cells.
+// Recovery, first pass: Kastaun (robuster), or the chain from Scheme2D.
+// CHAIN = false: cells where Scheme2D fails are appended to `list` (their
+// primitives left untouched) and finished by k_recovery_retry, so the long
+// 1Dvsq/1D Newton loops of a few cells do not hold whole warps of converged
+// cells. CHAIN = true: the failing lanes run Scheme1Dvsq and Scheme1D at
+// once (the retry pass's arithmetic, from the same inputs), and `list` (may
+// be null) receives the cells the whole chain fails, FixRecovery's list.
+// The chained form is used when the pass fits in one wave of CTAs: then the
+// few long chains overlap the rest of the wave instead of running as a
+// separate latency-bound launch (2D 512 x 256 torus at steady state: 0.387
+// against 0.403 ms per cycle), while on larger grids the registers the
+// chain adds (spills) cost more than the retry launch (3D torus 11.17
+// against 10.98 ms, 48-torus batch 7.15 against 7.05 ms).
 // (Folding the geometric source and electron heating into this kernel was
 // measured slower: their registers cut the occupancy of the Newton loops.)
-template <int MT>
-__global__ void __launch_bounds__(kRecoveryThreads, 7) k_recovery(Dims d, pangu_params p, PT *P,
-                                                       const double *U, double *flag,
-                                                       unsigned long long *cnt, int *nretry,
-                                                       long long *retry) {
-  pdl_grid_wait();
+template <int MT, bool CHAIN>
+__device__ __forceinline__ void recovery_cell(const Dims &d, const pangu_params &p, PT *P,
+                                              const double *U, double *flag,
+                                              unsigned long long *cnt, int *nlist,
+                                              long long *list) {
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
@@ -1940,13 +1948,48 @@ __global__ void __launch_bounds__(kRecoveryThreads, 7) k_recovery(Dims d, pangu_
   } else {
     Harm hs;
     harm_setup<MT>(UH, g, hs);
-    const bool ok = invert_2d<MT>(UH, PH, gam, g, hs) == 0;
+    bool ok = invert_2d<MT>(UH, PH, gam, g, hs) == 0;
     count(cnt, job_of(d, b), PANGU_CNT_C2P_2D, ok);
-    append(nretry, retry, !ok, fc);
-    a_flag(d, flag, b)[fc - (long long)b * d.ncell] = ok ? 1.0 : 0.0;
-    if (!ok) return;
+    if (!CHAIN) {
+      append(nlist, list, !ok, fc);
+      a_flag(d, flag, b)[fc - (long long)b * d.ncell] = ok ? 1.0 : 0.0;
+      if (!ok) return;
+    } else {
+      if (!ok) {
+        // Scheme1Dvsq, then Scheme1D (invertor.cc:185-197), from the stale
+        // guess as it stands in memory
+        c2p_inputs<MT>(d, p, P, U, b, k, j, i, g, UH, PH, false);
+        harm_setup<MT>(UH, g, hs);
+        ok = invert_1dvsq<MT>(UH, PH, gam, g, hs) == 0;
+        count(cnt, job_of(d, b), PANGU_CNT_C2P_1DVSQ, ok);
+        if (!ok) {
+          ok = invert_1d<MT>(UH, PH, gam, g, hs) == 0;
+          count(cnt, job_of(d, b), PANGU_CNT_C2P_1D, ok);
+          count(cnt, job_of(d, b), PANGU_CNT_C2P_FAIL, !ok);
+        }
+        if (list) append(nlist, list, !ok, fc);
+      }
+      a_flag(d, flag, b)[fc - (long long)b * d.ncell] = ok ? 1.0 : 0.0;
+    }
   }
   c2p_write(d, P, b, k, j, i, PH);
+}
+
+template <int MT>
+__global__ void __launch_bounds__(kRecoveryThreads, 7) k_recovery(Dims d, pangu_params p, PT *P,
+                                                       const double *U, double *flag,
+                                                       unsigned long long *cnt, int *nretry,
+                                                       long long *retry) {
+  pdl_grid_wait();
+  recovery_cell<MT, false>(d, p, P, U, flag, cnt, nretry, retry);
+}
+
+template <int MT>
+__global__ void __launch_bounds__(kRecoveryThreads, 7)
+    k_recovery_chain(Dims d, pangu_params p, PT *P, const double *U, double *flag,
+                     unsigned long long *cnt, int *nfix, long long *fix) {
+  pdl_grid_wait();
+  recovery_cell<MT, true>(d, p, P, U, flag, cnt, nfix, fix);
 }
 
 // Recovery, second pass over the cells Scheme2D failed: Scheme1Dvsq, then
@@ -2518,6 +2561,20 @@ inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, c
     }                                                                                        \
   } while (0)
 
+// Streaming multiprocessors of the current device (148 on a B200), queried
+// once per process and device.
+inline int device_sms() {
+  static int cached[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!cached[dev]) {
+    int n = 148;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    cached[dev] = n;
+  }
+  return cached[dev];
+}
+
 inline unsigned grid_flux(long long n, int threads) {
   return (unsigned)std::max<long long>(1, (n + threads - 1) / threads);
 }
@@ -2896,18 +2953,26 @@ int run_source(pangu_engine *e, const pangu_pack *md, double beta, const double 
 int run_recovery(pangu_engine *e, const pangu_pack *md, bool list_fix, cudaStream_t s) {
   const Dims d = bind(e, md);
   const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
+  const unsigned grid = (unsigned)((n + kRecoveryThreads - 1) / kRecoveryThreads);
+  if (e->p.recovery == PANGU_RECOVERY_CHAINER && (long long)grid <= 7LL * device_sms()) {
+    // one wave: the chain in the same pass; the cells the whole chain fails
+    // form FixRecovery's list (the stage path)
+    DISPATCH_MT_T(e->p.metric_type, k_recovery_chain, grid, kRecoveryThreads, s, d, e->p,
+                  prim_of(md), md->cons, md->flag, e->d_cnt,
+                  list_fix ? e->d_fix_count : nullptr, list_fix ? e->d_fix_list : nullptr);
+    ++e->launches;
+    return check_launch();
+  }
   if (!list_fix && cudaMemsetAsync(e->d_fail_count, 0, sizeof(int), s) != cudaSuccess)
     return PANGU_ECUDA;
-  DISPATCH_MT_T(e->p.metric_type, k_recovery,
-                (unsigned)((n + kRecoveryThreads - 1) / kRecoveryThreads), kRecoveryThreads, s, d,
-                e->p, prim_of(md), md->cons, md->flag,
-              e->d_cnt, e->d_fail_count, e->d_fail_list);
+  DISPATCH_MT_T(e->p.metric_type, k_recovery, grid, kRecoveryThreads, s, d, e->p, prim_of(md),
+                md->cons, md->flag, e->d_cnt, e->d_fail_count, e->d_fail_list);
   ++e->launches;
   if (e->p.recovery == PANGU_RECOVERY_CHAINER) {
     // one-warp CTAs: the few thousand retried cells spread over every SM
-    DISPATCH_MT_T(e->p.metric_type, k_recovery_retry, 8 * 148, 32, s, d, e->p, prim_of(md), md->cons,
-                md->flag, e->d_cnt, e->d_fail_count, e->d_fail_list,
-                list_fix ? e->d_fix_count : nullptr, list_fix ? e->d_fix_list : nullptr);
+    DISPATCH_MT_T(e->p.metric_type, k_recovery_retry, 8 * 148, 32, s, d, e->p, prim_of(md),
+                  md->cons, md->flag, e->d_cnt, e->d_fail_count, e->d_fail_list,
+                  list_fix ? e->d_fix_count : nullptr, list_fix ? e->d_fix_list : nullptr);
     ++e->launches;
   }
   return check_launch();

@@ -37,6 +37,12 @@ struct Arena {
   std::vector<void *> allocs;
 };
 
+// Cycles a class keeps queued on its stream ahead of the host loop, so that
+// the host's work for other classes (admission, retirement, graph capture)
+// does not leave this class's stream idle. Never more than any of its
+// running jobs still needs.
+constexpr int kQueue = 4;
+
 struct SClass {
   pangu_params p{};
   pangu_mesh block{};
@@ -47,9 +53,11 @@ struct SClass {
   pangu_engine *e = nullptr;
   Arena a;
   cudaStream_t stream = nullptr;
-  cudaEvent_t tick_done = nullptr;
+  // one event per queued cycle, a ring of kQueue: ev[head] is the oldest
+  cudaEvent_t ev[kQueue] = {};
+  int queued = 0, head = 0;
   cudaGraphExec_t graph = nullptr;
-  bool dirty = true, inflight = false, tuned = false;
+  bool dirty = true, tuned = false;
   int running = 0;
   bool lazy = false;       // allocated at admission, released when idle
   bool allocated = false;  // engine, arena, stream and event exist
@@ -107,18 +115,19 @@ void release(pangu_server *s, SClass &c) {
   if (c.graph) cudaGraphExecDestroy(c.graph);
   if (c.e) pangu_engine_destroy(c.e);
   for (void *p : c.a.allocs) cudaFree(p);
-  if (c.tick_done) cudaEventDestroy(c.tick_done);
+  for (cudaEvent_t &ev : c.ev)
+    if (ev) cudaEventDestroy(ev);
   if (c.stream) cudaStreamDestroy(c.stream);
   s->used -= std::min(s->used, c.bytes);
   c.graph = nullptr;
   c.e = nullptr;
   c.a = Arena{};
-  c.tick_done = nullptr;
+  for (cudaEvent_t &ev : c.ev) ev = nullptr;
+  c.queued = c.head = 0;
   c.stream = nullptr;
   c.bytes = 0;
   c.allocated = false;
   c.dirty = true;
-  c.inflight = false;
   c.tuned = false;
   c.running = 0;
 }
@@ -170,8 +179,9 @@ int allocate(pangu_server *s, SClass &c) {
   if (!rc) rc = salloc(s, c, &a.dt_est, c.max_jobs);
   if (!rc && cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess)
     rc = PANGU_ECUDA;
-  if (!rc && cudaEventCreateWithFlags(&c.tick_done, cudaEventDisableTiming) != cudaSuccess)
-    rc = PANGU_ECUDA;
+  for (cudaEvent_t &ev : c.ev)
+    if (!rc && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+      rc = PANGU_ECUDA;
   if (rc) {
     release(s, c);
     return rc;
@@ -425,31 +435,38 @@ int pangu_server_run(pangu_server *s) {
   st = pangu_server_stats{};
   const auto t0 = std::chrono::steady_clock::now();
   int rc = PANGU_OK;
-  // Every class advances on its own: when its previous cycle has finished,
-  // the cycle is credited to its running jobs, finished jobs are copied out
-  // and detached, arrived jobs admitted, and the next cycle launched.
+  // Every class advances on its own stream. Its finished cycles are credited
+  // to its running jobs; with none of its cycles in flight, finished and
+  // cancelled jobs are copied out and detached and arrived jobs admitted
+  // (both rewrite the block table that queued kernels read); then cycles are
+  // queued, up to kQueue and never past any running job's last cycle. An
+  // admissible waiting job lets the queue drain instead.
   while (done < s->jobs.size()) {
     bool busy = false, starved = false, released = false;
     for (int ci = 0; ci < (int)s->classes.size(); ++ci) {
       SClass &c = s->classes[ci];
-      if (c.inflight) {
-        const cudaError_t q = cudaEventQuery(c.tick_done);
-        if (q == cudaErrorNotReady) {
-          busy = true;
-          continue;
-        }
+      while (c.queued > 0) {
+        const cudaError_t q = cudaEventQuery(c.ev[c.head]);
+        if (q == cudaErrorNotReady) break;
         if (q != cudaSuccess) return PANGU_ECUDA;
-        c.inflight = false;
+        c.head = (c.head + 1) % kQueue;
+        --c.queued;
         ++st.ticks;
-        const double tnow = now_s(t0);
         for (SJob &j : s->jobs) {
           if (j.state != 1 || j.cls != ci) continue;
           ++j.done_cycles;
           st.zone_cycles += (double)c.interior * j.slots.size();
-          if (tnow >= j.cancel_at && j.done_cycles < j.cycles) {  // cancelled while running
+        }
+      }
+      if (c.queued > 0) busy = true;
+      const double t = now_s(t0);
+      if (c.queued == 0) {
+        for (SJob &j : s->jobs) {
+          if (j.state != 1 || j.cls != ci) continue;
+          if (t >= j.cancel_at && j.done_cycles < j.cycles) {  // cancelled while running
             if ((rc = drop(c, j))) return rc;
             j.state = 3;
-            j.t_done = tnow;
+            j.t_done = t;
             ++done;
             continue;
           }
@@ -460,8 +477,8 @@ int pangu_server_run(pangu_server *s) {
           ++done;
         }
       }
-      const double t = now_s(t0);
-      bool waiting = false;
+      bool waiting = false, admissible = false;
+      const int free_blocks = c.allocated ? c.capacity - pangu_active_blocks(c.e) : c.capacity;
       for (int q : order) {  // first fit in arrival order
         SJob &j = s->jobs[q];
         if (j.cls != ci || j.state != 0) continue;
@@ -473,6 +490,9 @@ int pangu_server_run(pangu_server *s) {
         }
         if (j.arrival > t) continue;
         waiting = true;
+        const long long nb = (long long)j.mesh.nbx1 * j.mesh.nbx2 * j.mesh.nbx3;
+        if (nb <= free_blocks && c.running < c.max_jobs) admissible = true;
+        if (c.queued > 0) continue;  // admitted once the queue has drained
         if (!c.allocated) {
           // the class's memory is charged at its first admission; a class
           // that does not fit yet waits for retiring work to free the budget
@@ -493,22 +513,34 @@ int pangu_server_run(pangu_server *s) {
       if (!c.running) {
         // an idle lazily allocated class with no arrived job waiting gives its
         // memory back
-        if (c.lazy && c.allocated && !c.inflight && !waiting) {
+        if (c.lazy && c.allocated && c.queued == 0 && !waiting) {
           release(s, c);
           released = true;
         }
         continue;
       }
-      if (!c.tuned) {  // flux tile shapes, tuned once on the class's first jobs
-        if ((rc = pangu_autotune(c.e, &c.a.base, c.stream))) return rc;
-        c.tuned = true;
+      bool cancelling = false;  // a running job to drop once the queue drains
+      for (const SJob &j : s->jobs)
+        cancelling |= j.state == 1 && j.cls == ci && t >= j.cancel_at;
+      if ((admissible || cancelling) && c.queued > 0) continue;  // drain first
+      if (c.queued == 0) {
+        if (!c.tuned) {  // flux tile shapes, tuned once on the class's first jobs
+          if ((rc = pangu_autotune(c.e, &c.a.base, c.stream))) return rc;
+          c.tuned = true;
+        }
+        if (c.dirty && (rc = capture(c))) return rc;
       }
-      if (c.dirty && (rc = capture(c))) return rc;
-      if (cudaGraphLaunch(c.graph, c.stream) != cudaSuccess ||
-          cudaEventRecord(c.tick_done, c.stream) != cudaSuccess)
-        return PANGU_ECUDA;
-      c.inflight = true;
-      busy = true;
+      long long room = kQueue - c.queued;
+      for (const SJob &j : s->jobs)
+        if (j.state == 1 && j.cls == ci)
+          room = std::min(room, j.cycles - j.done_cycles - c.queued);
+      for (long long n = 0; n < room; ++n) {
+        if (cudaGraphLaunch(c.graph, c.stream) != cudaSuccess ||
+            cudaEventRecord(c.ev[(c.head + c.queued) % kQueue], c.stream) != cudaSuccess)
+          return PANGU_ECUDA;
+        ++c.queued;
+      }
+      if (c.queued > 0) busy = true;
     }
     if (!busy && starved && !released) {
       // nothing runs, so nothing will free memory: an arrived job's class does
@@ -534,6 +566,7 @@ int pangu_server_run(pangu_server *s) {
   for (SClass &c : s->classes)
     if (c.lazy && c.allocated) {
       if (cudaStreamSynchronize(c.stream) != cudaSuccess) return PANGU_ECUDA;
+      c.queued = 0;
       release(s, c);
     }
   std::vector<double> lat;

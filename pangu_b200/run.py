@@ -102,7 +102,7 @@ def run(workload="torus2d", precision="fp64", cycles=40, graph_cycles=0, tiles=N
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", choices=["torus2d", "ot", "torus3d", "batch48"],
+    ap.add_argument("--workload", choices=["torus2d", "ot", "torus3d", "cks3d", "batch48"],
                     default="torus2d")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--cycles", type=int, default=40)

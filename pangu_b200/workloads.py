@@ -3,7 +3,11 @@
 * ``torus2d``: the 2D Fishbone-Moncrief torus in MKS coordinates, 512 x 256,
   PPM4, LAXF, chainer C2P, electron heating, one meshblock, 200 RK2 cycles.
 * ``ot``: the Orszag-Tang vortex, 256^2, Minkowski, MC, LAXF, 100 cycles.
-* ``torus3d``: the torus on 256 x 128 x 128 in 16 meshblocks of 64^3, 50 cycles.
+* ``torus3d``: the torus on 256 x 128 x 128 in 16 meshblocks of 64^3, HLL,
+  50 cycles.
+* ``cks3d``: a magnetised atmosphere around a spinning hole in Cartesian
+  Kerr-Schild coordinates with excision, 64^3 in 8 meshblocks of 32^3, MC,
+  LAXF, 50 cycles (the metric formed in the kernels, not tabulated).
 * ``batch48``: 48 tori of uneven grids in one block pool, 100 cycles each.
 * ``serve``: a seeded Poisson stream of Brio-Wu, Orszag-Tang and torus jobs.
 
@@ -29,14 +33,19 @@ SINGLE = {
            {"grid": "256x256", "meshblocks": 1, "limiter": "mc", "riemann_solver": "laxf",
             "recovery": "chainer", "electron_heating": False, "metric": "minkowski"}),
     "torus3d": (lambda seed: problems.fm_torus_input(nx1=256, nx2=128, nx3=128,
-                                                     bx=(64, 64, 64), seed=seed), 50,
+                                                     bx=(64, 64, 64), riemann="hll",
+                                                     seed=seed), 50,
                 {"grid": "256x128x128", "meshblocks": "16 x 64^3", "limiter": "ppm4",
-                 "riemann_solver": "laxf", "recovery": "chainer", "electron_heating": True,
+                 "riemann_solver": "hll", "recovery": "chainer", "electron_heating": True,
                  "metric": "mks a=0.9375 h=0.7"}),
+    "cks3d": (lambda seed: problems.cks_atmosphere_input(n=64, nblock=32), 50,
+              {"grid": "64^3", "meshblocks": "8 x 32^3", "limiter": "mc",
+               "riemann_solver": "laxf", "recovery": "chainer", "electron_heating": False,
+               "metric": "cks a=0.5, excised inside r = 1.5"}),
 }
 WORKLOAD_NAMES = {"torus2d": "fm_torus_mks_2d_512x256", "ot": "orszag_tang_2d_256x256",
-                  "torus3d": "fm_torus_mks_3d_256x128x128", "batch48": "fm_torus_mks_2d_batch48",
-                  "serve": "serving_stream_bw_ot_torus"}
+                  "torus3d": "fm_torus_mks_3d_256x128x128", "cks3d": "cks_atmosphere_3d_64",
+                  "batch48": "fm_torus_mks_2d_batch48", "serve": "serving_stream_bw_ot_torus"}
 
 # block shape of the batch and of the served tori
 BATCH_BLOCK = (128, 64, 1)
@@ -52,7 +61,8 @@ def job_input(workload: str, precision: str = "fp64", seed: int = 0) -> prm.Para
 def initial_state(pin: prm.ParameterInput):
     """(packages, mesh struct, geometry, interior primitives) of a job's
     inputfile: Orszag-Tang or Brio-Wu on a Minkowski metric (Brio-Wu when
-    gamma = 2), the Fishbone-Moncrief torus otherwise."""
+    gamma = 2), the Kerr-Schild atmosphere on a CKS metric, the
+    Fishbone-Moncrief torus otherwise."""
     packages = prm.process_packages(pin)
     mesh = prm.mesh_struct(pin)
     geo = problems.Geometry(mesh)
@@ -60,6 +70,8 @@ def initial_state(pin: prm.ParameterInput):
         gam = packages["core"].params["adiabatic_index"]
         prim = (problems.brio_wu(geo, packages) if gam == 2.0
                 else problems.orszag_tang(geo, packages))
+    elif packages["metric"].params["metric_type"] == "cks":
+        prim = problems.cks_atmosphere(geo, packages)
     else:
         prim = problems.fm_torus(geo, packages, pin)
     return packages, mesh, geo, prim
