@@ -1452,35 +1452,43 @@ __global__ void __launch_bounds__(kThreads) k_ct_faces(Dims d, double *F1, doubl
 // ---------------------------------------------------------------------------
 // FluxDivergence + UpdateIndependentData, interior (ideal_grmhd.cc:73-76).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_flux_div_update(Dims d, const double *F1,
-                                                              const double *F2, const double *F3,
-                                                              const double *Uinit, double *Uout,
-                                                              double beta, const double *dt) {
+// One thread per interior cell for all NF variables: the index decode, the
+// block's widths, areas, volume and beta dt are formed once per cell, not once
+// per (cell, variable) (4x fewer instructions; every variable's value is
+// computed as before).
+__global__ void __launch_bounds__(kThreads, 4) k_flux_div_update(Dims d, const double *F1,
+                                                                 const double *F2,
+                                                                 const double *F3,
+                                                                 const double *Uinit,
+                                                                 double *Uout, double beta,
+                                                                 const double *dt) {
   pdl_grid_wait();
   int b, k, j, i;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (!box_index(t, d.NB * d.NF, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
-  // b here runs over (active block, variable) pairs
-  const int v = b % d.NF;
-  b = slot_of(d, b / d.NF);
+  if (!box_index(t, d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie, b, k, j, i)) return;
+  b = slot_of(d, b);
   const long long q = coff(d, k, j, i);
   const double dx0 = dx_of(d, b, 0), dx1 = dx_of(d, b, 1), dx2 = dx_of(d, b, 2);
   const double A1 = MUL(dx1, dx2), A2 = MUL(dx0, dx2), A3 = MUL(dx0, dx1);
   const double V = MUL(MUL(dx0, dx1), dx2);
-  const double *f1 = a_flux1(d, F1, b, v) + q;
-  double du = SUB(MUL(A1, f1[1]), MUL(A1, f1[0]));
-  if (d.ndim >= 2) {
-    const double *f2 = a_flux2(d, F2, b, v) + q;
-    du = ADD(du, SUB(MUL(A2, f2[d.N1]), MUL(A2, f2[0])));
-  }
-  if (d.ndim == 3) {
-    const long long sk = (long long)d.N1 * d.N2;
-    const double *f3 = a_flux3(d, F3, b, v) + q;
-    du = ADD(du, SUB(MUL(A3, f3[sk]), MUL(A3, f3[0])));
-  }
-  const double dudt = DIV(-du, V);
   const double bdt = MUL(beta, dt[job_of(d, b)]);
-  a_cons(d, Uout, b, v)[q] = ADD(a_cons0(d, Uinit, b, v)[q], MUL(bdt, dudt));
+  const long long sj = d.N1, sk = (long long)d.N1 * d.N2;
+#pragma unroll
+  for (int v = 0; v < NPRIM; ++v) {
+    if (v >= d.NF) break;
+    const double *f1 = a_flux1(d, F1, b, v) + q;
+    double du = SUB(MUL(A1, f1[1]), MUL(A1, f1[0]));
+    if (d.ndim >= 2) {
+      const double *f2 = a_flux2(d, F2, b, v) + q;
+      du = ADD(du, SUB(MUL(A2, f2[sj]), MUL(A2, f2[0])));
+    }
+    if (d.ndim == 3) {
+      const double *f3 = a_flux3(d, F3, b, v) + q;
+      du = ADD(du, SUB(MUL(A3, f3[sk]), MUL(A3, f3[0])));
+    }
+    const double dudt = DIV(-du, V);
+    a_cons(d, Uout, b, v)[q] = ADD(a_cons0(d, Uinit, b, v)[q], MUL(bdt, dudt));
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1496,8 +1504,18 @@ __global__ void __launch_bounds__(kThreads) k_exchange(Dims d, long long n, cons
   long long db, dof, sb, sof;
   split_cell(dc, d.ncell, db, dof);
   split_cell(sc, d.ncell, sb, sof);
-  for (int v = 0; v < d.NF; ++v) a_prim(d, P, (int)db, v)[dof] = a_prim(d, P, (int)sb, v)[sof];
-  if (flag || d.tG) a_flag(d, flag, (int)db)[dof] = a_flag(d, flag, (int)sb)[sof];
+  // every load before the first store (a source is an interior cell, which
+  // the exchange never writes): one memory latency instead of NF in a row
+  PT val[NPRIM];
+#pragma unroll
+  for (int v = 0; v < NPRIM; ++v)
+    if (v < d.NF) val[v] = a_prim(d, P, (int)sb, v)[sof];
+  const bool has_flag = flag || d.tG;
+  const double fl = has_flag ? a_flag(d, flag, (int)sb)[sof] : 0.0;
+#pragma unroll
+  for (int v = 0; v < NPRIM; ++v)
+    if (v < d.NF) a_prim(d, P, (int)db, v)[dof] = val[v];
+  if (has_flag) a_flag(d, flag, (int)db)[dof] = fl;
 }
 
 // Halo messages of a sharded mesh: the cells of the exchange whose other end
@@ -2104,8 +2122,13 @@ __global__ void __launch_bounds__(kThreads) k_fixrec_write(Dims d, const int *co
     const long long fc = list[t];
     const long long b = fc / d.ncell;
     const long long c = fc - b * d.ncell;
-    for (int v = 0; v < d.NF; ++v) a_prim(d, P, (int)b, v)[c] = vals[t * d.NF + v];
-    for (int v = 2; v < 5; ++v) a_prim(d, P, (int)b, v)[c] = 0.;
+    double w[NPRIM];
+#pragma unroll
+    for (int v = 0; v < NPRIM; ++v)
+      if (v < d.NF) w[v] = vals[t * d.NF + v];
+#pragma unroll
+    for (int v = 0; v < NPRIM; ++v)
+      if (v < d.NF) a_prim(d, P, (int)b, v)[c] = (v >= 2 && v < 5) ? PT(0) : (PT)w[v];
     a_flag(d, flag, (int)b)[c] = 1;
     count(cnt, job_of(d, (int)b), PANGU_CNT_FIXRECOVERY, true);
   }
@@ -2154,18 +2177,27 @@ __global__ void __launch_bounds__(kThreads) k_bcs(Dims d, int enable_B, PT *P,
   if (!ghost) return;
   const long long dc = coff(d, idx[2], idx[1], idx[0]);
   const long long sc = coff(d, src[2], src[1], src[0]);
-  for (int v = 0; v < d.NF; ++v) {
-    PT *pv = a_prim(d, P, b, v);
-    double val = pv[sc];
+  // every load before the first store (the sources are never written here):
+  // one memory latency instead of NF in a row
+  double val[NPRIM];
+#pragma unroll
+  for (int v = 0; v < NPRIM; ++v)
+    if (v < d.NF) val[v] = a_prim(d, P, b, v)[sc];
+  const bool has_flag = flag || d.tG;
+  const double fl = has_flag ? a_flag(d, flag, b)[sc] : 0.0;
+#pragma unroll
+  for (int v = 0; v < NPRIM; ++v) {
+    if (v >= d.NF) continue;
+    double x = val[v];
 #pragma unroll
     for (int dir = 0; dir < 3; ++dir) {
       const bool vel = v == d.pidx[UX1] + dir;
       const bool mag = enable_B && v == d.pidx[BX1] + dir;
-      if (flip[dir] && (vel || mag)) val = -val;
+      if (flip[dir] && (vel || mag)) x = -x;
     }
-    pv[dc] = val;
+    a_prim(d, P, b, v)[dc] = (PT)x;
   }
-  if (flag || d.tG) a_flag(d, flag, b)[dc] = a_flag(d, flag, b)[sc];
+  if (has_flag) a_flag(d, flag, b)[dc] = fl;
 }
 
 // ---------------------------------------------------------------------------
@@ -2898,7 +2930,7 @@ int run_update(pangu_engine *e, const pangu_pack *mi, const pangu_pack *m0, cons
   Dims d = bind(e, m0);  // the fluxes of mc0
   d.tU = m1->cons_vars;  // written: mc1's conserved variables
   d.tUi = mi->cons_vars;  // read: the starting state's
-  const long long n = box_count(d.NB * d.NF, d.ks, d.ke, d.js, d.je, d.is, d.ie);
+  const long long n = box_count(d.NB, d.ks, d.ke, d.js, d.je, d.is, d.ie);
   launch_pdl(k_flux_div_update, dim3(grid_for(n)), dim3(kThreads), s, d, m0->flux1, m0->flux2,
              m0->flux3, mi->cons, m1->cons, beta, dt);
   ++e->launches;
