@@ -43,13 +43,21 @@ def sources():
     return out
 
 
+# Sources without stage kernels: the serving loop (host code over the C ABI)
+# and the FP64 peak probe. They do not enter the fingerprint below.
+NOT_STAGE = ("serve.cu", "fp64_peak.cu")
+
+
 def source_hash() -> str:
-    """Fingerprint of the engine's sources (csrc/ and the C ABI header): the
-    build that a profile summary was captured on carries it, so measurements
-    of other sources are never reported against this build."""
+    """Fingerprint of the sources of the stage kernels and their launchers
+    (csrc/ but the files of NOT_STAGE, and the C ABI header): the build that a
+    profile summary was captured on carries it, so measurements of other
+    kernel sources are never reported against this build."""
     import hashlib
     h = hashlib.sha256()
     for src in sorted(sources()):
+        if os.path.basename(src) in NOT_STAGE:
+            continue
         with open(src, "rb") as f:
             h.update(os.path.basename(src).encode() + b"\0" + f.read())
     return h.hexdigest()[:16]

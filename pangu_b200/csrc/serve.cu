@@ -10,7 +10,8 @@
 // and released again when none of the class's jobs is running or waiting.
 // Submitted jobs wait until their arrival
 // time; a job is admitted as soon as its class pool has a free job id and
-// enough free block slots (first fit in arrival order) and then runs one RK2
+// enough free block slots (first fit in arrival order; of jobs that arrive
+// together, the one with the most work first) and then runs one RK2
 // cycle per tick of its class together with every other admitted job of the
 // class (one graph launch per tick). Classes tick independently, each on its
 // own stream, so their kernels overlap and a class of small jobs is not held
@@ -427,8 +428,17 @@ int pangu_server_run(pangu_server *s) {
   if (!s) return PANGU_EINVAL;
   std::vector<int> order(s->jobs.size());
   for (size_t q = 0; q < order.size(); ++q) order[q] = (int)q;
-  std::stable_sort(order.begin(), order.end(),
-                   [&](int x, int y) { return s->jobs[x].arrival < s->jobs[y].arrival; });
+  // admission order: arrival time; among jobs that arrive together, the one
+  // with the most work (cells x cycles) first, so that a long job does not
+  // start last and set the makespan (longest processing time first)
+  auto work = [&](const SJob &j) {
+    return (double)j.cycles * j.mesh.nbx1 * j.mesh.nbx2 * j.mesh.nbx3;
+  };
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    const SJob &a = s->jobs[x], &b = s->jobs[y];
+    if (a.arrival != b.arrival) return a.arrival < b.arrival;
+    return work(a) > work(b);
+  });
   size_t done = 0;
   for (const SJob &j : s->jobs) done += j.state == 2;
   pangu_server_stats &st = s->stats;
@@ -524,7 +534,11 @@ int pangu_server_run(pangu_server *s) {
         cancelling |= j.state == 1 && j.cls == ci && t >= j.cancel_at;
       if ((admissible || cancelling) && c.queued > 0) continue;  // drain first
       if (c.queued == 0) {
-        if (!c.tuned) {  // flux tile shapes, tuned once on the class's first jobs
+        if (!c.tuned) {
+          // flux tile shapes, tuned once on the class's first jobs, with the
+          // device to itself: the other classes' queued cycles would make the
+          // timings (and so the choice) depend on what else was running
+          if (cudaDeviceSynchronize() != cudaSuccess) return PANGU_ECUDA;
           if ((rc = pangu_autotune(c.e, &c.a.base, c.stream))) return rc;
           c.tuned = true;
         }
