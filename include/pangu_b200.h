@@ -450,8 +450,7 @@ int pangu_generate(pangu_engine *e, int32_t job, const pangu_problem *problem,
  * that needs it; such a class is released again whenever none of its jobs is
  * running or has arrived and waits. pangu_server_run admits every submitted job once its
  * arrival time (seconds after the run starts) has passed and its class pool
- * has room (first fit in arrival order; of jobs that arrive together, the one with
- * the most work first), steps the admitted jobs of each
+ * has room (first fit in arrival order), steps the admitted jobs of each
  * class one RK2 cycle per tick of that class (classes tick independently on
  * their own streams, so their kernels overlap), copies each job's primitives
  * back and detaches it after its last cycle. A job's result is identical to
