@@ -878,6 +878,15 @@ void or_pgm_pow(int n, const double *x, const double *y, double *out) {
 void or_pgm_pow_slow(int n, const double *x, const double *y, double *out) {
   for (int i = 0; i < n; ++i) out[i] = pgm::exp_round(pgm::mul_d(pgm::log_dd(x[i]), y[i]));
 }
+// The fast path alone (finite x > 0): ok[i] = 1 where its error bound decided
+// the rounding, with out[i] its result; 0 where the slow path would decide.
+void or_pgm_pow_fast(int n, const double *x, const double *y, double *out, int *ok) {
+  for (int i = 0; i < n; ++i) {
+    double r = 0.0;
+    ok[i] = pgm::pow_fast(x[i], y[i], r) ? 1 : 0;
+    out[i] = r;
+  }
+}
 void or_pgm_exp(int n, const double *x, double *out) {
   for (int i = 0; i < n; ++i) out[i] = pgm::exp(x[i]);
 }

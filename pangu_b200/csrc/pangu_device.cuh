@@ -970,16 +970,19 @@ struct HeatParams {
   int limit_kel, suppress_highb_heat, enforce_positive_dissipation;
 };
 
+// The proton and electron temperatures (tpr, tel) are formed only by the
+// models that read them: the same values, without the electron power in the
+// constant, Werner and Rowan models.
 PGD double heating_fraction(const HeatParams &p, double rho, double energy, double bsq,
                             double adv_electron) {
-  const double tpr = (p.gamma_p - 1.0) * energy / rho;
-  const double tel = adv_electron * PGD_POW(rho, p.gamma_e - 1.0);
+  const auto tpr = [&] { return (p.gamma_p - 1.0) * energy / rho; };
+  const auto tel = [&] { return adv_electron * PGD_POW(rho, p.gamma_e - 1.0); };
   switch (p.model) {
     case 0:
       return p.fel_constant;
     case 1: {
-      const double trat = tpr / tel;
-      const double pres = rho * tpr;
+      const double trat = tpr() / tel();
+      const double pres = rho * tpr();
       const double beta = kmin(2.0 * pres / bsq, 1.0e20);
       const double log_trat = PGD_LOG(trat) / PGD_LOG(10.0);
       const double mbeta = 2.0 - 0.2 * log_trat;
@@ -991,8 +994,8 @@ PGD double heating_fraction(const HeatParams &p, double rho, double energy, doub
       return 1.0 / (1.0 + qrat);
     }
     case 2: {
-      const double trat = tpr / tel;
-      const double pres = rho * tpr;
+      const double trat = tpr() / tel();
+      const double pres = rho * tpr();
       const double beta = kmin(2.0 * pres / bsq, 1.0e20);
       const double qi_qe = 35.0 / (1.0 + PGD_POW(beta / 15.0, -1.4) * PGD_EXP(-0.1 / trat));
       return 1.0 / (1.0 + qi_qe);
@@ -1010,7 +1013,7 @@ PGD double heating_fraction(const HeatParams &p, double rho, double energy, doub
       return 0.5 * PGD_EXP(-PGD_POW(1.0 - beta / betamax, 3.3) / (1.0 + 1.2 * PGD_POW(sigma, 0.7)));
     }
     case 5: {
-      const double trat_inv = tel / tpr;
+      const double trat_inv = tel() / tpr();
       const double qe_qi = 0.33 * sqrt(trat_inv);
       return 1.0 / (1.0 + 1.0 / qe_qi);
     }
@@ -1198,14 +1201,14 @@ PGD void ppm4_t(T qm2, T qm1, T q, T qp1, T qp2, T &ql_ip1, T &qr_i) {
 // heating_model.h:53-179
 template <typename T>
 PGD T heating_fraction_t(const HeatParams &p, T rho, T energy, T bsq, T adv_electron) {
-  const T tpr = (T(p.gamma_p) - T(1)) * energy / rho;
-  const T tel = adv_electron * tpow(rho, T(p.gamma_e) - T(1));
+  const auto tpr = [&] { return (T(p.gamma_p) - T(1)) * energy / rho; };
+  const auto tel = [&] { return adv_electron * tpow(rho, T(p.gamma_e) - T(1)); };
   switch (p.model) {
     case 0:
       return T(p.fel_constant);
     case 1: {
-      const T trat = tpr / tel;
-      const T beta = tmin(T(2) * rho * tpr / bsq, T(1.0e20));
+      const T trat = tpr() / tel();
+      const T beta = tmin(T(2) * rho * tpr() / bsq, T(1.0e20));
       const T log_trat = tlog(trat) / tlog(T(10));
       const T mbeta = T(2) - T(0.2) * log_trat;
       const T c2 = (trat <= T(1)) ? T(1.6) / trat : T(1.2) / trat;
@@ -1216,8 +1219,8 @@ PGD T heating_fraction_t(const HeatParams &p, T rho, T energy, T bsq, T adv_elec
       return T(1) / (T(1) + qrat);
     }
     case 2: {
-      const T trat = tpr / tel;
-      const T beta = tmin(T(2) * rho * tpr / bsq, T(1.0e20));
+      const T trat = tpr() / tel();
+      const T beta = tmin(T(2) * rho * tpr() / bsq, T(1.0e20));
       const T qi_qe = T(35) / (T(1) + tpow(beta / T(15), T(-1.4)) * texp(T(-0.1) / trat));
       return T(1) / (T(1) + qi_qe);
     }
@@ -1235,7 +1238,7 @@ PGD T heating_fraction_t(const HeatParams &p, T rho, T energy, T bsq, T adv_elec
                            (T(1) + T(1.2) * tpow(sigma, T(0.7))));
     }
     case 5: {
-      const T qe_qi = T(0.33) * sqrt(tel / tpr);
+      const T qe_qi = T(0.33) * sqrt(tel() / tpr());
       return T(1) / (T(1) + T(1) / qe_qi);
     }
   }

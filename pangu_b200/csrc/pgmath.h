@@ -17,11 +17,13 @@
 //     of exp(r) - 1 to r^12 (first five terms in double-double), then six
 //     squarings. Relative error before the final rounding below 2^-95.
 //   * fast path of pow (table-driven, pgmath_tables.h): ln m = L_j +
-//     log1p(m inv_j - 1) with |m inv_j - 1| < 2^-9.5 (363 intervals of width
-//     1/512; the product m inv_j is formed exactly), log1p by its series with
-//     the r^2 and r^3 terms in double-double (relative error < 2^-80);
-//     exp t = 2^(k/128) exp(r), |r| <= ln2/256, Cody-Waite reduction, series
-//     to r^8 (relative error < 2^-76). The result hi + lo is returned only if
+//     log1p(m inv_j - 1) with |m inv_j - 1| < 2^-9.49 (363 intervals of width
+//     1/512; the product m inv_j is formed exactly), the high parts summed by
+//     exact two-sums and the low parts in double (error < 2^-80.5 +
+//     2^-84 |ln x|); exp t = 2^(k/128) exp(r), |r| <= ln2/256, Cody-Waite
+//     reduction, r + r^2/2 exact and the series to r^7 in double (relative
+//     error < 2^-76.9). Horner steps use explicit fused multiply-adds, which
+//     round identically on both sides. The result hi + lo is returned only if
 //     every value within the error bound rounds to the same double (Ziv's
 //     rounding test); otherwise the slow path decides, so both paths give
 //     the same correctly rounded result except within 2^-95 of a rounding
@@ -32,6 +34,7 @@
 #define PANGU_PGMATH_H
 
 #include <cmath>
+#include <cstring>
 
 #include "pgmath_tables.h"
 
@@ -52,6 +55,25 @@ PGM_FN double fma_(double a, double b, double c) {
   return __fma_rn(a, b, c);
 #else
   return std::fma(a, b, c);
+#endif
+}
+
+PGM_FN long long as_bits(double x) {
+#if defined(__CUDA_ARCH__)
+  return __double_as_longlong(x);
+#else
+  long long b;
+  std::memcpy(&b, &x, sizeof b);
+  return b;
+#endif
+}
+PGM_FN double from_bits(long long b) {
+#if defined(__CUDA_ARCH__)
+  return __longlong_as_double(b);
+#else
+  double x;
+  std::memcpy(&x, &b, sizeof x);
+  return x;
 #endif
 }
 
@@ -215,67 +237,117 @@ __device__ __forceinline__ void prefetch_tables_l1() {
 }
 #endif
 
-// ln x as double-double for finite x > 0, relative error below 2^-80.
-PGM_FN dd log_fast(double x) {
-  int e;
-  double m = frexp(x, &e);  // x = m 2^e, m in [0.5, 1)
-  m *= 2.0;
-  e -= 1;
+// x = 2^e m for finite x > 0, m in [1/sqrt2, sqrt2), by the bits of x.
+PGM_FN double split_exponent(double x, int &e) {
+  long long bits = as_bits(x);
+  int shift = 0;
+  if ((bits >> 52) == 0) {  // subnormal: scale by 2^54 first (exact)
+    bits = as_bits(x * 0x1p54);
+    shift = 54;
+  }
+  e = (int)(bits >> 52) - 1023 - shift;
+  double m = from_bits((bits & 0x000fffffffffffffLL) | 0x3ff0000000000000LL);  // [1, 2)
   if (m > 1.4142135623730951) {
     m *= 0.5;
     e += 1;
   }
-  const int j = (int)((m - PGM_LOG_M0) * 512.0);
-  const double inv = log_tab(3 * j);
-  const dd L = {log_tab(3 * j + 1), log_tab(3 * j + 2)};
-  const dd p = two_prod(m, inv);                   // m inv exactly
-  const dd r = quick_two_sum(p.hi - 1.0, p.lo);    // p.hi - 1 exact (Sterbenz)
-  // log1p(r) = r - r^2/2 + r^3/3 + r^4 Q(r)
-  dd r2 = two_prod(r.hi, r.hi);
-  r2.lo += 2.0 * r.hi * r.lo;
-  const dd r3 = mul(r2, r);
-  const dd t3 = mul(r3, dd{0x1.5555555555555p-2, 0x1.5555555555555p-56});  // r^3/3
-  double q = -0x1.999999999999ap-4;             // -1/10
-  q = 0x1.c71c71c71c71cp-4 + r.hi * q;          // 1/9
-  q = -0x1.0000000000000p-3 + r.hi * q;         // -1/8
-  q = 0x1.2492492492492p-3 + r.hi * q;          // 1/7
-  q = -0x1.5555555555555p-3 + r.hi * q;         // -1/6
-  q = 0x1.999999999999ap-3 + r.hi * q;          // 1/5
-  q = -0x1.0000000000000p-2 + r.hi * q;         // -1/4
-  const double t4 = (r2.hi * r2.hi) * q;
-  dd lg = add(r, dd{-0.5 * r2.hi, -0.5 * r2.lo});
-  lg = add(lg, t3);
-  lg = add(lg, dd{t4, 0.0});
-  lg = add(lg, L);
-  if (e != 0) lg = add(mul_d(PGM_LN2, (double)e), lg);
-  return lg;
+  return m;
 }
 
-// exp t for a double-double t with |t.hi| <= 708 as hi + lo (relative error
-// below 2^-76) and the power of two k >> 7 still to apply.
-PGM_FN dd exp_fast(dd t, int &scale) {
-  const double kd = rint(t.hi * PGM_INV_LN2_128);
+// ln x = hi + lo for finite x > 0, error below 2^-80.5 + 2^-84 |ln x|.
+//   ln x = e ln2 + L + log1p(r), r = m inv - 1 = rh + rl exactly (two_prod),
+//   |rh| < 2^-9.49, |rl| <= 2^-53; L = 0 and rl = 0 in the interval centred
+//   on 1. log1p(r) = r - r^2/2 + f(r), f(r) = r^3 Q(r) with Q to its r^6 term
+//   (truncation below 2^-98); f(rh) carries about five roundings (below
+//   2^-80.9 for |f| < 2^-30); f(rh + rl) = f(rh) + rh^2 (1 - rh) rl up to
+//   2^-91; -r^2/2 is exact up to 2^-106. The high parts
+//   L + rh - rh^2/2 + f + e ln2_hi are summed by exact two-sums, each ordered
+//   by binade: |L| lies above every |rh| of its interval where L != 0 (a
+//   property of the table), and |e ln2| >= 0.69 > |ln m|. The low parts add to
+//   below 2^-51 + 2^-43.5 |ln x|, so their rounding is below 2^-95 |ln x|.
+PGM_FN dd log_fast(double x) {
+  int e;
+  const double m = split_exponent(x, e);
+  const int j = (int)((m - PGM_LOG_M0) * 512.0);
+  const double inv = log_tab(3 * j);
+  const double Lh = log_tab(3 * j + 1), Ll = log_tab(3 * j + 2);
+  const double ph = m * inv;
+  const double rl = fma_(m, inv, -ph);
+  const double rh = ph - 1.0;  // exact (Sterbenz)
+  const double sq = rh * rh;
+  const double sh = -0.5 * sq;
+  const double sl = -0.5 * fma_(rh, rh, -sq) - rh * rl;
+  double q = 0x1.c71c71c71c71cp-4;          // 1/9
+  q = fma_(rh, q, -0x1.0000000000000p-3);   // -1/8
+  q = fma_(rh, q, 0x1.2492492492492p-3);    // 1/7
+  q = fma_(rh, q, -0x1.5555555555555p-3);   // -1/6
+  q = fma_(rh, q, 0x1.999999999999ap-3);    // 1/5
+  q = fma_(rh, q, -0x1.0000000000000p-2);   // -1/4
+  q = fma_(rh, q, 0x1.5555555555555p-2);    // 1/3
+  const double f = (sq * rh) * q;
+  const dd s = quick_two_sum(Lh, rh);
+  const dd u = quick_two_sum(s.hi, sh);
+  const dd w = quick_two_sum(u.hi, f);
+  const dd z = quick_two_sum((double)e * PGM_LN2_HI, w.hi);
+  const double lo = ((Ll + rl) + (sl + (sq * rl) * (1.0 - rh))) + (double)e * PGM_LN2_LO +
+                    ((s.lo + u.lo) + (w.lo + z.lo));
+  return {z.hi, lo};
+}
+
+// e^t for t = th + tl (|th| < 700, |tl| <= 2^-33) as hi + lo with the power of
+// two k >> 7 still to apply, relative error below 2^-76.9.
+//   k = rint(th 128/ln2), r = t - k ln2/128 with |r| <= 2^-8.52: th - k C1 is
+//   exact (k C1 has at most 52 bits and lies within a factor of 2 of th, or
+//   th - k C1 fits in 53 bits), k C2 - tl has one rounding below 2^-78, and
+//   r = rh + rl by an exact two-sum (|rl| <= 2^-62).
+//   e^r - 1 = rh + rh^2/2 + rest, rest = rl (1 + rh) + rh^3 P(rh), P to the
+//   r^4 term (truncation below 2^-83); rh + rh^2/2 by an exact product and
+//   two-sum, rest < 2^-28 in double (below 2^-79).
+//   2^(k/128) e^r = Th + Th ph + (Th pl + Tl (1 + ph)): Th + Th ph exact, the
+//   rest (below 2^-27) in one fused rounding (below 2^-80).
+PGM_FN dd exp_fast(double th, double tl, int &scale) {
+  const double kd = rint(th * PGM_INV_LN2_128);
   const int k = (int)kd;
-  // r = t - k ln2/128, Cody-Waite: k C1 is exact and t.hi - k C1 exact
-  const dd kc2 = two_prod(kd, PGM_LN2_128_C2);
-  dd r = two_sum(t.hi - kd * PGM_LN2_128_C1, -kc2.hi);
-  r.lo += (t.lo - kc2.lo) - kd * PGM_LN2_128_C3;
-  r = quick_two_sum(r.hi, r.lo);
-  // exp(r) - 1 = r + r^2/2 + r^3 P(r)
-  dd r2 = two_prod(r.hi, r.hi);
-  r2.lo += 2.0 * r.hi * r.lo;
-  double P = 0x1.a01a01a01a01ap-16;             // 1/8!
-  P = 0x1.a01a01a01a01ap-13 + r.hi * P;         // 1/7!
-  P = 0x1.6c16c16c16c17p-10 + r.hi * P;         // 1/6!
-  P = 0x1.1111111111111p-7 + r.hi * P;          // 1/5!
-  P = 0x1.5555555555555p-5 + r.hi * P;          // 1/4!
-  P = 0x1.5555555555555p-3 + r.hi * P;          // 1/3!
-  dd q = add(r, dd{0.5 * r2.hi, 0.5 * r2.lo});
-  q = add(q, dd{(r2.hi * r.hi) * P, 0.0});
-  const dd E = add(dd{1.0, 0.0}, q);
+  const double a = th - kd * PGM_LN2_128_C1;
+  const double b = fma_(kd, PGM_LN2_128_C2, -tl);
+  const dd r = two_sum(a, -b);
+  const double rh = r.hi, rl = r.lo - kd * PGM_LN2_128_C3;
+  double P = 0x1.a01a01a01a01ap-13;         // 1/7!
+  P = fma_(rh, P, 0x1.6c16c16c16c17p-10);   // 1/6!
+  P = fma_(rh, P, 0x1.1111111111111p-7);    // 1/5!
+  P = fma_(rh, P, 0x1.5555555555555p-5);    // 1/4!
+  P = fma_(rh, P, 0x1.5555555555555p-3);    // 1/3!
+  const double sq = rh * rh;
+  const double rest = (0.5 * fma_(rh, rh, -sq) + fma_(rh, rl, rl)) + (sq * rh) * P;
+  const dd p = quick_two_sum(rh, 0.5 * sq);
+  const double pl = p.lo + rest;
   const int jj = k & 127;
   scale = k >> 7;  // arithmetic shift: floor(k / 128)
-  return mul(dd{exp_tab(2 * jj), exp_tab(2 * jj + 1)}, E);
+  const double Th = exp_tab(2 * jj), Tl = exp_tab(2 * jj + 1);
+  const dd h = two_prod(Th, p.hi);
+  const dd v = quick_two_sum(Th, h.hi);
+  return {v.hi, fma_(Th, pl, ((h.lo + v.lo) + Tl) + Tl * p.hi)};
+}
+
+// x^y for finite x > 0 when the fast path's error bound decides the rounding.
+// t = y ln x = th + tl is within |y| 2^-80.4 + |t| 2^-83.9 of y ln x (the
+// log's error times |y|, and the product's roundings), and e^t within a
+// relative 2^-76.9 of 2^scale (hi + lo); the bound below doubles each term.
+// The result is returned only if every value within it rounds to the same
+// double (Ziv's rounding test). |th| < 700 keeps the result normal.
+PGM_FN bool pow_fast(double x, double y, double &out) {
+  const dd l = log_fast(x);
+  const double th = l.hi * y;
+  if (!(fabs(th) < 700.0)) return false;
+  const double tl = fma_(l.hi, y, -th) + l.lo * y;
+  int scale;
+  const dd v0 = exp_fast(th, tl, scale);
+  const dd v = quick_two_sum(v0.hi, v0.lo);
+  const double err = v.hi * ((0x1p-76 + fabs(y) * 0x1p-79) + fabs(th) * 0x1p-83);
+  const double a = v.hi + (v.lo + err), b = v.hi + (v.lo - err);
+  if (a != b) return false;
+  out = a * from_bits((long long)(scale + 1023) << 52);  // exact: |scale| <= 1010
+  return true;
 }
 
 PGM_FN bool is_inf(double x) { return fabs(x) == HUGE_VAL; }
@@ -309,19 +381,7 @@ PGM_FN double pow(double x, double y) {
   } else if (is_inf(x)) {
     r = y < 0.0 ? 0.0 : HUGE_VAL;
   } else {
-    const dd t = mul_d(log_fast(x), y);
-    bool done = false;
-    if (fabs(t.hi) < 700.0) {
-      int scale;
-      const dd v = exp_fast(t, scale);
-      // error bound of v: exp part 2^-70, plus |t| times the log's 2^-78
-      const double err = fabs(v.hi) * (0x1p-70 + fabs(t.hi) * 0x1p-78);
-      const double a = v.hi + (v.lo + err), b = v.hi + (v.lo - err);
-      if (a == b) {
-        r = ldexp(a, scale);
-        done = true;
-      }
-    }
+    const bool done = pow_fast(x, y, r);
     if (!done) r = exp_round(mul_d(log_dd(x), y));  // slow path
   }
   return negate ? -r : r;

@@ -77,6 +77,67 @@ def test_fast_path_agrees_with_slow_path():
         assert not bad.any(), (x[bad][:3], y[bad][:3], fast[bad][:3], slow[bad][:3])
 
 
+def _pow_fast(x, y):
+    out = np.empty_like(x)
+    ok = np.empty(len(x), dtype=np.int32)
+    L.or_pgm_pow_fast(len(x), x.ctypes.data_as(_D), y.ctypes.data_as(_D),
+                      out.ctypes.data_as(_D), ok.ctypes.data_as(C.POINTER(C.c_int)))
+    return out, ok.astype(bool)
+
+
+def test_fast_path_next_to_one():
+    """The log intervals next to the one centred on 1 carry the largest
+    relative error of the fast path's log (|ln m| down to 2^-10 with the
+    product's low part up to 2^-53); large exponents magnify it in t."""
+    rng = np.random.default_rng(12)
+    n = 300000
+    side = rng.choice([-1.0, 1.0], n)
+    x = 1.0 + side * rng.uniform(1 / 1024, 3 / 1024, n)
+    y = rng.uniform(-2.5e5, 2.5e5, n)
+    fast, ok = _pow_fast(x, y)
+    slow = _pow_slow(x, y)
+    assert np.array_equal(fast[ok], slow[ok])
+    for xi, yi, oi in list(zip(x[ok], y[ok], fast[ok]))[:300]:
+        exact = (Decimal(float(xi)).ln() * Decimal(float(yi))).exp()
+        assert _is_correctly_rounded(oi, exact), (xi.hex(), yi.hex(), oi.hex())
+
+
+def test_fast_path_decides_almost_always():
+    """With the physics exponents over the floor-to-torus range of values the
+    fast path decides nearly every rounding (a warp waits for any lane that
+    falls to the slow path)."""
+    rng = np.random.default_rng(13)
+    n = 400000
+    x = 10 ** rng.uniform(-12, 6, n)
+    y = rng.choice([-13 / 9, -4 / 3, -5 / 3, 13 / 9 - 4 / 3, 1 / 3, 0.7, -1.4, 3.3], n)
+    fast, ok = _pow_fast(x, y)
+    assert ok.mean() > 0.99999, ok.mean()
+    assert np.array_equal(fast[ok], _pow(x[ok], y[ok]))
+
+
+def test_log_table_binades():
+    """The fast path sums L_j + r with an ordered (fast) two-sum: in every
+    interval with L_j != 0, |L_j| lies in a higher binade than any |r|."""
+    import math
+    import os
+    import re
+    here = os.path.dirname(os.path.abspath(__file__))
+    txt = open(os.path.join(here, "..", "pangu_b200", "csrc", "pgmath_tables.h")).read()
+    m0 = float.fromhex(re.search(r"#define PGM_LOG_M0 (\S+)", txt).group(1))
+    body = txt.split("PGM_LOG_TABLE_INIT {")[1].split("}")[0]
+    vals = [0.0 if v == "0.0" else float.fromhex(v)
+            for v in re.findall(r"(-?0x[0-9a-fp.+-]+|0\.0)", body)]
+    for j in range(len(vals) // 3):
+        inv, lh = vals[3 * j], vals[3 * j + 1]
+        lo, hi = max(m0 + j / 512, 2 ** -0.5), min(m0 + (j + 1) / 512, 2 ** 0.5)
+        rmax = max(abs(lo * inv - 1.0), abs(hi * inv - 1.0))
+        assert rmax < 2 ** -9.49
+        if lh == 0.0:
+            assert inv == 1.0
+            continue
+        assert math.frexp(abs(lh))[1] > math.frexp(rmax)[1], j
+
+
 def test_exp_log_correctly_rounded():
     rng = np.random.default_rng(8)
     e = rng.uniform(-700, 700, 2000)
