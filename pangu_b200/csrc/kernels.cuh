@@ -1473,21 +1473,45 @@ __global__ void __launch_bounds__(kThreads, 4) k_flux_div_update(Dims d, const d
   const double V = MUL(MUL(dx0, dx1), dx2);
   const double bdt = MUL(beta, dt[job_of(d, b)]);
   const long long sj = d.N1, sk = (long long)d.N1 * d.N2;
+  // Components in groups of kUpdGroup: every load of a group is issued before
+  // its first store (Uout may be Uinit, so the compiler would not move a
+  // later component's loads above an earlier store). Two per group: measured
+  // 2-4 % faster per RK2 cycle than one at a time on the 2D and 3D tori and
+  // Orszag-Tang; groups of three or more spill at the 64-register bound.
+  constexpr int kUpdGroup = 2;
 #pragma unroll
-  for (int v = 0; v < NPRIM; ++v) {
-    if (v >= d.NF) break;
-    const double *f1 = a_flux1(d, F1, b, v) + q;
-    double du = SUB(MUL(A1, f1[1]), MUL(A1, f1[0]));
-    if (d.ndim >= 2) {
-      const double *f2 = a_flux2(d, F2, b, v) + q;
-      du = ADD(du, SUB(MUL(A2, f2[sj]), MUL(A2, f2[0])));
+  for (int v0 = 0; v0 < NPRIM; v0 += kUpdGroup) {
+    double f1l[kUpdGroup], f1r[kUpdGroup], f2l[kUpdGroup], f2r[kUpdGroup], f3l[kUpdGroup],
+        f3r[kUpdGroup], u0[kUpdGroup];
+#pragma unroll
+    for (int c = 0; c < kUpdGroup; ++c) {
+      const int v = v0 + c;
+      if (v >= d.NF) break;
+      const double *f1 = a_flux1(d, F1, b, v) + q;
+      f1l[c] = f1[0];
+      f1r[c] = f1[1];
+      if (d.ndim >= 2) {
+        const double *f2 = a_flux2(d, F2, b, v) + q;
+        f2l[c] = f2[0];
+        f2r[c] = f2[sj];
+      }
+      if (d.ndim == 3) {
+        const double *f3 = a_flux3(d, F3, b, v) + q;
+        f3l[c] = f3[0];
+        f3r[c] = f3[sk];
+      }
+      u0[c] = a_cons0(d, Uinit, b, v)[q];
     }
-    if (d.ndim == 3) {
-      const double *f3 = a_flux3(d, F3, b, v) + q;
-      du = ADD(du, SUB(MUL(A3, f3[sk]), MUL(A3, f3[0])));
+#pragma unroll
+    for (int c = 0; c < kUpdGroup; ++c) {
+      const int v = v0 + c;
+      if (v >= d.NF) break;
+      double du = SUB(MUL(A1, f1r[c]), MUL(A1, f1l[c]));
+      if (d.ndim >= 2) du = ADD(du, SUB(MUL(A2, f2r[c]), MUL(A2, f2l[c])));
+      if (d.ndim == 3) du = ADD(du, SUB(MUL(A3, f3r[c]), MUL(A3, f3l[c])));
+      const double dudt = DIV(-du, V);
+      a_cons(d, Uout, b, v)[q] = ADD(u0[c], MUL(bdt, dudt));
     }
-    const double dudt = DIV(-du, V);
-    a_cons(d, Uout, b, v)[q] = ADD(a_cons0(d, Uinit, b, v)[q], MUL(bdt, dudt));
   }
 }
 
@@ -1676,16 +1700,28 @@ __device__ __forceinline__ void source_cell(const Dims &d, const pangu_params &p
     const long long plane = (long long)d.N2 * d.N1;
     const double *cn = d.ctab + (long long)b * L.ncen * plane + (long long)j * d.N1 + i +
                        (long long)L.nmet * plane;
+    // the four contractions first, then the four updates: no Christoffel load
+    // waits behind a store to U
+    double con[4];
 #pragma unroll
     for (int dir = 0; dir < 4; ++dir) {
-      double con = 0.0;
+      con[dir] = 0.0;
 #pragma unroll
       for (int r = 0; r < 4; ++r)
 #pragma unroll
         for (int c = 0; c < 4; ++c)
-          if (L.conn[c][dir][r] >= 0) con += T[r][c] * __ldg(cn + L.conn[c][dir][r] * plane);
+          if (L.conn[c][dir][r] >= 0)
+            con[dir] += T[r][c] * __ldg(cn + L.conn[c][dir][r] * plane);
+    }
+    const long long q = coff(d, k, j, i);
+    double u[4];
+#pragma unroll
+    for (int dir = 0; dir < 4; ++dir)
+      u[dir] = a_cons(d, U, b, dir == 0 ? d.pidx[ENY] : d.pidx[UX1] + dir - 1)[q];
+#pragma unroll
+    for (int dir = 0; dir < 4; ++dir) {
       const int v = dir == 0 ? d.pidx[ENY] : d.pidx[UX1] + dir - 1;
-      a_cons(d, U, b, v)[coff(d, k, j, i)] += con * sg * bdt;
+      a_cons(d, U, b, v)[q] = u[dir] + con[dir] * sg * bdt;
     }
   } else {
     double conn[4][4][4];
