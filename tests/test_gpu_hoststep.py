@@ -1,7 +1,9 @@
 """A job whose state lives in pinned host memory (HostState, step_host):
-the overlapped copies in and out give, cycle after cycle, the same bits as
-stepping the device-resident state, in FP64 and in the mixed form, with and
-without block-to-block ghost exchange."""
+the overlapped copies in and out (piece by piece, each piece going back in
+as soon as it has come out, with two device copies of container "1" used in
+turn) give, cycle after cycle, the same bits as stepping the device-resident
+state, in FP64 and in the mixed form, with and without block-to-block ghost
+exchange, and device-resident and host-resident cycles may alternate."""
 import numpy as np
 import pytest
 
@@ -39,3 +41,16 @@ def test_host_resident_cycles_match_device_cycles(name, precision):
         sim.step()
     torch.cuda.synchronize()
     np.testing.assert_array_equal(sim.primitives(), ref.primitives())
+    # and host-resident ones again, from the state pulled back to the host
+    # (an odd number of cycles, so the two device copies of container "1"
+    # have swapped roles)
+    sim.pull(host)
+    for _ in range(3):
+        ref.step()
+        sim.step_host(host)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(host.base_prim.double().numpy(), ref.primitives())
+    np.testing.assert_array_equal(host.one_prim.numpy(), ref.one.prim.cpu().numpy())
+    assert host.dt.item() == ref.dt.item()
+    np.testing.assert_array_equal(sim.primitives(), ref.primitives())
+    np.testing.assert_array_equal(sim.one.prim.cpu().numpy(), ref.one.prim.cpu().numpy())
