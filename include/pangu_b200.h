@@ -69,8 +69,9 @@ extern "C" {
 #define PANGU_HEAT_SHARMA 5
 /* Arithmetic of the engine (no reference counterpart; the reference is
  * FP64 throughout). MIXED stores primitives in FP32 (the pack's prim pointer
- * then addresses floats) and runs reconstruction, Riemann flux, electron
- * heating and the geometric source term (MKS/BL) in FP32; conserved variables
+ * then addresses floats) and runs reconstruction, Riemann flux, the floors of
+ * FixPrimitive, electron heating and the geometric source term (MKS/BL) in
+ * FP32; conserved variables
  * and their update, C2P, the metric and CT stay FP64. The conserved magnetic field is then evolved only
  * by the FP64 CT update: CalculateConservative leaves it unchanged, and
  * pangu_job_start computes it once from the initial primitives. */

@@ -1,6 +1,7 @@
 // engine_mixed.cu -- the mixed-precision instantiation of the engine's
 // kernels (namespace pgkmx): primitives stored in FP32; reconstruction,
-// Riemann fluxes, electron heating and the geometric source term in FP32;
+// Riemann fluxes, FixPrimitive's floors, electron heating and the geometric
+// source term in FP32;
 // conserved variables and the flux divergence update, C2P, the metric and CT
 // in FP64.
 // Built with --use_fast_math (FMA contraction, approximate FP32 division,
