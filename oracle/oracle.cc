@@ -887,6 +887,23 @@ void or_pgm_pow_fast(int n, const double *x, const double *y, double *out, int *
     out[i] = r;
   }
 }
+// The fast path's log and exp parts (hi + lo, and exp's power of two), for
+// the test of their error bounds.
+void or_pgm_log_fast(int n, const double *x, double *hi, double *lo) {
+  for (int i = 0; i < n; ++i) {
+    const pgm::dd l = pgm::log_fast(x[i]);
+    hi[i] = l.hi;
+    lo[i] = l.lo;
+  }
+}
+void or_pgm_exp_fast(int n, const double *th, const double *tl, double *hi, double *lo,
+                     int *scale) {
+  for (int i = 0; i < n; ++i) {
+    const pgm::dd v = pgm::exp_fast(th[i], tl[i], scale[i]);
+    hi[i] = v.hi;
+    lo[i] = v.lo;
+  }
+}
 void or_pgm_exp(int n, const double *x, double *out) {
   for (int i = 0; i < n; ++i) out[i] = pgm::exp(x[i]);
 }

@@ -138,6 +138,47 @@ def test_log_table_binades():
         assert math.frexp(abs(lh))[1] > math.frexp(rmax)[1], j
 
 
+def test_fast_path_error_bounds():
+    """The bounds the fast path's rounding test relies on, against 60-digit
+    decimals: the log within 2^-80.5 + 2^-84 |ln x| (arguments next to 1,
+    at the edges of the table's intervals and of [1/sqrt2, sqrt2), and over
+    the whole range), the exp within a relative 2^-76.9 (over |t| < 700,
+    with the largest reduced arguments, and with a low part)."""
+    rng = np.random.default_rng(14)
+    n = 1500
+    xs = np.concatenate([
+        1.0 + rng.choice([-1.0, 1.0], n) * rng.uniform(1 / 1024, 3 / 1024, n),
+        1.0 + rng.uniform(-1 / 1024, 1 / 1024, n),
+        (361.5 + rng.integers(0, 363, n) + rng.choice([1e-7, -1e-7, 0.5], n)) / 512,
+        10 ** rng.uniform(-300, 300, n),
+        np.ldexp(rng.choice([2 ** -0.5, 2 ** 0.5], n) * (1 + rng.uniform(-1e-3, 1e-3, n)),
+                 rng.integers(-5, 5, n)),
+    ])
+    hi, lo = np.empty_like(xs), np.empty_like(xs)
+    L.or_pgm_log_fast(len(xs), xs.ctypes.data_as(_D), hi.ctypes.data_as(_D),
+                      lo.ctypes.data_as(_D))
+    two = Decimal(2)
+    for x, h, l in zip(xs, hi, lo):
+        exact = Decimal(float(x)).ln()
+        err = abs(Decimal(float(h)) + Decimal(float(l)) - exact)
+        assert err <= two ** Decimal("-80.5") + two ** -84 * abs(exact), float(x).hex()
+    k = rng.integers(-120000, 120000, n)
+    th = np.concatenate([rng.uniform(-699, 699, n),
+                         (k + 0.5) * np.log(2) / 128 * (1 + rng.uniform(-1e-12, 1e-12, n)),
+                         rng.uniform(-0.01, 0.01, n)])
+    tl = th * np.concatenate([rng.uniform(-2 ** -43, 2 ** -43, n), np.zeros(n),
+                              rng.uniform(-2 ** -52, 2 ** -52, n)])
+    hi, lo = np.empty_like(th), np.empty_like(th)
+    sc = np.empty(len(th), dtype=np.int32)
+    L.or_pgm_exp_fast(len(th), th.ctypes.data_as(_D), tl.ctypes.data_as(_D),
+                      hi.ctypes.data_as(_D), lo.ctypes.data_as(_D),
+                      sc.ctypes.data_as(C.POINTER(C.c_int)))
+    for a, b, h, l, s in zip(th, tl, hi, lo, sc):
+        exact = (Decimal(float(a)) + Decimal(float(b))).exp()
+        v = (Decimal(float(h)) + Decimal(float(l))) * two ** int(s)
+        assert abs(v - exact) / exact <= two ** Decimal("-76.9"), (float(a).hex(), float(b).hex())
+
+
 def test_exp_log_correctly_rounded():
     rng = np.random.default_rng(8)
     e = rng.uniform(-700, 700, 2000)
